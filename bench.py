@@ -1,0 +1,309 @@
+#!/usr/bin/env python3
+"""Benchmark: HEOM ADO-updates/s in FP64 on B200.
+
+Workload (one GPU): 8 sites, one Drude-Lorentz bath per site (lambda = 35
+cm^-1, invnu = 50 fs, T = 300 K) with one Matsubara term (16 modes), depth 8:
+735,471 ADOs of 8 x 8 complex doubles (753 MB per state); RK4 with dt = 0.5
+fs.  Synthetic H (seed 22): diagonal U[12100, 12700] cm^-1, off-diagonal
+N(0, 50 cm^-1), real-symmetric.  One "step" = one RK4 step of the whole
+hierarchy; 1 ADO-update = one ADO advanced through one RK4 step.
+
+  value     device-resident throughput: K steps enqueued on the handle's
+            stream, timed with CUDA events on that stream (state is 753 MB,
+            larger than L2, so no flush is needed between steps)
+  e2e       the same metric through the C ABI with host buffers: upload of
+            the initial hierarchy state from pinned host memory
+            (heom_set_state), K steps with the top matrix recorded every 10
+            steps and copied back to the host (heom_propagate)
+  roofline  the heom_stage kernel (every launch in the timed region is one):
+            algorithmic bytes per launch = ADOs x 32 N^2 B (read the stage
+            input, write the stage output) / average launch duration
+  cpu_baseline  the reference's own heom_ode.cl + rk_weighted_add.cl compiled
+            for the host (oracle/_ref) with OpenMP over all host cores, one
+            RK4 step of the same workload
+
+--impl reference times that CPU implementation as the reference arm.
+Multi-GPU (torchrun): every rank propagates its own replica of the hierarchy
+(replicas only: the single-hierarchy path has no exchange step), value is the
+sum of ADO-updates over ranks / the max over ranks of the device time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "dm-heom_b200"))
+
+METRIC = "HEOM ADO-updates/s FP64 on 1 B200; batched & adjoint vs plain at \u22641e-10 error"
+UNIT = "ADO-updates/s"
+N_SITES, DEPTH, MATSUBARAS, SEED, DT = 8, 8, 2, 22, 0.5e-15
+OBSERVE_EVERY = 10
+FALLBACK_HBM = 6650.0
+
+
+def synthetic_h(n, seed):
+    rng = np.random.default_rng(seed)
+    h = np.zeros((n, n))
+    diag = rng.uniform(12100.0, 12700.0, size=n)
+    iu = np.triu_indices(n, 1)
+    h[iu] = rng.normal(0.0, 50.0, size=len(iu[0]))
+    h = h + h.T
+    h[np.diag_indices(n)] = diag
+    return h
+
+
+def workload_config(scheme):
+    return {"workload": "8 sites, 1 Drude-Lorentz bath/site, 1 Matsubara term (16 modes), depth 8, "
+                        "735471 ADOs of 8x8, RK4 dt=0.5 fs",
+            "ados": 735471, "states": N_SITES, "modes": 16, "depth": DEPTH, "dt_fs": 0.5,
+            "rk4_scheme": scheme, "l2": "inputs larger than L2 (753 MB state), no flush",
+            "seed": SEED}
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+def profiled_traffic():
+    """Per-launch DRAM bytes of heom_stage from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "heom_stage_cfg2.md")
+    try:
+        for line in open(path):
+            if line.strip().startswith("traffic_bytes_per_launch"):
+                return float(line.split("=")[1].strip().split()[0])
+    except Exception:
+        pass
+    return None
+
+
+def cpu_reference_sample(steps_cap=1, scheme_note="reference"):
+    """Time the reference's own kernels (compiled for the host) on the bench
+    workload: RK4 steps of the full hierarchy with all host threads."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import heom_oracle as ho
+    prob = ho.build_problem(ho.drude_system(N_SITES, DEPTH, MATSUBARAS, seed=SEED))
+    y = prob.initial_state()
+    threads = os.cpu_count() or 1
+    kind = "reference" if ho.ref_lib() is not None else "port"
+    step = (lambda v: ho.ref_rk4_step(prob, DT, v, threads)) if kind == "reference" else \
+        (lambda v: ho.rk4_step(prob, DT, v, threads))
+    y = step(y)  # warm-up (page in, thread pool)
+    t0 = time.perf_counter()
+    for _ in range(steps_cap):
+        y = step(y)
+    secs = time.perf_counter() - t0
+    value = prob.graph.nodes * steps_cap / secs
+    return {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"{steps_cap} RK4 step(s) of the full 735471-ADO hierarchy "
+                      f"({'heom_ode.cl + rk_weighted_add.cl compiled for the host' if kind == 'reference' else 'oracle C port'}, "
+                      f"OpenMP over {threads} threads), {secs:.2f} s"}
+
+
+def run_reference_arm(args, rank):
+    if rank != 0:
+        return
+    # each step is one full-hierarchy RK4 step of the reference kernels on the
+    # host; the number of timed steps is capped so the run ends in minutes
+    per_step_cap = max(1, min(args.steps, 6))
+    base = cpu_reference_sample(steps_cap=per_step_cap)
+    line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT,
+            "n_gpus": args.gpus, "steps": per_step_cap, "warmup": 1,
+            "ms_per_step": 735471 / base["value"] * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config("classical RK4 (rk_weighted_add)"),
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": f"requested --steps {args.steps}; timed {per_step_cap} full-hierarchy steps on the host"}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--scheme", default="product", choices=["product", "horner", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+
+    import torch
+    import heom_b200 as hb
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    h = synthetic_h(N_SITES, SEED)
+    system = hb.System(h, [35.0] * N_SITES, [50.0] * N_SITES, [0.0] * N_SITES, MATSUBARAS, 300.0, DEPTH)
+    H = hb.from_system(system, device=local_rank, scheme=args.scheme)
+    nodes = H.matrices
+    y0 = torch.zeros(H.state_len, dtype=torch.float64, pin_memory=True)
+    y0[0] = 1.0
+    H.set_state(y0.numpy())
+    stream = torch.cuda.ExternalStream(H.stream(), device=local_rank)
+
+    # warm-up
+    H.rk4_steps(DT, max(args.warmup, 0))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local_rank)
+    barrier()
+    launches0 = H.kernel_launches()
+    clocks.start()
+    with torch.cuda.stream(stream):
+        start.record(stream)
+        H.rk4_steps_async(DT, args.steps)
+        stop.record(stream)
+    H.synchronize()
+    clk = clocks.stop()
+    barrier()
+    launches = H.kernel_launches() - launches0
+    ms = start.elapsed_time(stop)
+    if dist is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    secs = ms / 1e3
+    value = world * nodes * args.steps / secs
+    per_launch_s = secs / launches if args.scheme != "reference" else None
+
+    # e2e through the C ABI with host buffers
+    barrier()
+    t0 = time.perf_counter()
+    H.set_state(y0.numpy())
+    tops = H.propagate(DT, args.steps - args.steps % OBSERVE_EVERY or OBSERVE_EVERY, OBSERVE_EVERY)
+    e2e_secs = time.perf_counter() - t0
+    e2e_steps = args.steps - args.steps % OBSERVE_EVERY or OBSERVE_EVERY
+    if dist is not None:
+        t = torch.tensor([e2e_secs], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_secs = float(t.item())
+    e2e_value = world * nodes * e2e_steps / e2e_secs
+    h2d = H.state_len * 8
+    d2h = tops.size * 8
+    trace = float(np.sum([tops[-1][(N_SITES + 1) * 2 * i] for i in range(N_SITES)]))
+
+    peak, peak_kind = measured_hbm_peak()
+    roofline = None
+    if per_launch_s:
+        alg_bytes = nodes * 32 * N_SITES * N_SITES
+        achieved = alg_bytes / per_launch_s / 1e9
+        traffic = profiled_traffic()
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "traffic": traffic,
+                    "peak_source": f"{peak_kind} hbm_gbs", "kernel": "heom_stage",
+                    "alg_bytes_per_launch": alg_bytes, "avg_launch_us": per_launch_s * 1e6}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded H, Drude-Lorentz baths)",
+                "config": dict(workload_config(args.scheme),
+                               parallelism=f"replicas{world}" if world > 1 else "single"),
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / e2e_steps,
+                        "d2h_bytes_per_step": d2h / e2e_steps,
+                        "note": f"{e2e_steps} steps: full state upload from pinned host memory + "
+                                f"top matrix every {OBSERVE_EVERY} steps copied back; final trace {trace:.15f}"},
+                "gpu_launches": int(launches), "roofline": roofline, "clocks": clk}
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_reference_sample(steps_cap=1)
+        print(json.dumps(line), flush=True)
+
+    H.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

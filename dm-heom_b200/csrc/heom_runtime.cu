@@ -1,0 +1,897 @@
+// heom_runtime.cu -- implementation of the C ABI in include/heom_b200.h.
+//
+// Owns the device copies of the hierarchy tables (the role of heom::ode,
+// dm-heom/src/heom/ode.cpp:35-95), the propagation state (the y_n buffers of
+// population_dynamics_solver, dm-heom/include/heom/population_dynamics_solver.hpp:90-91)
+// and the RK4 stepping that the reference delegates to the noma/num stepper
+// (population_dynamics_solver.hpp:242).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "heom_b200.h"
+#include "heom_kernels.cuh"
+
+using heomk::StageParams;
+
+namespace {
+
+constexpr double kHbar = 1.05457148e-34; // dm-heom/cl/heom/common.cl:46
+constexpr int kMaxStates = 16;
+constexpr int kMaxWidth = 255;
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                        \
+    do {                                                                                      \
+        cudaError_t err_ = (expr);                                                            \
+        if (err_ != cudaSuccess)                                                              \
+            return fail(HEOM_E_CUDA, "%s failed: %s", #expr, cudaGetErrorString(err_));        \
+    } while (0)
+
+// Factors of the RK4 stability polynomial 1 + z + z^2/2 + z^3/6 + z^4/24 =
+// prod_k (1 - z / r_k); the stage coefficient is -1/r_k (times the step size).
+// Roots r = -1.7294442310677054566 +/- 0.8889743761218658272 i and
+//           -0.2705557689322945434 +/- 2.5047759043624344897 i
+// (computed at 50 digits; the four -1/r_k sum to 1).
+constexpr double kProdBeta[4][2] = {
+    {0.4573733434972976, 0.23510048799854266},
+    {0.4573733434972976, -0.23510048799854266},
+    {0.04262665650270243, -0.3946329531721134},
+    {0.04262665650270243, 0.3946329531721134},
+};
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    ~DevBuf() { reset(); }
+    void reset()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    int alloc(size_t count)
+    {
+        reset();
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return fail(HEOM_E_NOMEM, "cudaMalloc of %zu bytes failed: %s", count * sizeof(T),
+                        cudaGetErrorString(e));
+        }
+        n = count;
+        return 0;
+    }
+};
+
+typedef void (*stage_fn_t)(const StageParams);
+
+template <int N, bool RH>
+stage_fn_t pick_epi(int epi)
+{
+    switch (epi) {
+    case heomk::EPI_PURE: return heomk::heom_stage<N, RH, heomk::EPI_PURE>;
+    case heomk::EPI_AXPY_SELF: return heomk::heom_stage<N, RH, heomk::EPI_AXPY_SELF>;
+    case heomk::EPI_AXPY_Y: return heomk::heom_stage<N, RH, heomk::EPI_AXPY_Y>;
+    default: return heomk::heom_stage<N, RH, heomk::EPI_ACC>;
+    }
+}
+
+template <int N>
+stage_fn_t pick_n(bool real_h, int epi)
+{
+    return real_h ? pick_epi<N, true>(epi) : pick_epi<N, false>(epi);
+}
+
+stage_fn_t pick_stage(int n, bool real_h, int epi)
+{
+    switch (n) {
+#define HEOM_CASE(K) \
+    case K: return pick_n<K>(real_h, epi);
+        HEOM_CASE(1) HEOM_CASE(2) HEOM_CASE(3) HEOM_CASE(4) HEOM_CASE(5) HEOM_CASE(6)
+        HEOM_CASE(7) HEOM_CASE(8) HEOM_CASE(9) HEOM_CASE(10) HEOM_CASE(11) HEOM_CASE(12)
+        HEOM_CASE(13) HEOM_CASE(14) HEOM_CASE(15) HEOM_CASE(16)
+#undef HEOM_CASE
+    default: return nullptr;
+    }
+}
+
+// number of tuples over d coordinates with sum <= r
+int64_t simplex_count(int d, int r, const std::vector<std::vector<int64_t>>& binom)
+{
+    if (r < 0) return 0;
+    return binom[r + d][d];
+}
+
+} // namespace
+
+namespace heomhost {
+int set_error(int code, const std::string& msg)
+{
+    g_last_error = msg;
+    return code;
+}
+} // namespace heomhost
+
+struct heom_buffer {
+    heom_handle* owner = nullptr;
+    DevBuf<double2> data;
+    bool borrowed = false;
+};
+
+struct heom_handle {
+    heom_options opt{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int sm_count = 0;
+
+    // instance sizes
+    int N = 0, M = 0, B = 0, BPS = 0, W = 0, D = 0;
+    int64_t nodes = 0;
+    int32_t first_non_plus = 0;
+    int LS = 0, SL = 0;
+    bool real_h = true;
+
+    // host copies in reference layout
+    std::vector<int32_t> coupling, tuples, plus, minus;
+    std::vector<double> ham, pss, pf_same, pf_circ, cbk, cbk_sqrt;
+    std::vector<uint8_t> mask;
+    std::vector<int64_t> int_of_ref, ref_of_int;
+    int64_t top_int = 0;
+
+    // device tables
+    DevBuf<int32_t> d_nbr;
+    DevBuf<uint8_t> d_tup;
+    DevBuf<double2> d_pss, d_kmin, d_hs, d_gamma0;
+    DevBuf<double> d_cplus;
+    DevBuf<int16_t> d_slots;
+    DevBuf<int64_t> d_ref_of_int;
+
+    // propagation state + stage buffers
+    heom_buffer y;
+    DevBuf<double2> work[5];
+    DevBuf<double2> xfer;   // reference-layout staging buffer for host transfers
+    DevBuf<double2> toplog;
+    DevBuf<int> d_flag;
+
+    // launch accounting
+    int64_t launches = 0;
+    int stage_blocks[4] = {0, 0, 0, 0};
+
+    // cached graph of one RK4 step
+    cudaGraphExec_t step_graph = nullptr;
+    double graph_dt = 0.0;
+
+    size_t state_elems() const { return (size_t)nodes * N * N; }
+};
+
+namespace {
+
+int G_of(int n) { return heomk::kThreads / (n * n); }
+
+int build_neighbours(heom_handle* h)
+{
+    // internal neighbour table with the reference's gating folded in:
+    //   plus read only when uid < first_non_plus_id (heom_ode.cl:183) and mask[plus] != 0 (:199)
+    //   minus read only when tuple > 0 (:293) and mask[minus] != 0 (:297)
+    const int W = h->W;
+    std::vector<int32_t> nbr((size_t)h->nodes * 2 * W);
+    std::vector<uint8_t> tup((size_t)h->nodes * W);
+    std::vector<double2> pss(h->nodes);
+    for (int64_t u = 0; u < h->nodes; ++u) {
+        const int64_t r = h->ref_of_int[u];
+        for (int m = 0; m < W; ++m) {
+            const int32_t t = h->tuples[r * W + m];
+            tup[u * W + m] = (uint8_t)t;
+            int32_t pv = -1, mv = -1;
+            const int32_t pr = h->plus[r * W + m];
+            if (r < h->first_non_plus && pr >= 0 && h->mask[pr]) pv = (int32_t)h->int_of_ref[pr];
+            const int32_t mr = h->minus[r * W + m];
+            if (t > 0 && mr >= 0 && h->mask[mr]) mv = (int32_t)h->int_of_ref[mr];
+            nbr[u * 2 * W + m] = pv;
+            nbr[u * 2 * W + W + m] = mv;
+        }
+        pss[u] = make_double2(h->pss[2 * r], h->pss[2 * r + 1]);
+    }
+    if (!h->d_nbr.p) {
+        if (int rc = h->d_nbr.alloc(nbr.size())) return rc;
+        if (int rc = h->d_tup.alloc(tup.size())) return rc;
+        if (int rc = h->d_pss.alloc(pss.size())) return rc;
+    }
+    CUDA_TRY(cudaMemcpy(h->d_nbr.p, nbr.data(), nbr.size() * 4, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(h->d_tup.p, tup.data(), tup.size(), cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(h->d_pss.p, pss.data(), pss.size() * 16, cudaMemcpyHostToDevice));
+    return 0;
+}
+
+int upload_hamiltonian(heom_handle* h)
+{
+    const int N = h->N;
+    std::vector<double2> hs(N * N), g0(N * N);
+    h->real_h = true;
+    for (int q = 0; q < N * N; ++q) {
+        hs[q] = make_double2(h->ham[2 * q] / kHbar, h->ham[2 * q + 1] / kHbar);
+        if (h->ham[2 * q + 1] != 0.0) h->real_h = false;
+    }
+    // same term (heom_ode.cl:138-168): for i != j subtract pf_same of every
+    // bath coupled to site i and to site j
+    for (int i = 0; i < N; ++i)
+        for (int j = 0; j < N; ++j) {
+            double gr = 0.0, gi = 0.0;
+            if (i != j)
+                for (int b = 0; b < h->BPS; ++b) {
+                    const int bi = h->coupling[i * h->BPS + b];
+                    if (bi >= 0) { gr -= h->pf_same[2 * bi]; gi -= h->pf_same[2 * bi + 1]; }
+                    const int bj = h->coupling[j * h->BPS + b];
+                    if (bj >= 0) { gr -= h->pf_same[2 * bj]; gi -= h->pf_same[2 * bj + 1]; }
+                }
+            g0[i * N + j] = make_double2(gr, gi);
+        }
+    if (!h->d_hs.p) {
+        if (int rc = h->d_hs.alloc(N * N)) return rc;
+        if (int rc = h->d_gamma0.alloc(N * N)) return rc;
+    }
+    CUDA_TRY(cudaMemcpy(h->d_hs.p, hs.data(), hs.size() * 16, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(h->d_gamma0.p, g0.data(), g0.size() * 16, cudaMemcpyHostToDevice));
+    // the real/complex-H kernel variant may change: re-resolve launch shapes and graphs
+    for (int& b : h->stage_blocks) b = 0;
+    if (h->step_graph) {
+        cudaGraphExecDestroy(h->step_graph);
+        h->step_graph = nullptr;
+    }
+    return 0;
+}
+
+int upload_coefficients(heom_handle* h)
+{
+    const int W = h->W, LS = h->LS, M = h->M;
+    std::vector<double> cplus((size_t)W * LS, 0.0);
+    std::vector<double2> kmin((size_t)3 * W * LS, make_double2(0.0, 0.0));
+    for (int sl = 0; sl < W; ++sl) {
+        const int b = sl / M;
+        const int m = sl - b * M;
+        const double cr = h->cbk[2 * sl], ci = h->cbk[2 * sl + 1];
+        const double qr = m == 0 ? h->pf_circ[2 * b] : 0.0;
+        const double qi = m == 0 ? h->pf_circ[2 * b + 1] : 0.0;
+        const double habs = std::hypot(cr, ci);
+        for (int n = 0; n < LS; ++n) {
+            cplus[sl * LS + n] = std::sqrt((n + 1.0) * habs / kHbar); // heom_ode.cl:211
+            const double sc = std::sqrt(n / habs * kHbar);             // heom_ode.cl:321
+            const double kir = sc * (-ci / kHbar + qr), kii = sc * (cr / kHbar + qi);
+            const double kjr = sc * (ci / kHbar + qr), kji = sc * (-cr / kHbar + qi);
+            kmin[0 * W * LS + sl * LS + n] = make_double2(kir, kii);
+            kmin[1 * W * LS + sl * LS + n] = make_double2(kjr, kji);
+            kmin[2 * W * LS + sl * LS + n] = make_double2(2.0 * sc * qr, 2.0 * sc * qi);
+        }
+    }
+    // slots of each state: b * M + m for every bath b coupled to the state
+    std::vector<int16_t> slots((size_t)h->N * h->SL, (int16_t)-1);
+    for (int s = 0; s < h->N; ++s) {
+        int q = 0;
+        for (int b = 0; b < h->BPS; ++b) {
+            const int bs = h->coupling[s * h->BPS + b];
+            if (bs < 0) continue;
+            for (int m = 0; m < M; ++m) slots[s * h->SL + q++] = (int16_t)(bs * M + m);
+        }
+    }
+    if (int rc = h->d_cplus.alloc(cplus.size())) return rc;
+    if (int rc = h->d_kmin.alloc(kmin.size())) return rc;
+    if (int rc = h->d_slots.alloc(slots.size())) return rc;
+    CUDA_TRY(cudaMemcpy(h->d_cplus.p, cplus.data(), cplus.size() * 8, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(h->d_kmin.p, kmin.data(), kmin.size() * 16, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(h->d_slots.p, slots.data(), slots.size() * 2, cudaMemcpyHostToDevice));
+    return 0;
+}
+
+StageParams base_params(const heom_handle* h)
+{
+    StageParams p{};
+    p.nbr = h->d_nbr.p;
+    p.tup = h->d_tup.p;
+    p.pss = h->d_pss.p;
+    p.cplus = h->d_cplus.p;
+    p.kmin = h->d_kmin.p;
+    p.hs = h->d_hs.p;
+    p.gamma0 = h->d_gamma0.p;
+    p.slots = h->d_slots.p;
+    p.nodes = h->nodes;
+    p.W = h->W;
+    p.LS = h->LS;
+    p.SL = h->SL;
+    return p;
+}
+
+// resolve the launch shape of a stage variant (outside of any stream capture)
+int resolve_stage(heom_handle* h, int epi, stage_fn_t* fn_out, size_t* smem_out)
+{
+    stage_fn_t fn = pick_stage(h->N, h->real_h, epi);
+    if (!fn) return fail(HEOM_E_UNSUPPORTED, "states = %d not supported", h->N);
+    const int G = G_of(h->N);
+    const size_t smem = heomk::stage_smem_bytes(G, h->W, h->LS);
+    int& blocks = h->stage_blocks[epi];
+    if (blocks == 0) {
+        if (smem > 48 * 1024)
+            CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem));
+        int per_sm = 0;
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn,
+                                                               heomk::kThreads, smem));
+        if (per_sm < 1) return fail(HEOM_E_UNSUPPORTED, "stage kernel cannot be resident");
+        const int64_t groups = (h->nodes + G - 1) / G;
+        blocks = (int)std::min<int64_t>(groups, (int64_t)per_sm * h->sm_count);
+    }
+    *fn_out = fn;
+    *smem_out = smem;
+    return 0;
+}
+
+int launch_stage(heom_handle* h, int epi, const double2* in, const double2* y, double2* out,
+                 double2* acc, double2 beta, int acc_init)
+{
+    stage_fn_t fn = nullptr;
+    size_t smem = 0;
+    if (int rc = resolve_stage(h, epi, &fn, &smem)) return rc;
+    StageParams p = base_params(h);
+    p.in = in;
+    p.y = y;
+    p.out = out;
+    p.acc = acc;
+    p.beta = beta;
+    p.acc_init = acc_init;
+    const int blocks = h->stage_blocks[epi];
+    fn<<<blocks, heomk::kThreads, smem, h->stream>>>(p);
+    h->launches++;
+    CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+int launch_wadd(heom_handle* h, int n, double step, double2* out, const double2* y,
+                const double* c, const double2* const* k)
+{
+    heomk::WaddParams p{};
+    p.out = reinterpret_cast<double*>(out);
+    p.y = reinterpret_cast<const double*>(y);
+    p.n = n;
+    p.h = step;
+    p.len = (int64_t)h->state_elems() * 2;
+    for (int l = 0; l < 7; ++l) {
+        p.c[l] = l < n ? c[l] : 0.0;
+        p.k[l] = l < n ? reinterpret_cast<const double*>(k[l]) : p.y;
+    }
+    const int blocks = std::max(1, std::min<int>((int)((p.len + 255) / 256), h->sm_count * 8));
+    heomk::heom_weighted_add<<<blocks, 256, 0, h->stream>>>(p);
+    h->launches++;
+    CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+int ensure_work(heom_handle* h, int count)
+{
+    for (int q = 0; q < count; ++q)
+        if (!h->work[q].p)
+            if (int rc = h->work[q].alloc(h->state_elems())) return rc;
+    return 0;
+}
+
+// enqueue one RK4 step of y_n (in place) on the handle's stream
+int enqueue_step(heom_handle* h, double dt)
+{
+    double2* y = h->y.data.p;
+    const double2 zero = make_double2(0.0, 0.0);
+    switch (h->opt.rk4_scheme) {
+    case HEOM_RK4_PRODUCT: {
+        double2* a = h->work[0].p;
+        double2* b = h->work[1].p;
+        const double2* ins[4] = {y, a, b, a};
+        double2* outs[4] = {a, b, a, y};
+        for (int k = 0; k < 4; ++k) {
+            const double2 beta = make_double2(dt * kProdBeta[k][0], dt * kProdBeta[k][1]);
+            if (int rc = launch_stage(h, heomk::EPI_AXPY_SELF, ins[k], nullptr, outs[k], nullptr, beta, 0))
+                return rc;
+        }
+        return 0;
+    }
+    case HEOM_RK4_HORNER: {
+        double2* a = h->work[0].p;
+        double2* b = h->work[1].p;
+        const double c[4] = {dt / 4.0, dt / 3.0, dt / 2.0, dt};
+        if (int rc = launch_stage(h, heomk::EPI_AXPY_SELF, y, nullptr, a, nullptr, make_double2(c[0], 0.0), 0)) return rc;
+        if (int rc = launch_stage(h, heomk::EPI_AXPY_Y, a, y, b, nullptr, make_double2(c[1], 0.0), 0)) return rc;
+        if (int rc = launch_stage(h, heomk::EPI_AXPY_Y, b, y, a, nullptr, make_double2(c[2], 0.0), 0)) return rc;
+        if (int rc = launch_stage(h, heomk::EPI_AXPY_Y, a, y, y, nullptr, make_double2(c[3], 0.0), 0)) return rc;
+        return 0;
+    }
+    default: { // HEOM_RK4_REFERENCE
+        double2* k1 = h->work[0].p;
+        double2* k2 = h->work[1].p;
+        double2* k3 = h->work[2].p;
+        double2* k4 = h->work[3].p;
+        double2* st = h->work[4].p;
+        const double2* ks[4] = {k1, k2, k3, k4};
+        const double a2[1] = {0.5}, a3[2] = {0.0, 0.5}, a4[3] = {0.0, 0.0, 1.0};
+        const double bb[4] = {1.0 / 6, 1.0 / 3, 1.0 / 3, 1.0 / 6};
+        if (int rc = launch_stage(h, heomk::EPI_PURE, y, nullptr, k1, nullptr, zero, 0)) return rc;
+        if (int rc = launch_wadd(h, 1, dt, st, y, a2, ks)) return rc;
+        if (int rc = launch_stage(h, heomk::EPI_PURE, st, nullptr, k2, nullptr, zero, 0)) return rc;
+        if (int rc = launch_wadd(h, 2, dt, st, y, a3, ks)) return rc;
+        if (int rc = launch_stage(h, heomk::EPI_PURE, st, nullptr, k3, nullptr, zero, 0)) return rc;
+        if (int rc = launch_wadd(h, 3, dt, st, y, a4, ks)) return rc;
+        if (int rc = launch_stage(h, heomk::EPI_PURE, st, nullptr, k4, nullptr, zero, 0)) return rc;
+        return launch_wadd(h, 4, dt, y, y, bb, ks);
+    }
+    }
+}
+
+int prepare_scheme(heom_handle* h)
+{
+    switch (h->opt.rk4_scheme) {
+    case HEOM_RK4_PRODUCT:
+    case HEOM_RK4_HORNER: return ensure_work(h, 2);
+    case HEOM_RK4_REFERENCE: return ensure_work(h, 5);
+    default: return fail(HEOM_E_ARG, "unknown rk4 scheme %d", h->opt.rk4_scheme);
+    }
+}
+
+int launches_per_step(const heom_handle* h)
+{
+    return h->opt.rk4_scheme == HEOM_RK4_REFERENCE ? 8 : 4;
+}
+
+int run_steps(heom_handle* h, double dt, int64_t steps)
+{
+    if (steps <= 0) return 0;
+    if (int rc = prepare_scheme(h)) return rc;
+    if (!h->opt.use_graphs) {
+        for (int64_t s = 0; s < steps; ++s)
+            if (int rc = enqueue_step(h, dt)) return rc;
+        return 0;
+    }
+    if (h->step_graph && h->graph_dt != dt) {
+        cudaGraphExecDestroy(h->step_graph);
+        h->step_graph = nullptr;
+    }
+    if (!h->step_graph) {
+        // make sure launch shapes are resolved outside of capture
+        for (int e = 0; e < 4; ++e) {
+            stage_fn_t fn = nullptr;
+            size_t smem = 0;
+            if (int rc = resolve_stage(h, e, &fn, &smem)) return rc;
+        }
+        cudaGraph_t graph = nullptr;
+        const int64_t saved = h->launches;
+        CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = enqueue_step(h, dt);
+        cudaError_t ce = cudaStreamEndCapture(h->stream, &graph);
+        h->launches = saved;
+        if (rc) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        if (ce != cudaSuccess) return fail(HEOM_E_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+        ce = cudaGraphInstantiate(&h->step_graph, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) return fail(HEOM_E_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ce));
+        h->graph_dt = dt;
+    }
+    for (int64_t s = 0; s < steps; ++s) {
+        CUDA_TRY(cudaGraphLaunch(h->step_graph, h->stream));
+        h->launches += launches_per_step(h);
+    }
+    return 0;
+}
+
+int check_desc(const heom_instance_desc* d)
+{
+    if (!d) return fail(HEOM_E_ARG, "desc is NULL");
+    if (d->states < 1 || d->states > kMaxStates)
+        return fail(HEOM_E_UNSUPPORTED, "states = %d outside 1..%d", d->states, kMaxStates);
+    if (d->matsubaras < 1 || d->baths < 1 || d->baths_per_state < 1)
+        return fail(HEOM_E_ARG, "matsubaras, baths and baths_per_state must be >= 1");
+    if (d->ado_width != d->baths * d->matsubaras)
+        return fail(HEOM_E_TABLE, "ado_width %d != baths * matsubaras", d->ado_width);
+    if (d->ado_width > kMaxWidth) return fail(HEOM_E_UNSUPPORTED, "ado_width %d too large", d->ado_width);
+    if (d->ado_depth < 1 || d->ado_depth > 250) return fail(HEOM_E_UNSUPPORTED, "ado_depth %d", d->ado_depth);
+    if (d->matrices < 1 || d->matrices > INT32_MAX) return fail(HEOM_E_ARG, "matrices = %lld", (long long)d->matrices);
+    if (d->first_non_plus_id < 0 || d->first_non_plus_id > d->matrices)
+        return fail(HEOM_E_TABLE, "first_non_plus_id out of range");
+    if (!d->baths_coupling || !d->hamiltonian || !d->ado_tuples || !d->ado_plus || !d->ado_minus ||
+        !d->pf_same_sum || !d->pf_same || !d->pf_circ || !d->cbk || !d->cbk_sqrt)
+        return fail(HEOM_E_ARG, "a table pointer is NULL");
+    for (int q = 0; q < d->states * d->baths_per_state; ++q)
+        if (d->baths_coupling[q] >= d->baths) return fail(HEOM_E_TABLE, "baths_coupling value out of range");
+    const int64_t n = d->matrices * d->ado_width;
+    for (int64_t q = 0; q < n; ++q) {
+        const int32_t t = d->ado_tuples[q], p = d->ado_plus[q], m = d->ado_minus[q];
+        if (t < 0 || t > d->ado_depth) return fail(HEOM_E_TABLE, "ado_tuples[%lld] = %d out of range", (long long)q, t);
+        if (!(p == HEOM_INVALID_UID || (p >= 0 && p < d->matrices)))
+            return fail(HEOM_E_TABLE, "ado_plus[%lld] = %d out of range", (long long)q, p);
+        if (!(m == HEOM_INVALID_UID || (m >= 0 && m < d->matrices)))
+            return fail(HEOM_E_TABLE, "ado_minus[%lld] = %d out of range", (long long)q, m);
+        if (t > 0 && m == HEOM_INVALID_UID)
+            return fail(HEOM_E_TABLE, "ado_minus[%lld] missing for a non-zero tuple entry", (long long)q);
+    }
+    return 0;
+}
+
+// internal order: lexicographic rank of the tuple when the tuples form the
+// complete hierarchy, else the reference order
+void build_order(heom_handle* h)
+{
+    const int W = h->W, D = h->D;
+    const int64_t nodes = h->nodes;
+    h->int_of_ref.assign(nodes, 0);
+    h->ref_of_int.assign(nodes, 0);
+    bool lex = h->opt.ado_order == HEOM_ORDER_LEX;
+    if (lex) {
+        std::vector<std::vector<int64_t>> binom(W + D + 2, std::vector<int64_t>(W + 2, 0));
+        for (int a = 0; a < W + D + 2; ++a) {
+            binom[a][0] = 1;
+            for (int b = 1; b <= std::min(a, W + 1); ++b)
+                binom[a][b] = binom[a - 1][b - 1] + (b <= a - 1 ? binom[a - 1][b] : 0);
+        }
+        if (binom[W + D][W] != nodes) lex = false;
+        std::vector<char> seen(lex ? nodes : 0, 0);
+        for (int64_t r = 0; lex && r < nodes; ++r) {
+            int64_t rank = 0;
+            int prefix = 0;
+            for (int k = 0; k < W; ++k) {
+                const int t = h->tuples[r * W + k];
+                for (int x = 0; x < t; ++x) rank += simplex_count(W - 1 - k, D - prefix - x, binom);
+                prefix += t;
+            }
+            if (prefix > D || rank < 0 || rank >= nodes || seen[rank]) {
+                lex = false;
+                break;
+            }
+            seen[rank] = 1;
+            h->int_of_ref[r] = rank;
+        }
+    }
+    if (!lex)
+        for (int64_t r = 0; r < nodes; ++r) h->int_of_ref[r] = r;
+    for (int64_t r = 0; r < nodes; ++r) h->ref_of_int[h->int_of_ref[r]] = r;
+    h->top_int = h->int_of_ref[0];
+}
+
+int to_internal(heom_handle* h, double2* dst, const double* host)
+{
+    const size_t bytes = h->state_elems() * sizeof(double2);
+    CUDA_TRY(cudaMemcpyAsync(h->xfer.p, host, bytes, cudaMemcpyHostToDevice, h->stream));
+    const int64_t total = (int64_t)h->state_elems();
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, h->sm_count * 16));
+    heomk::heom_permute_tiles<<<blocks, 256, 0, h->stream>>>(dst, h->xfer.p, h->d_ref_of_int.p, h->nodes,
+                                                              h->N * h->N, 1);
+    h->launches++;
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int from_internal(heom_handle* h, double* host, const double2* src)
+{
+    const size_t bytes = h->state_elems() * sizeof(double2);
+    const int64_t total = (int64_t)h->state_elems();
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, h->sm_count * 16));
+    heomk::heom_permute_tiles<<<blocks, 256, 0, h->stream>>>(h->xfer.p, src, h->d_ref_of_int.p, h->nodes,
+                                                              h->N * h->N, 0);
+    h->launches++;
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(host, h->xfer.p, bytes, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+} // namespace
+
+extern "C" {
+
+const char* heom_last_error(void) { return g_last_error.c_str(); }
+
+void heom_default_options(heom_options* opt)
+{
+    if (!opt) return;
+    opt->device = 0;
+    opt->ado_order = HEOM_ORDER_LEX;
+    opt->rk4_scheme = HEOM_RK4_PRODUCT;
+    opt->use_graphs = 1;
+}
+
+int heom_create(const heom_instance_desc* d, const heom_options* opt, heom_handle** out)
+{
+    if (!out) return fail(HEOM_E_ARG, "out is NULL");
+    *out = nullptr;
+    if (int rc = check_desc(d)) return rc;
+    std::unique_ptr<heom_handle> h(new heom_handle());
+    heom_default_options(&h->opt);
+    if (opt) h->opt = *opt;
+    int ndev = 0;
+    CUDA_TRY(cudaGetDeviceCount(&ndev));
+    if (h->opt.device < 0 || h->opt.device >= ndev)
+        return fail(HEOM_E_CUDA, "device %d not available (%d devices)", h->opt.device, ndev);
+    h->device = h->opt.device;
+    CUDA_TRY(cudaSetDevice(h->device));
+    cudaDeviceProp prop;
+    CUDA_TRY(cudaGetDeviceProperties(&prop, h->device));
+    if (prop.major < 10)
+        return fail(HEOM_E_CUDA, "device %d is sm_%d%d; this build targets sm_100a", h->device, prop.major, prop.minor);
+    h->sm_count = prop.multiProcessorCount;
+    CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+
+    h->N = d->states;
+    h->M = d->matsubaras;
+    h->B = d->baths;
+    h->BPS = d->baths_per_state;
+    h->W = d->ado_width;
+    h->D = d->ado_depth;
+    h->nodes = d->matrices;
+    h->first_non_plus = d->first_non_plus_id;
+    h->LS = h->D + 1;
+    h->SL = h->BPS * h->M;
+    const int64_t nw = h->nodes * h->W;
+    h->coupling.assign(d->baths_coupling, d->baths_coupling + h->N * h->BPS);
+    h->tuples.assign(d->ado_tuples, d->ado_tuples + nw);
+    h->plus.assign(d->ado_plus, d->ado_plus + nw);
+    h->minus.assign(d->ado_minus, d->ado_minus + nw);
+    h->ham.assign(d->hamiltonian, d->hamiltonian + 2 * h->N * h->N);
+    h->pss.assign(d->pf_same_sum, d->pf_same_sum + 2 * h->nodes);
+    h->pf_same.assign(d->pf_same, d->pf_same + 2 * h->B);
+    h->pf_circ.assign(d->pf_circ, d->pf_circ + 2 * h->B);
+    h->cbk.assign(d->cbk, d->cbk + 2 * h->B * h->M);
+    h->cbk_sqrt.assign(d->cbk_sqrt, d->cbk_sqrt + h->B * h->M);
+    h->mask.assign(h->nodes, 1);
+    for (int q = 0; q < h->B * h->M; ++q)
+        if (!(std::hypot(h->cbk[2 * q], h->cbk[2 * q + 1]) > 0.0))
+            return fail(HEOM_E_TABLE, "cbk[%d] is zero or not finite", q);
+
+    build_order(h.get());
+    if (int rc = h->d_ref_of_int.alloc(h->nodes)) return rc;
+    CUDA_TRY(cudaMemcpy(h->d_ref_of_int.p, h->ref_of_int.data(), h->nodes * 8, cudaMemcpyHostToDevice));
+    if (int rc = build_neighbours(h.get())) return rc;
+    if (int rc = upload_coefficients(h.get())) return rc;
+    if (int rc = upload_hamiltonian(h.get())) return rc;
+    h->y.owner = h.get();
+    h->y.borrowed = true;
+    if (int rc = h->y.data.alloc(h->state_elems())) return rc;
+    CUDA_TRY(cudaMemset(h->y.data.p, 0, h->state_elems() * sizeof(double2)));
+    if (int rc = h->xfer.alloc(h->state_elems())) return rc;
+    if (int rc = h->d_flag.alloc(1)) return rc;
+    *out = h.release();
+    return 0;
+}
+
+int heom_destroy(heom_handle* h)
+{
+    if (!h) return 0;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
+    cudaStream_t s = h->stream;
+    delete h;
+    if (s) cudaStreamDestroy(s);
+    return 0;
+}
+
+int heom_set_hamiltonian(heom_handle* h, const double* ham)
+{
+    if (!h || !ham) return fail(HEOM_E_ARG, "NULL argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    h->ham.assign(ham, ham + 2 * h->N * h->N);
+    return upload_hamiltonian(h);
+}
+
+int heom_set_mask(heom_handle* h, const uint8_t* mask)
+{
+    if (!h || !mask) return fail(HEOM_E_ARG, "NULL argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    for (int64_t q = 0; q < h->nodes; ++q)
+        if (mask[q] > 2) return fail(HEOM_E_ARG, "mask[%lld] = %d is not a mask value", (long long)q, mask[q]);
+    h->mask.assign(mask, mask + h->nodes);
+    return build_neighbours(h);
+}
+
+size_t heom_buffer_size_byte(const heom_handle* h) { return h ? h->state_elems() * sizeof(double2) : 0; }
+
+int heom_buffer_create(heom_handle* h, heom_buffer** out)
+{
+    if (!h || !out) return fail(HEOM_E_ARG, "NULL argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    std::unique_ptr<heom_buffer> b(new heom_buffer());
+    b->owner = h;
+    if (int rc = b->data.alloc(h->state_elems())) return rc;
+    CUDA_TRY(cudaMemset(b->data.p, 0, h->state_elems() * sizeof(double2)));
+    *out = b.release();
+    return 0;
+}
+
+int heom_buffer_destroy(heom_buffer* b)
+{
+    if (!b) return 0;
+    if (b->borrowed) return fail(HEOM_E_ARG, "cannot destroy a borrowed buffer view");
+    cudaSetDevice(b->owner->device);
+    delete b;
+    return 0;
+}
+
+int heom_buffer_write(heom_handle* h, heom_buffer* b, const double* host)
+{
+    if (!h || !b || !host || b->owner != h) return fail(HEOM_E_ARG, "bad argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    return to_internal(h, b->data.p, host);
+}
+
+int heom_buffer_read(heom_handle* h, const heom_buffer* b, double* host)
+{
+    if (!h || !b || !host || b->owner != h) return fail(HEOM_E_ARG, "bad argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    return from_internal(h, host, b->data.p);
+}
+
+int heom_solve(heom_handle* h, double, double, const heom_buffer* in, heom_buffer* out,
+               double out_coeff, heom_buffer* acc, double acc_coeff, int acc_init, int mode)
+{
+    if (!h || !in || in->owner != h) return fail(HEOM_E_ARG, "bad input buffer");
+    CUDA_TRY(cudaSetDevice(h->device));
+    int rc = 0;
+    switch (mode) {
+    case HEOM_SOLVE_PURE:
+        if (!out || out->owner != h || out == in) return fail(HEOM_E_ARG, "bad output buffer");
+        rc = launch_stage(h, heomk::EPI_PURE, in->data.p, nullptr, out->data.p, nullptr,
+                          make_double2(0.0, 0.0), 0);
+        break;
+    case HEOM_SOLVE_ACCUMULATE:
+        if (!out || out->owner != h || out == in || !acc || acc->owner != h || acc == in || acc == out)
+            return fail(HEOM_E_ARG, "bad output/accumulation buffer");
+        rc = launch_stage(h, heomk::EPI_ACC, in->data.p, nullptr, out->data.p, acc->data.p,
+                          make_double2(acc_coeff, 0.0), acc_init ? 1 : 0);
+        break;
+    case HEOM_SOLVE_SUBDIAGONAL:
+        if (!acc || acc->owner != h || acc == in) return fail(HEOM_E_ARG, "bad accumulation buffer");
+        rc = launch_stage(h, heomk::EPI_AXPY_SELF, in->data.p, nullptr, acc->data.p, nullptr,
+                          make_double2(out_coeff, 0.0), 0);
+        break;
+    default: return fail(HEOM_E_ARG, "unknown solve mode %d", mode);
+    }
+    if (rc) return rc;
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int heom_weighted_add(heom_handle* h, int n, double step, heom_buffer* out, const heom_buffer* y,
+                      const double* coeffs, const heom_buffer* const* k)
+{
+    if (!h || !out || !y || n < 0 || n > 7 || (n > 0 && (!coeffs || !k)))
+        return fail(HEOM_E_ARG, "bad argument");
+    const double2* kp[7];
+    for (int l = 0; l < n; ++l) {
+        if (!k[l] || k[l]->owner != h) return fail(HEOM_E_ARG, "bad k buffer");
+        kp[l] = k[l]->data.p;
+    }
+    CUDA_TRY(cudaSetDevice(h->device));
+    if (int rc = launch_wadd(h, n, step, out->data.p, y->data.p, coeffs, kp)) return rc;
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int heom_set_state(heom_handle* h, const double* host)
+{
+    if (!h || !host) return fail(HEOM_E_ARG, "NULL argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    return to_internal(h, h->y.data.p, host);
+}
+
+int heom_get_state(heom_handle* h, double* host)
+{
+    if (!h || !host) return fail(HEOM_E_ARG, "NULL argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    return from_internal(h, host, h->y.data.p);
+}
+
+int heom_set_top(heom_handle* h, const double* top)
+{
+    if (!h || !top) return fail(HEOM_E_ARG, "NULL argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    const size_t nn = (size_t)h->N * h->N;
+    CUDA_TRY(cudaMemcpyAsync(h->y.data.p + h->top_int * nn, top, nn * 16, cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int heom_get_top(heom_handle* h, double* top)
+{
+    if (!h || !top) return fail(HEOM_E_ARG, "NULL argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    const size_t nn = (size_t)h->N * h->N;
+    CUDA_TRY(cudaMemcpyAsync(top, h->y.data.p + h->top_int * nn, nn * 16, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int heom_state_buffer(heom_handle* h, heom_buffer** view)
+{
+    if (!h || !view) return fail(HEOM_E_ARG, "NULL argument");
+    *view = &h->y;
+    return 0;
+}
+
+int heom_rk4_steps_async(heom_handle* h, double dt, int64_t steps)
+{
+    if (!h || steps < 0 || !(dt > 0.0)) return fail(HEOM_E_ARG, "bad argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    return run_steps(h, dt, steps);
+}
+
+int heom_synchronize(heom_handle* h)
+{
+    if (!h) return fail(HEOM_E_ARG, "NULL handle");
+    CUDA_TRY(cudaSetDevice(h->device));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int heom_rk4_steps(heom_handle* h, double dt, int64_t steps)
+{
+    if (int rc = heom_rk4_steps_async(h, dt, steps)) return rc;
+    return heom_synchronize(h);
+}
+
+int heom_propagate(heom_handle* h, double dt, int64_t steps, int64_t observe_every, double* host_tops)
+{
+    if (!h || !host_tops || steps < 0 || observe_every <= 0 || steps % observe_every != 0 || !(dt > 0.0))
+        return fail(HEOM_E_ARG, "bad argument (steps must be a multiple of observe_every)");
+    CUDA_TRY(cudaSetDevice(h->device));
+    const int64_t rows = steps / observe_every + 1;
+    const int nn = h->N * h->N;
+    if ((int64_t)h->toplog.n < rows * nn)
+        if (int rc = h->toplog.alloc(rows * nn)) return rc;
+    heomk::heom_record_top<<<1, 256, 0, h->stream>>>(h->toplog.p, h->y.data.p, h->top_int, nn, 0);
+    h->launches++;
+    CUDA_TRY(cudaGetLastError());
+    for (int64_t r = 1; r < rows; ++r) {
+        if (int rc = run_steps(h, dt, observe_every)) return rc;
+        heomk::heom_record_top<<<1, 256, 0, h->stream>>>(h->toplog.p, h->y.data.p, h->top_int, nn, r);
+        h->launches++;
+        CUDA_TRY(cudaGetLastError());
+    }
+    CUDA_TRY(cudaMemcpyAsync(host_tops, h->toplog.p, rows * nn * 16, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    // failure detection: a non-finite state is reported instead of returned silently
+    CUDA_TRY(cudaMemsetAsync(h->d_flag.p, 0, sizeof(int), h->stream));
+    heomk::heom_check_finite<<<h->sm_count * 4, 256, 0, h->stream>>>(
+        reinterpret_cast<const double*>(h->y.data.p), (int64_t)h->state_elems() * 2, h->d_flag.p);
+    h->launches++;
+    int flag = 0;
+    CUDA_TRY(cudaMemcpyAsync(&flag, h->d_flag.p, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (flag) return fail(HEOM_E_NONFINITE, "non-finite value in the hierarchy state after propagation");
+    return 0;
+}
+
+void* heom_stream(heom_handle* h) { return h ? (void*)h->stream : nullptr; }
+int64_t heom_matrices(const heom_handle* h) { return h ? h->nodes : 0; }
+int32_t heom_states(const heom_handle* h) { return h ? h->N : 0; }
+int64_t heom_kernel_launches(const heom_handle* h) { return h ? h->launches : 0; }
+
+} // extern "C"

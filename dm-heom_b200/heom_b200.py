@@ -1,0 +1,407 @@
+"""ctypes binding of the C ABI in include/heom_b200.h.
+
+Used by the parity tests, the gradient-check harness and bench.py.  It loads
+lib/libheom_b200.so from this directory and fails loudly when it is missing:
+there is no CPU fallback.
+
+The host-side arrays follow the reference layouts
+(dm-heom/include/heom/instance.hpp:202-214): a hierarchy state is a float64
+vector of length matrices * states * states * 2 (interleaved re/im, row-major
+ADO tiles in uid order).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libheom_b200.so")
+
+ORDER_LEX, ORDER_REFERENCE = 0, 1
+RK4_REFERENCE, RK4_HORNER, RK4_PRODUCT = 0, 1, 2
+SOLVE_PURE, SOLVE_ACCUMULATE, SOLVE_SUBDIAGONAL = 0, 1, 2
+SCHEMES = {"reference": RK4_REFERENCE, "horner": RK4_HORNER, "product": RK4_PRODUCT}
+ORDERS = {"lex": ORDER_LEX, "reference": ORDER_REFERENCE}
+
+# every symbol declared in include/heom_b200.h
+EXPORTS = [
+    "heom_last_error", "heom_default_options", "heom_create", "heom_destroy",
+    "heom_set_hamiltonian", "heom_set_mask", "heom_buffer_create", "heom_buffer_destroy",
+    "heom_buffer_write", "heom_buffer_read", "heom_buffer_size_byte", "heom_solve",
+    "heom_weighted_add", "heom_set_state", "heom_get_state", "heom_set_top", "heom_get_top",
+    "heom_state_buffer", "heom_rk4_steps", "heom_propagate", "heom_rk4_steps_async",
+    "heom_synchronize", "heom_stream", "heom_matrices", "heom_states", "heom_kernel_launches",
+    "heom_tables_build", "heom_tables_view", "heom_tables_free", "heom_create_from_system",
+    "heom_config_load", "heom_config_free", "heom_config_system", "heom_config_rho_init",
+    "heom_config_get", "heom_tables_mask",
+]
+
+
+class HeomError(RuntimeError):
+    pass
+
+
+class InstanceDesc(C.Structure):
+    _fields_ = [("states", C.c_int32), ("matsubaras", C.c_int32), ("baths", C.c_int32),
+                ("baths_per_state", C.c_int32), ("ado_width", C.c_int32), ("ado_depth", C.c_int32),
+                ("matrices", C.c_int64), ("first_non_plus_id", C.c_int32),
+                ("baths_coupling", C.c_void_p), ("hamiltonian", C.c_void_p),
+                ("ado_tuples", C.c_void_p), ("ado_plus", C.c_void_p), ("ado_minus", C.c_void_p),
+                ("pf_same_sum", C.c_void_p), ("pf_same", C.c_void_p), ("pf_circ", C.c_void_p),
+                ("cbk", C.c_void_p), ("cbk_sqrt", C.c_void_p)]
+
+
+class SystemDesc(C.Structure):
+    _fields_ = [("sites", C.c_int32), ("ado_depth", C.c_int32), ("hamiltonian", C.c_void_p),
+                ("baths", C.c_int32), ("baths_max_per_site", C.c_int32),
+                ("baths_coupling", C.c_void_p), ("lambda_", C.c_void_p), ("invnu", C.c_void_p),
+                ("omega", C.c_void_p), ("matsubaras", C.c_int32), ("temperature", C.c_double)]
+
+
+class Options(C.Structure):
+    _fields_ = [("device", C.c_int32), ("ado_order", C.c_int32), ("rk4_scheme", C.c_int32),
+                ("use_graphs", C.c_int32)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise HeomError(f"CUDA library not built: {LIB_PATH}")
+        L = C.CDLL(LIB_PATH)
+        vp, i32, i64, dbl = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+        L.heom_last_error.restype = C.c_char_p
+        L.heom_default_options.argtypes = [C.POINTER(Options)]
+        L.heom_create.argtypes = [C.POINTER(InstanceDesc), C.POINTER(Options), C.POINTER(vp)]
+        for name in ["heom_destroy", "heom_synchronize"]:
+            getattr(L, name).argtypes = [vp]
+        L.heom_set_hamiltonian.argtypes = [vp, vp]
+        L.heom_set_mask.argtypes = [vp, vp]
+        L.heom_buffer_create.argtypes = [vp, C.POINTER(vp)]
+        L.heom_buffer_destroy.argtypes = [vp]
+        L.heom_buffer_write.argtypes = [vp, vp, vp]
+        L.heom_buffer_read.argtypes = [vp, vp, vp]
+        L.heom_buffer_size_byte.restype = C.c_size_t
+        L.heom_buffer_size_byte.argtypes = [vp]
+        L.heom_solve.argtypes = [vp, dbl, dbl, vp, vp, dbl, vp, dbl, C.c_int, C.c_int]
+        L.heom_weighted_add.argtypes = [vp, C.c_int, dbl, vp, vp, vp, vp]
+        for name in ["heom_set_state", "heom_get_state", "heom_set_top", "heom_get_top"]:
+            getattr(L, name).argtypes = [vp, vp]
+        L.heom_state_buffer.argtypes = [vp, C.POINTER(vp)]
+        L.heom_rk4_steps.argtypes = [vp, dbl, i64]
+        L.heom_rk4_steps_async.argtypes = [vp, dbl, i64]
+        L.heom_propagate.argtypes = [vp, dbl, i64, i64, vp]
+        L.heom_stream.restype = vp
+        L.heom_stream.argtypes = [vp]
+        L.heom_matrices.restype = i64
+        L.heom_matrices.argtypes = [vp]
+        L.heom_states.restype = i32
+        L.heom_states.argtypes = [vp]
+        L.heom_kernel_launches.restype = i64
+        L.heom_kernel_launches.argtypes = [vp]
+        L.heom_tables_build.argtypes = [C.POINTER(SystemDesc), C.POINTER(vp)]
+        L.heom_tables_view.argtypes = [vp, C.POINTER(InstanceDesc)]
+        L.heom_tables_free.argtypes = [vp]
+        L.heom_tables_free.restype = None
+        L.heom_tables_mask.argtypes = [vp, C.c_char_p, i64, vp]
+        L.heom_create_from_system.argtypes = [C.POINTER(SystemDesc), C.POINTER(Options), C.POINTER(vp)]
+        L.heom_config_load.argtypes = [C.c_char_p, C.POINTER(vp)]
+        L.heom_config_free.argtypes = [vp]
+        L.heom_config_free.restype = None
+        L.heom_config_system.argtypes = [vp, C.POINTER(SystemDesc)]
+        L.heom_config_rho_init.argtypes = [vp, vp]
+        L.heom_config_get.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_size_t]
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != 0:
+        msg = lib().heom_last_error().decode(errors="replace")
+        raise HeomError(f"heom error {rc}: {msg}")
+
+
+def _ptr(a):
+    return a.ctypes.data
+
+
+class Buffer:
+    def __init__(self, owner: "Heom"):
+        self.owner = owner
+        self.h = C.c_void_p()
+        _check(lib().heom_buffer_create(owner.h, C.byref(self.h)))
+
+    def write(self, y):
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        assert y.size == self.owner.state_len
+        _check(lib().heom_buffer_write(self.owner.h, self.h, _ptr(y)))
+
+    def read(self):
+        y = np.empty(self.owner.state_len)
+        _check(lib().heom_buffer_read(self.owner.h, self.h, _ptr(y)))
+        return y
+
+    def close(self):
+        if self.h:
+            lib().heom_buffer_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Heom:
+    """One hierarchy instance on one GPU (a heom_handle)."""
+
+    def __init__(self, *, states, matsubaras, baths, baths_per_state, ado_width, ado_depth,
+                 matrices, first_non_plus_id, baths_coupling, hamiltonian, ado_tuples, ado_plus,
+                 ado_minus, pf_same_sum, pf_same, pf_circ, cbk, cbk_sqrt, device=0,
+                 order="lex", scheme="product", graphs=True):
+        keep = {}
+
+        def arr(name, a, dt):
+            a = np.ascontiguousarray(np.asarray(a, dtype=dt).reshape(-1))
+            keep[name] = a
+            return a.ctypes.data
+
+        d = InstanceDesc(states, matsubaras, baths, baths_per_state, ado_width, ado_depth, matrices,
+                         first_non_plus_id,
+                         arr("c", baths_coupling, np.int32), arr("h", hamiltonian, np.float64),
+                         arr("t", ado_tuples, np.int32), arr("p", ado_plus, np.int32),
+                         arr("m", ado_minus, np.int32), arr("pss", pf_same_sum, np.float64),
+                         arr("pfs", pf_same, np.float64), arr("pfc", pf_circ, np.float64),
+                         arr("cbk", cbk, np.float64), arr("cbs", cbk_sqrt, np.float64))
+        o = Options()
+        lib().heom_default_options(C.byref(o))
+        o.device = device
+        o.ado_order = ORDERS[order] if isinstance(order, str) else order
+        o.rk4_scheme = SCHEMES[scheme] if isinstance(scheme, str) else scheme
+        o.use_graphs = 1 if graphs else 0
+        self.h = C.c_void_p()
+        _check(lib().heom_create(C.byref(d), C.byref(o), C.byref(self.h)))
+        self.states = states
+        self.matrices = matrices
+        self.state_len = matrices * states * states * 2
+
+    @classmethod
+    def from_problem(cls, prob, **kw):
+        """Build from an oracle Problem (tables in reference layout)."""
+        s = prob.system
+        g = prob.graph
+        return cls(states=s.states, matsubaras=s.matsubaras, baths=s.baths,
+                   baths_per_state=s.coupling.shape[1], ado_width=g.width, ado_depth=g.depth,
+                   matrices=g.nodes, first_non_plus_id=g.first_non_plus,
+                   baths_coupling=prob.coupling_flat, hamiltonian=prob.hamiltonian,
+                   ado_tuples=g.tuples, ado_plus=g.plus, ado_minus=g.minus,
+                   pf_same_sum=prob.pf_same_sum, pf_same=prob.pf_same, pf_circ=prob.pf_circ,
+                   cbk=prob.cbk, cbk_sqrt=prob.cbk_sqrt, **kw)
+
+    def close(self):
+        if self.h:
+            lib().heom_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # -- state ---------------------------------------------------------------
+    def set_state(self, y):
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        assert y.size == self.state_len
+        _check(lib().heom_set_state(self.h, _ptr(y)))
+
+    def get_state(self):
+        y = np.empty(self.state_len)
+        _check(lib().heom_get_state(self.h, _ptr(y)))
+        return y
+
+    def set_top(self, top):
+        top = np.ascontiguousarray(top, dtype=np.float64)
+        _check(lib().heom_set_top(self.h, _ptr(top)))
+
+    def get_top(self):
+        t = np.empty(self.states * self.states * 2)
+        _check(lib().heom_get_top(self.h, _ptr(t)))
+        return t
+
+    def set_hamiltonian(self, ham):
+        ham = np.ascontiguousarray(ham, dtype=np.float64)
+        _check(lib().heom_set_hamiltonian(self.h, _ptr(ham)))
+
+    def set_mask(self, mask):
+        mask = np.ascontiguousarray(mask, dtype=np.uint8)
+        _check(lib().heom_set_mask(self.h, _ptr(mask)))
+
+    # -- stepping ------------------------------------------------------------
+    def rk4_steps(self, dt, steps):
+        _check(lib().heom_rk4_steps(self.h, dt, steps))
+
+    def rk4_steps_async(self, dt, steps):
+        _check(lib().heom_rk4_steps_async(self.h, dt, steps))
+
+    def synchronize(self):
+        _check(lib().heom_synchronize(self.h))
+
+    def propagate(self, dt, steps, observe_every):
+        rows = steps // observe_every + 1
+        tops = np.empty(rows * self.states * self.states * 2)
+        _check(lib().heom_propagate(self.h, dt, steps, observe_every, _ptr(tops)))
+        return tops.reshape(rows, self.states * self.states * 2)
+
+    def populations_from_tops(self, tops):
+        n = self.states
+        return tops[:, [(n + 1) * 2 * i for i in range(n)]]
+
+    def stream(self):
+        return lib().heom_stream(self.h)
+
+    def kernel_launches(self):
+        return lib().heom_kernel_launches(self.h)
+
+    # -- reference solve() interface -------------------------------------------
+    def buffer(self):
+        return Buffer(self)
+
+    def solve(self, inb: Buffer, out: Buffer | None, mode=SOLVE_PURE, out_coeff=1.0,
+              acc: Buffer | None = None, acc_coeff=1.0, acc_init=False, time=0.0, step_size=0.0):
+        _check(lib().heom_solve(self.h, time, step_size, inb.h, out.h if out else None, out_coeff,
+                                acc.h if acc else None, acc_coeff, int(acc_init), mode))
+
+    def weighted_add(self, step, out: Buffer, y: Buffer, coeffs, ks):
+        c = np.ascontiguousarray(np.asarray(coeffs, np.float64))
+        kp = (C.c_void_p * max(1, len(ks)))(*[k.h.value for k in ks])
+        _check(lib().heom_weighted_add(self.h, len(ks), step, out.h, y.h, _ptr(c), kp))
+
+
+# --------------------------------------------------------------------------
+# host set-up (graph, tables, config)
+# --------------------------------------------------------------------------
+
+class System:
+    """A system in the reference's config units (cm^-1, fs, K)."""
+
+    def __init__(self, hamiltonian, lambda_, invnu, omega, matsubaras, temperature, depth,
+                 coupling=None):
+        h = np.asarray(hamiltonian, dtype=np.complex128)
+        self.sites = h.shape[0]
+        self.depth = int(depth)
+        self.h = np.empty(self.sites * self.sites * 2)
+        self.h[0::2] = h.reshape(-1).real
+        self.h[1::2] = h.reshape(-1).imag
+        self.lambda_ = np.ascontiguousarray(np.asarray(lambda_, np.float64))
+        self.invnu = np.ascontiguousarray(np.asarray(invnu, np.float64))
+        self.omega = np.ascontiguousarray(np.asarray(omega, np.float64))
+        self.baths = self.lambda_.size
+        if coupling is None:
+            coupling = np.arange(self.sites, dtype=np.int32).reshape(self.sites, 1)
+        self.coupling = np.ascontiguousarray(np.asarray(coupling, np.int32))
+        self.matsubaras = int(matsubaras)
+        self.temperature = float(temperature)
+
+    def desc(self):
+        return SystemDesc(self.sites, self.depth, self.h.ctypes.data, self.baths,
+                          self.coupling.shape[1], self.coupling.ctypes.data,
+                          self.lambda_.ctypes.data, self.invnu.ctypes.data, self.omega.ctypes.data,
+                          self.matsubaras, self.temperature)
+
+
+def build_tables(system: System) -> dict:
+    """Host tables built by the library (reference layouts), copied to numpy."""
+    t = C.c_void_p()
+    d = system.desc()
+    _check(lib().heom_tables_build(C.byref(d), C.byref(t)))
+    try:
+        v = InstanceDesc()
+        _check(lib().heom_tables_view(t, C.byref(v)))
+        n, w, b, m, s = v.matrices, v.ado_width, v.baths, v.matsubaras, v.states
+
+        def get(ptr, count, ct, dt):
+            return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ct)), shape=(count,)).astype(dt).copy()
+
+        out = dict(states=s, matsubaras=m, baths=b, baths_per_state=v.baths_per_state,
+                   ado_width=w, ado_depth=v.ado_depth, matrices=n,
+                   first_non_plus_id=v.first_non_plus_id,
+                   baths_coupling=get(v.baths_coupling, s * v.baths_per_state, C.c_int32, np.int32),
+                   hamiltonian=get(v.hamiltonian, s * s * 2, C.c_double, np.float64),
+                   ado_tuples=get(v.ado_tuples, n * w, C.c_int32, np.int32),
+                   ado_plus=get(v.ado_plus, n * w, C.c_int32, np.int32),
+                   ado_minus=get(v.ado_minus, n * w, C.c_int32, np.int32),
+                   pf_same_sum=get(v.pf_same_sum, n * 2, C.c_double, np.float64),
+                   pf_same=get(v.pf_same, b * 2, C.c_double, np.float64),
+                   pf_circ=get(v.pf_circ, b * 2, C.c_double, np.float64),
+                   cbk=get(v.cbk, b * m * 2, C.c_double, np.float64),
+                   cbk_sqrt=get(v.cbk_sqrt, b * m, C.c_double, np.float64))
+        return out
+    finally:
+        lib().heom_tables_free(t)
+
+
+def tables_mask(system: System, strategy="none", first_layer=-1):
+    t = C.c_void_p()
+    d = system.desc()
+    _check(lib().heom_tables_build(C.byref(d), C.byref(t)))
+    try:
+        v = InstanceDesc()
+        _check(lib().heom_tables_view(t, C.byref(v)))
+        mask = np.zeros(v.matrices, np.uint8)
+        _check(lib().heom_tables_mask(t, strategy.encode(), first_layer, mask.ctypes.data))
+        return mask
+    finally:
+        lib().heom_tables_free(t)
+
+
+def from_system(system: System, **kw) -> Heom:
+    """Build the tables with the library's host code and create a handle."""
+    return Heom(**build_tables(system), **kw)
+
+
+class Config:
+    """A parsed population_dynamics .cfg file (heom_config_*)."""
+
+    def __init__(self, path):
+        self.h = C.c_void_p()
+        _check(lib().heom_config_load(str(path).encode(), C.byref(self.h)))
+
+    def get(self, key):
+        buf = C.create_string_buffer(1 << 16)
+        _check(lib().heom_config_get(self.h, key.encode(), buf, len(buf)))
+        return buf.value.decode()
+
+    def system_desc(self):
+        d = SystemDesc()
+        _check(lib().heom_config_system(self.h, C.byref(d)))
+        return d
+
+    def rho_init(self):
+        d = self.system_desc()
+        out = np.zeros(d.sites * d.sites * 2)
+        _check(lib().heom_config_rho_init(self.h, out.ctypes.data))
+        return out
+
+    def close(self):
+        if self.h:
+            lib().heom_config_free(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,235 @@
+/*
+ * heom_b200.h -- C ABI of the B200 HEOM propagator.
+ *
+ * Drop-in boundary for the reference's OpenCL derivative + RK4 path
+ * (noma/dm-heom).  The entry points replace, one for one:
+ *
+ *   heom_create / heom_destroy       heom::ode ctor + ode::initialise(), which
+ *                                    uploads H, tuples, plus, minus, pf_* and
+ *                                    cbk tables (dm-heom/src/heom/ode.cpp:23-95)
+ *   heom_set_hamiltonian             ode::update_hamiltonian (ode.cpp:198-204) /
+ *                                    solver_base::update_hamiltonian
+ *                                    (solver_base.hpp:272-277)
+ *   heom_set_mask                    ode::set_hierarchy_mask (ode.cpp:206-211) /
+ *                                    solver_base::update_hierarchy_mask
+ *                                    (solver_base.hpp:289-296)
+ *   heom_buffer_create / _destroy    ocl_helper::create_buffer of a hierarchy
+ *                                    buffer (population_dynamics_solver.hpp:140-141)
+ *   heom_buffer_write / _read        enqueueWriteBuffer / enqueueReadBuffer of a
+ *                                    hierarchy buffer (population_dynamics_solver.hpp:162-166,
+ *                                    solver_base.hpp:199-222)
+ *   heom_solve                       the four ode::solve overloads (ode.cpp:97-195):
+ *                                    one heom_ode kernel launch in the write modes
+ *                                    pure / NOMA_NUM_ODE_ACCUMULATE /
+ *                                    NOMA_NUM_ODE_SUBDIAGONAL (heom_ode.cl:416-434)
+ *   heom_weighted_add                rk_weighted_add kernel (rk_weighted_add.cl:19-106)
+ *   heom_set_state / heom_get_state  population_dynamics_solver::reset (:159-172) /
+ *                                    solver_base::update_instance (:225-228)
+ *   heom_set_top / heom_get_top      solver_base::update_hierarchy_top (:279-286) /
+ *                                    solver_base::hierarchy_top (:219-222)
+ *   heom_rk4_steps                   population_dynamics_solver::step_forward
+ *                                    (:233-265) driving the absent noma/num RK4
+ *                                    stepper (rk_rk4)
+ *   heom_propagate                   the observe loop of
+ *                                    app_population_dynamics.cpp:88-106 with the top
+ *                                    matrix recorded on the device at every observation
+ *
+ * Conventions
+ *   - Every call returns 0 on success or a negative HEOM_E_* code;
+ *     heom_last_error() gives a message for the calling thread's last failure.
+ *   - Host arrays use the reference layouts (dm-heom/include/heom/instance.hpp:202-214):
+ *     a hierarchy state is [matrices][states][states] complex doubles stored as
+ *     interleaved (re, im), ADOs in the reference's uid order; tuples, plus and
+ *     minus are int32 [matrices][ado_width]; hierarchy_graph::invalid_uid (-2)
+ *     marks absent neighbours.
+ *   - Device hierarchy buffers (heom_buffer) are opaque: they hold the state in
+ *     the library's own HBM layout (ADOs reordered for neighbour locality).
+ *   - A handle owns one CUDA stream; calls on one handle are not thread-safe.
+ *     All calls are blocking with respect to the host (like the reference's
+ *     CL_TRUE transfers) except where documented.
+ *   - Only the CUDA path exists: there is no CPU fallback.  Without a usable
+ *     sm_100 device heom_create fails with HEOM_E_CUDA.
+ */
+#ifndef HEOM_B200_H
+#define HEOM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HEOM_OK 0
+#define HEOM_E_ARG (-1)       /* invalid argument (null pointer, size, range) */
+#define HEOM_E_CUDA (-2)      /* CUDA runtime error or no usable device */
+#define HEOM_E_NOMEM (-3)     /* device or host allocation failed */
+#define HEOM_E_TABLE (-4)     /* inconsistent hierarchy tables rejected at admission */
+#define HEOM_E_UNSUPPORTED (-5) /* size or mode outside what this build supports */
+#define HEOM_E_NONFINITE (-6) /* a non-finite value was detected in the state */
+#define HEOM_E_CONFIG (-7)    /* configuration file error */
+
+#define HEOM_INVALID_UID (-2)
+
+/* Hierarchy instance in the reference's host layouts: the arguments 7-17 of
+ * the heom_ode kernel (heom_ode.cl:24-45) plus the compile-time defines the
+ * reference generates (solver_base.hpp:179-195). */
+typedef struct heom_instance_desc {
+    int32_t states;            /* NUM_STATES */
+    int32_t matsubaras;        /* NUM_MATSUBARAS */
+    int32_t baths;             /* number of baths (rows of pf_same / pf_circ) */
+    int32_t baths_per_state;   /* BATHS_MAX_PER_STATE */
+    int32_t ado_width;         /* ADO_WIDTH = baths * matsubaras */
+    int32_t ado_depth;         /* hierarchy depth */
+    int64_t matrices;          /* NUM_MATRICES (hierarchy nodes) */
+    int32_t first_non_plus_id; /* first uid of the last layer */
+    const int32_t* baths_coupling; /* [states * baths_per_state], < 0 = none */
+    const double* hamiltonian;     /* [states*states*2] J */
+    const int32_t* ado_tuples;     /* [matrices * ado_width] */
+    const int32_t* ado_plus;       /* [matrices * ado_width] */
+    const int32_t* ado_minus;      /* [matrices * ado_width] */
+    const double* pf_same_sum;     /* [matrices * 2] */
+    const double* pf_same;         /* [baths * 2] */
+    const double* pf_circ;         /* [baths * 2] */
+    const double* cbk;             /* [baths * matsubaras * 2] */
+    const double* cbk_sqrt;        /* [baths * matsubaras] */
+} heom_instance_desc;
+
+/* Order of ADOs in device memory. */
+#define HEOM_ORDER_LEX 0       /* lexicographic order of the ADO tuples (default) */
+#define HEOM_ORDER_REFERENCE 1 /* the reference's uid order */
+
+/* RK4 evaluation schemes for heom_rk4_steps / heom_propagate.  All are the
+ * classical 4-stage RK4 (a = 1/2, 1/2, 1; b = 1/6, 1/3, 1/3, 1/6) for the
+ * linear, time-independent HEOM operator L; they differ in the order of
+ * floating-point operations and in HBM traffic per step:
+ *   REFERENCE: four pure derivative evaluations + rk_weighted_add, as the
+ *              reference runs them (23 state passes per step)
+ *   HORNER:    y + hL(y + h/2 L(y + h/3 L(y + h/4 L y)))       (11 passes)
+ *   PRODUCT:   prod_k (I - hL/r_k) y over the four complex roots r_k of
+ *              1 + z + z^2/2 + z^3/6 + z^4/24                     (8 passes) */
+#define HEOM_RK4_REFERENCE 0
+#define HEOM_RK4_HORNER 1
+#define HEOM_RK4_PRODUCT 2
+
+typedef struct heom_options {
+    int32_t device;      /* CUDA device ordinal */
+    int32_t ado_order;   /* HEOM_ORDER_* */
+    int32_t rk4_scheme;  /* HEOM_RK4_* */
+    int32_t use_graphs;  /* capture the per-step launch sequence in a CUDA graph */
+} heom_options;
+
+/* heom_solve write modes (heom_ode.cl:416-434). */
+#define HEOM_SOLVE_PURE 0        /* out = L(in) */
+#define HEOM_SOLVE_ACCUMULATE 1  /* out = L(in); acc = (acc_init ? in : acc) + acc_coeff L(in) */
+#define HEOM_SOLVE_SUBDIAGONAL 2 /* acc = in + out_coeff L(in) */
+
+typedef struct heom_handle heom_handle;
+typedef struct heom_buffer heom_buffer;
+
+const char* heom_last_error(void);
+void heom_default_options(heom_options* opt);
+
+int heom_create(const heom_instance_desc* desc, const heom_options* opt, heom_handle** out);
+int heom_destroy(heom_handle* h);
+
+int heom_set_hamiltonian(heom_handle* h, const double* hamiltonian);
+int heom_set_mask(heom_handle* h, const uint8_t* mask);
+
+int heom_buffer_create(heom_handle* h, heom_buffer** out);
+int heom_buffer_destroy(heom_buffer* b);
+int heom_buffer_write(heom_handle* h, heom_buffer* b, const double* host_state);
+int heom_buffer_read(heom_handle* h, const heom_buffer* b, double* host_state);
+size_t heom_buffer_size_byte(const heom_handle* h);
+
+/* One derivative evaluation with the reference's solve() semantics.  time and
+ * step_size are accepted for interface parity (the path has no time-dependent
+ * terms).  out or acc may be NULL where the mode does not write them. */
+int heom_solve(heom_handle* h, double time, double step_size, const heom_buffer* in,
+               heom_buffer* out, double out_coeff, heom_buffer* acc, double acc_coeff,
+               int acc_init, int mode);
+/* out = y + step_size * sum_l coeffs[l] * k[l] (0 <= n <= 7), terms with a zero
+ * coefficient skipped, in rk_weighted_add's operation order. */
+int heom_weighted_add(heom_handle* h, int n, double step_size, heom_buffer* out,
+                      const heom_buffer* y, const double* coeffs, const heom_buffer* const* k);
+
+/* The handle's own propagation state y_n. */
+int heom_set_state(heom_handle* h, const double* host_state);
+int heom_get_state(heom_handle* h, double* host_state);
+int heom_set_top(heom_handle* h, const double* host_top);
+int heom_get_top(heom_handle* h, double* host_top);
+int heom_state_buffer(heom_handle* h, heom_buffer** view); /* borrowed view of y_n */
+
+/* Advance y_n by steps RK4 steps of size dt. */
+int heom_rk4_steps(heom_handle* h, double dt, int64_t steps);
+/* Advance y_n by steps RK4 steps, recording the top matrix (states*states
+ * complex, interleaved) at t = 0 and after every observe_every steps into
+ * host_tops (rows = steps / observe_every + 1).  steps must be a multiple of
+ * observe_every.  Tops are gathered on the device and copied back once. */
+int heom_propagate(heom_handle* h, double dt, int64_t steps, int64_t observe_every,
+                   double* host_tops);
+/* Non-blocking variant of heom_rk4_steps: enqueues the work on the handle's
+ * stream and returns; heom_synchronize waits for it. */
+int heom_rk4_steps_async(heom_handle* h, double dt, int64_t steps);
+int heom_synchronize(heom_handle* h);
+/* The handle's CUDA stream (a cudaStream_t), for event timing by callers. */
+void* heom_stream(heom_handle* h);
+
+/* Instance facts. */
+int64_t heom_matrices(const heom_handle* h);
+int32_t heom_states(const heom_handle* h);
+/* Number of kernel launches this handle has issued (for launch accounting). */
+int64_t heom_kernel_launches(const heom_handle* h);
+
+/* ------------------------------------------------------------------------
+ * Host set-up: the reference's hierarchy_graph + instance construction
+ * (dm-heom/src/heom/hierarchy_graph.cpp:30-181, instance.cpp:25-71,155-273)
+ * and config parsing (config.cpp:20-191, population_dynamics_config.cpp).
+ * ------------------------------------------------------------------------ */
+
+/* A system in the reference's config units (config.cpp:37-67): energies in
+ * cm^-1, bath correlation times invnu in fs, Omega in cm^-1; sites map to
+ * states one to one (sites_to_states identity mode).  Converted to SI as in
+ * config::post_process (config.cpp:182-191). */
+typedef struct heom_system_desc {
+    int32_t sites;
+    int32_t ado_depth;
+    const double* hamiltonian;     /* [sites*sites*2] cm^-1, interleaved re/im */
+    int32_t baths;
+    int32_t baths_max_per_site;
+    const int32_t* baths_coupling; /* [sites * baths_max_per_site], < 0 = none */
+    const double* lambda;          /* [baths] cm^-1 */
+    const double* invnu;           /* [baths] fs */
+    const double* omega;           /* [baths] cm^-1 */
+    int32_t matsubaras;            /* includes the k = 0 term, 1..10 */
+    double temperature;            /* K */
+} heom_system_desc;
+
+typedef struct heom_tables heom_tables;
+/* Build the hierarchy graph and the bath tables of a system on the host. */
+int heom_tables_build(const heom_system_desc* sys, heom_tables** out);
+/* Borrowed view of the tables (valid until heom_tables_free). */
+int heom_tables_view(const heom_tables* t, heom_instance_desc* view);
+void heom_tables_free(heom_tables* t);
+/* heom_tables_build + heom_create. */
+int heom_create_from_system(const heom_system_desc* sys, const heom_options* opt, heom_handle** out);
+
+typedef struct heom_config heom_config;
+/* Parse and validate a population_dynamics .cfg file. */
+int heom_config_load(const char* path, heom_config** out);
+void heom_config_free(heom_config* c);
+/* Borrowed view of the [system]/[baths] values in config units. */
+int heom_config_system(const heom_config* c, heom_system_desc* view);
+/* population_dynamics.rho_init as sites*sites*2 interleaved doubles. */
+int heom_config_rho_init(const heom_config* c, double* out);
+/* Raw text of "section.key" copied into buf (NUL-terminated). */
+int heom_config_get(const heom_config* c, const char* key, char* buf, size_t len);
+/* Mask of a filtering strategy ("none" or "single_excitation",
+ * hierarchy_mask.cpp:20-110) for the hierarchy of the tables, written to
+ * mask[matrices]. */
+int heom_tables_mask(const heom_tables* t, const char* strategy, int64_t first_layer, uint8_t* mask);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

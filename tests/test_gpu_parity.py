@@ -1,0 +1,209 @@
+"""GPU parity: the CUDA path (through the C ABI) against the oracle.
+
+Tolerances (floating point; the CUDA kernels contract products into FMAs and
+combine the per-neighbour coefficients on the host, so results differ from
+the reference's operation order by rounding only):
+  * one derivative evaluation: max |gpu - ref| <= 1e-13 * max |ref|
+  * propagated populations:   max |gpu - ref| <= 1e-10 (relative to the
+    total population 1)
+"""
+import numpy as np
+import pytest
+
+import heom_b200 as hb
+import heom_oracle as ho
+import make_golden as mg
+
+pytestmark = pytest.mark.gpu
+
+DERIV_TOL = 1e-13
+POP_TOL = 1e-10
+
+
+def rel_err(a, b):
+    return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
+def derivative_gpu(prob, y, mask=None, **kw):
+    with hb.Heom.from_problem(prob, **kw) as H:
+        if mask is not None:
+            H.set_mask(mask)
+        bi, bo = H.buffer(), H.buffer()
+        bi.write(y)
+        H.solve(bi, bo, hb.SOLVE_PURE)
+        out = bo.read()
+        bi.close(), bo.close()
+    return out
+
+
+def complex_problem():
+    return ho.build_problem(mg.complex_system())
+
+
+CASES = {
+    "cfg1_real_m1": lambda: ho.build_problem(ho.drude_system(7, 4, 1, seed=11)),
+    "cfg2_small_m2": lambda: ho.build_problem(ho.drude_system(8, 3, 2, seed=22)),
+    "complex_m2": complex_problem,
+    "shared_baths": lambda: ho.build_problem(mg.shared_system()),
+    "n12_m1": lambda: ho.build_problem(ho.drude_system(12, 2, 1, seed=5)),
+    "n1": lambda: ho.build_problem(ho.drude_system(1, 5, 2, seed=6)),
+    "n16_m1": lambda: ho.build_problem(ho.drude_system(16, 1, 1, seed=7)),
+    "m3_t77": lambda: ho.build_problem(ho.make_system(ho.synthetic_hamiltonian(4, 9), [35] * 4,
+                                                      [50] * 4, [0] * 4, 3, 77.0, 3)),
+}
+
+
+@pytest.mark.parametrize("order", ["lex", "reference"])
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_derivative_matches_oracle(case, order):
+    prob = CASES[case]()
+    y = np.random.default_rng(1).normal(size=prob.state_len)
+    out = derivative_gpu(prob, y, order=order)
+    ref = ho.derivative(prob, y)
+    assert rel_err(out, ref) <= DERIV_TOL
+
+
+def test_derivative_modes_match_reference_kernels(golden):
+    """pure / ACCUMULATE / SUBDIAGONAL against outputs of heom_ode.cl itself."""
+    prob = complex_problem()
+    y = golden["d_complex_y"]
+    acc0 = golden["d_complex_acc0"]
+    with hb.Heom.from_problem(prob) as H:
+        bi, bo, ba = H.buffer(), H.buffer(), H.buffer()
+        bi.write(y)
+        H.solve(bi, bo, hb.SOLVE_PURE)
+        assert rel_err(bo.read(), golden["d_complex_pure"]) <= DERIV_TOL
+        ba.write(acc0)
+        H.solve(bi, bo, hb.SOLVE_ACCUMULATE, acc=ba, acc_coeff=0.25, acc_init=False)
+        assert rel_err(bo.read(), golden["d_complex_acc_out"]) <= DERIV_TOL
+        assert rel_err(ba.read(), golden["d_complex_acc_acc"]) <= DERIV_TOL
+        ba.write(acc0)
+        H.solve(bi, bo, hb.SOLVE_ACCUMULATE, acc=ba, acc_coeff=0.5, acc_init=True)
+        assert rel_err(ba.read(), golden["d_complex_accinit_acc"]) <= DERIV_TOL
+        ba.write(acc0)
+        H.solve(bi, None, hb.SOLVE_SUBDIAGONAL, out_coeff=0.5e-15, acc=ba)
+        assert rel_err(ba.read(), golden["d_complex_subdiag_acc"]) <= DERIV_TOL
+        for b in (bi, bo, ba):
+            b.close()
+
+
+def test_masked_and_shared_match_reference_kernels(golden):
+    prob = complex_problem()
+    out = derivative_gpu(prob, golden["d_masked_y"], mask=golden["d_masked_mask"])
+    assert rel_err(out, golden["d_masked_pure"]) <= DERIV_TOL
+    ps = ho.build_problem(mg.shared_system())
+    out = derivative_gpu(ps, golden["d_shared_y"])
+    assert rel_err(out, golden["d_shared_pure"]) <= DERIV_TOL
+
+
+def test_weighted_add_matches_reference_order():
+    prob = ho.build_problem(ho.drude_system(5, 2, 1, seed=3))
+    rng = np.random.default_rng(4)
+    y = rng.normal(size=prob.state_len)
+    ks = [rng.normal(size=prob.state_len) for _ in range(4)]
+    c = [1.0 / 6, 0.0, 1.0 / 3, 1.0 / 6]
+    with hb.Heom.from_problem(prob) as H:
+        bufs = [H.buffer() for _ in range(6)]
+        bufs[0].write(y)
+        for b, k in zip(bufs[1:5], ks):
+            b.write(k)
+        H.weighted_add(1e-15, bufs[5], bufs[0], c, bufs[1:5])
+        out = bufs[5].read()
+        for b in bufs:
+            b.close()
+    # rk_weighted_add.cl order: acc = sum c_l k_l (zero c skipped), acc *= h, acc += y
+    acc = np.zeros_like(y)
+    for cl, k in zip(c, ks):
+        if cl != 0.0:
+            acc = acc + cl * k
+    ref = acc * 1e-15 + y
+    assert np.array_equal(out, ref)
+
+
+@pytest.mark.parametrize("scheme", ["product", "horner", "reference"])
+def test_cfg1_populations_match_reference_run(golden, scheme):
+    """7 sites, depth 4, RK4 dt = 1 fs, 1000 steps vs the reference kernels' run."""
+    prob = ho.build_problem(ho.drude_system(7, 4, 1, seed=11))
+    with hb.Heom.from_problem(prob, scheme=scheme) as H:
+        H.set_state(prob.initial_state())
+        tops = H.propagate(1.0e-15, 1000, 1)
+        pops = H.populations_from_tops(tops)
+        final = H.get_state()
+    err = np.max(np.abs(pops - golden["cfg1_pops"]))
+    assert err <= POP_TOL, err
+    assert rel_err(final, golden["cfg1_final"]) <= 1e-9
+
+
+@pytest.mark.parametrize("scheme", ["product", "horner", "reference"])
+def test_cfg2_shape_reduced_depth(scheme):
+    """8 sites, 16 modes (M=2), depth 4, dt = 0.5 fs, 200 steps vs the oracle."""
+    prob = ho.build_problem(ho.drude_system(8, 4, 2, seed=22))
+    _, ref = ho.propagate(prob, 0.5e-15, 200, 10)
+    with hb.Heom.from_problem(prob, scheme=scheme) as H:
+        H.set_state(prob.initial_state())
+        pops = H.populations_from_tops(H.propagate(0.5e-15, 200, 10))
+    assert np.max(np.abs(pops - ref)) <= POP_TOL
+
+
+def test_complex_hamiltonian_masked_propagation(golden):
+    prob = ho.build_problem(mg.complex_system(), mask=golden["d_masked_mask"])
+    _, ref = ho.propagate(prob, 1e-15, 100, 10)
+    with hb.Heom.from_problem(prob) as H:
+        H.set_mask(golden["d_masked_mask"])
+        H.set_state(prob.initial_state())
+        pops = H.populations_from_tops(H.propagate(1e-15, 100, 10))
+    assert np.max(np.abs(pops - ref)) <= POP_TOL
+
+
+def test_state_roundtrip_and_top():
+    prob = ho.build_problem(ho.drude_system(6, 3, 2, seed=2))
+    y = np.random.default_rng(3).normal(size=prob.state_len)
+    with hb.Heom.from_problem(prob) as H:
+        H.set_state(y)
+        assert np.array_equal(H.get_state(), y)
+        assert np.array_equal(H.get_top(), y[: 6 * 6 * 2])
+        top = np.arange(72, dtype=np.float64)
+        H.set_top(top)
+        y2 = y.copy()
+        y2[:72] = top
+        assert np.array_equal(H.get_state(), y2)
+
+
+def test_set_hamiltonian_switches_variant():
+    prob = complex_problem()
+    y = np.random.default_rng(8).normal(size=prob.state_len)
+    real_prob = ho.build_problem(ho.make_system(ho.synthetic_hamiltonian(4, 404), [35.0, 40.0, 30.0, 45.0],
+                                                [50.0, 60.0, 40.0, 55.0], [0.0] * 4, 2, 300.0, 3))
+    with hb.Heom.from_problem(real_prob) as H:
+        bi, bo = H.buffer(), H.buffer()
+        bi.write(y)
+        H.solve(bi, bo)
+        assert rel_err(bo.read(), ho.derivative(real_prob, y)) <= DERIV_TOL
+        H.set_hamiltonian(prob.hamiltonian)
+        H.solve(bi, bo)
+        assert rel_err(bo.read(), ho.derivative(prob, y)) <= DERIV_TOL
+        bi.close(), bo.close()
+
+
+def test_library_built_tables_drive_the_gpu():
+    """heom_create_from_system path (tables from the library's own host code)."""
+    h = ho.synthetic_hamiltonian(7, 11)
+    with hb.from_system(hb.System(h, [35.0] * 7, [50.0] * 7, [0.0] * 7, 1, 300.0, 4)) as H:
+        y0 = np.zeros(H.state_len)
+        y0[0] = 1.0
+        H.set_state(y0)
+        pops = H.populations_from_tops(H.propagate(1e-15, 100, 100))
+    prob = ho.build_problem(ho.drude_system(7, 4, 1, seed=11))
+    _, ref = ho.propagate(prob, 1e-15, 100, 100)
+    assert np.max(np.abs(pops - ref)) <= POP_TOL
+
+
+def test_nonfinite_state_is_reported():
+    prob = ho.build_problem(ho.drude_system(3, 2, 1, seed=1))
+    y = np.zeros(prob.state_len)
+    y[5] = np.nan
+    with hb.Heom.from_problem(prob) as H:
+        H.set_state(y)
+        with pytest.raises(hb.HeomError) as e:
+            H.propagate(1e-15, 2, 1)
+        assert "heom error -6" in str(e.value)

@@ -1,0 +1,166 @@
+"""CPU: host set-up code of the library (graph, tables, config, masks) and
+the C ABI library itself (exports, admission checks that need no GPU)."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import heom_b200 as hb
+import heom_oracle as ho
+
+from conftest import gpu_available
+
+FMO_CFG = """[program]
+task=population_dynamics
+observations={(matrix_complete, m.dat), (matrix_diagonal, d.dat), (matrix_trace_id, t.dat)}
+observe_steps=5
+
+[filtering]
+strategy=none
+first_layer=-1
+
+[solver]
+stepper_type=rk_rk4
+step_size=1.0e-15
+steps=20
+track_flows=false
+flow_filename=
+
+[system]
+sites=3
+hamiltonian={{12410.0, -87.7, 5.5}, {-87.7, 12530.0, 30.8}, {5.5, 30.8, 12210.0}}
+ado_depth=3
+
+[baths]
+number=3
+max_per_site=1
+coupling={{0}, {1}, {2}}
+lambda={35, 35, 35}
+invnu={50, 50, 50}
+Omega={0, 0, 0}
+matsubaras=2
+temperature=77 # K
+
+[population_dynamics]
+rho_init={{1.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}}
+"""
+
+
+def header_functions(root):
+    src = open(os.path.join(root, "include", "heom_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(heom_\w+)\s*\(", src)))
+
+
+def test_library_exports_every_header_symbol(root):
+    names = header_functions(root)
+    assert sorted(hb.EXPORTS) == names
+    L = C.CDLL(hb.LIB_PATH)
+    for n in names:
+        assert hasattr(L, n), n
+
+
+@pytest.mark.parametrize("n,d,m,seed", [(7, 4, 1, 11), (8, 3, 2, 22), (5, 3, 3, 5), (2, 6, 1, 1)])
+def test_tables_identical_to_oracle(n, d, m, seed):
+    h = ho.synthetic_hamiltonian(n, seed)
+    prob = ho.build_problem(ho.make_system(h, [35.0] * n, [50.0] * n, [0.0] * n, m, 300.0, d))
+    t = hb.build_tables(hb.System(h, [35.0] * n, [50.0] * n, [0.0] * n, m, 300.0, d))
+    g = prob.graph
+    assert t["matrices"] == g.nodes and t["first_non_plus_id"] == g.first_non_plus
+    for k, v in [("ado_tuples", g.tuples), ("ado_plus", g.plus), ("ado_minus", g.minus),
+                 ("pf_same_sum", prob.pf_same_sum), ("pf_same", prob.pf_same), ("pf_circ", prob.pf_circ),
+                 ("cbk", prob.cbk), ("cbk_sqrt", prob.cbk_sqrt), ("hamiltonian", prob.hamiltonian)]:
+        assert np.array_equal(t[k], np.asarray(v).reshape(-1)), k
+
+
+def test_tables_omega_and_shared_coupling():
+    h = ho.synthetic_hamiltonian(3, 8)
+    cpl = np.array([[0, 1], [1, 2], [2, -1]], np.int32)
+    lam, inv, om = [35, 25, 45], [50, 45, 65], [0.0, 15.0, -15.0]
+    prob = ho.build_problem(ho.make_system(h, lam, inv, om, 2, 280.0, 3, coupling=cpl))
+    t = hb.build_tables(hb.System(h, lam, inv, om, 2, 280.0, 3, coupling=cpl))
+    for k, v in [("pf_same_sum", prob.pf_same_sum), ("pf_same", prob.pf_same), ("pf_circ", prob.pf_circ),
+                 ("cbk", prob.cbk), ("cbk_sqrt", prob.cbk_sqrt)]:
+        assert np.array_equal(t[k], v), k
+
+
+def test_config_parses_reference_style_file(tmp_path):
+    p = tmp_path / "a.cfg"
+    p.write_text(FMO_CFG)
+    c = hb.Config(p)
+    assert c.get("solver.stepper_type") == "rk_rk4"
+    d = c.system_desc()
+    assert d.sites == 3 and d.ado_depth == 3 and d.matsubaras == 2 and d.temperature == 77.0
+    r = c.rho_init()
+    assert r[0] == 1.0 and r[1:].sum() == 0.0
+
+
+@pytest.mark.parametrize("edit,msg", [
+    (("steps=20", "steps=21"), "remainder"),
+    (("strategy=none", "strategy=bogus"), "filtering"),
+    (("first_layer=-1", "first_layer=0"), "first_layer"),
+    (("{-87.7, 12530.0, 30.8}", "{-87.0, 12530.0, 30.8}"), "hermitian"),
+    (("sites=3", "sites=4"), "matrix"),
+    (("task=population_dynamics", "task=linear_absorption"), "program_task"),
+    (("stepper_type=rk_rk4", "stepper_type=rk_euler"), "rk_rk4"),
+    (("lambda={35, 35, 35}", "lambda={35, 35}"), "lambda"),
+    (("invnu={50, 50, 50}", "invnu={50, 0, 50}"), "invnu"),
+    (("coupling={{0}, {1}, {2}}", "coupling={{0}, {1}, {3}}"), "coupling"),
+    (("observe_steps=5", "observe_steps=5\nbogus_key=1"), "unrecognised"),
+    (("matsubaras=2", "matsubaras=11"), "matsubaras"),
+])
+def test_config_rejects_invalid(tmp_path, edit, msg):
+    p = tmp_path / "bad.cfg"
+    p.write_text(FMO_CFG.replace(*edit))
+    with pytest.raises(hb.HeomError) as e:
+        hb.Config(p)
+    assert msg in str(e.value)
+
+
+def test_config_missing_file():
+    with pytest.raises(hb.HeomError):
+        hb.Config("/nonexistent/file.cfg")
+
+
+def test_single_excitation_mask_matches_restatement():
+    import make_golden as mg
+    s = hb.System(ho.synthetic_hamiltonian(4, 1), [35] * 4, [50] * 4, [0] * 4, 2, 300.0, 3)
+    m = hb.tables_mask(s, "single_excitation", 1)
+    g = ho.build_graph(8, 3)
+    assert np.array_equal(m, mg.single_excitation_mask(g, 2, 1))
+    assert (hb.tables_mask(s, "none", -1) == 1).all()
+
+
+def _good_desc():
+    h = ho.synthetic_hamiltonian(3, 2)
+    return hb.build_tables(hb.System(h, [35] * 3, [50] * 3, [0] * 3, 1, 300.0, 2))
+
+
+@pytest.mark.parametrize("field,index,value,code", [
+    ("ado_plus", 0, 999, -4), ("ado_minus", 5, -7, -4), ("ado_tuples", 3, 9, -4),
+    ("baths_coupling", 0, 7, -4)])
+def test_admission_rejects_bad_tables(field, index, value, code):
+    # table admission runs before any CUDA call, so it is testable on the CPU
+    d = _good_desc()
+    d[field] = d[field].copy()
+    d[field][index] = value
+    with pytest.raises(hb.HeomError) as e:
+        hb.Heom(**d)
+    assert f"heom error {code}" in str(e.value)
+
+
+def test_admission_rejects_sizes():
+    d = _good_desc()
+    d["states"] = 17
+    with pytest.raises(hb.HeomError) as e:
+        hb.Heom(**d)
+    assert "heom error -5" in str(e.value)
+
+
+@pytest.mark.skipif(gpu_available(), reason="checks the no-GPU error path")
+def test_create_without_gpu_fails_loudly():
+    with pytest.raises(hb.HeomError) as e:
+        hb.Heom(**_good_desc())
+    assert "heom error -2" in str(e.value)
