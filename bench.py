@@ -60,10 +60,10 @@ def synthetic_h(n, seed):
     return h
 
 
-def workload_config(scheme):
-    return {"workload": "8 sites, 1 Drude-Lorentz bath/site, 1 Matsubara term (16 modes), depth 8, "
-                        "735471 ADOs of 8x8, RK4 dt=0.5 fs",
-            "ados": 735471, "states": N_SITES, "modes": 16, "depth": DEPTH, "dt_fs": 0.5,
+def workload_config(scheme, depth=DEPTH, ados=735471):
+    return {"workload": f"8 sites, 1 Drude-Lorentz bath/site, 1 Matsubara term (16 modes), depth {depth}, "
+                        f"{ados} ADOs of 8x8, RK4 dt=0.5 fs",
+            "ados": ados, "states": N_SITES, "modes": 16, "depth": depth, "dt_fs": 0.5,
             "rk4_scheme": scheme, "l2": "inputs larger than L2 (753 MB state), no flush",
             "seed": SEED}
 
@@ -189,6 +189,28 @@ def run_reference_arm(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def run_e2e(H, y0, args, world, dist, nodes, barrier):
+    """Same metric through the C ABI with host buffers: full state upload from
+    pinned host memory, then heom_propagate with the top matrix copied back."""
+    import torch
+    barrier()
+    e2e_steps = args.steps - args.steps % OBSERVE_EVERY or OBSERVE_EVERY
+    t0 = time.perf_counter()
+    H.set_state(y0.numpy())
+    tops = H.propagate(DT, e2e_steps, OBSERVE_EVERY)
+    e2e_secs = time.perf_counter() - t0
+    if dist is not None:
+        t = torch.tensor([e2e_secs], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_secs = float(t.item())
+    trace = float(np.sum([tops[-1][(N_SITES + 1) * 2 * i] for i in range(N_SITES)]))
+    return {"value": world * nodes * e2e_steps / e2e_secs, "unit": UNIT,
+            "h2d_bytes_per_step": H.state_len * 8 / e2e_steps,
+            "d2h_bytes_per_step": tops.size * 8 / e2e_steps,
+            "note": f"{e2e_steps} steps: full state upload from pinned host memory + top matrix "
+                    f"every {OBSERVE_EVERY} steps copied back; final trace {trace:.15f}"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -197,6 +219,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--scheme", default="product", choices=["product", "horner", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--depth", type=int, default=DEPTH,
+                    help="hierarchy depth (8 = the benchmark workload; smaller for profiling captures)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -218,7 +243,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     h = synthetic_h(N_SITES, SEED)
-    system = hb.System(h, [35.0] * N_SITES, [50.0] * N_SITES, [0.0] * N_SITES, MATSUBARAS, 300.0, DEPTH)
+    system = hb.System(h, [35.0] * N_SITES, [50.0] * N_SITES, [0.0] * N_SITES, MATSUBARAS, 300.0, args.depth)
     H = hb.from_system(system, device=local_rank, scheme=args.scheme)
     nodes = H.matrices
     y0 = torch.zeros(H.state_len, dtype=torch.float64, pin_memory=True)
@@ -258,20 +283,9 @@ def main():
     per_launch_s = secs / launches if args.scheme != "reference" else None
 
     # e2e through the C ABI with host buffers
-    barrier()
-    t0 = time.perf_counter()
-    H.set_state(y0.numpy())
-    tops = H.propagate(DT, args.steps - args.steps % OBSERVE_EVERY or OBSERVE_EVERY, OBSERVE_EVERY)
-    e2e_secs = time.perf_counter() - t0
-    e2e_steps = args.steps - args.steps % OBSERVE_EVERY or OBSERVE_EVERY
-    if dist is not None:
-        t = torch.tensor([e2e_secs], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_secs = float(t.item())
-    e2e_value = world * nodes * e2e_steps / e2e_secs
-    h2d = H.state_len * 8
-    d2h = tops.size * 8
-    trace = float(np.sum([tops[-1][(N_SITES + 1) * 2 * i] for i in range(N_SITES)]))
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(H, y0, args, world, dist, nodes, barrier)
 
     peak, peak_kind = measured_hbm_peak()
     roofline = None
@@ -289,12 +303,9 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded H, Drude-Lorentz baths)",
-                "config": dict(workload_config(args.scheme),
+                "config": dict(workload_config(args.scheme, args.depth, nodes),
                                parallelism=f"replicas{world}" if world > 1 else "single"),
-                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / e2e_steps,
-                        "d2h_bytes_per_step": d2h / e2e_steps,
-                        "note": f"{e2e_steps} steps: full state upload from pinned host memory + "
-                                f"top matrix every {OBSERVE_EVERY} steps copied back; final trace {trace:.15f}"},
+                "e2e": e2e,
                 "gpu_launches": int(launches), "roofline": roofline, "clocks": clk}
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_reference_sample(steps_cap=1)

@@ -1,36 +1,42 @@
 // heom_kernels.cuh -- sm_100a kernels of the HEOM derivative + RK4 path.
 //
-// One launch of heom_stage evaluates the HEOM time derivative L(w) for every
-// ADO of the hierarchy (the reference's heom_ode kernel,
+// heom_pair_stage evaluates the HEOM time derivative L(w) for every ADO of
+// the hierarchy (the reference's heom_ode kernel,
 // dm-heom/cl/heom/heom_ode.cl:24-451) and fuses the Runge-Kutta write of the
-// stage into the same pass (the reference's NOMA_NUM_ODE_ACCUMULATE /
-// NOMA_NUM_ODE_SUBDIAGONAL modes, heom_ode.cl:416-434, generalised to a
+// stage into the same pass (the NOMA_NUM_ODE_ACCUMULATE /
+// NOMA_NUM_ODE_SUBDIAGONAL write modes, heom_ode.cl:416-434, generalised to a
 // complex stage coefficient).
 //
 // Per element (i, j) of ADO u the derivative is
 //   L(w)_u(i,j) = i * sum_k [ w_u(i,k) Hs(k,j) - Hs(i,k) w_u(k,j) ]        (:89-114, Hs = H / hbar)
 //               + (pf_same_sum[u] + gamma0(i,j)) w_u(i,j)                 (:131-168)
-//               + sum over baths b of site i, Matsubara terms m:
+//               + sum over slots e = b*M+m of the baths b of site i:
 //                    i cplus(n) w_{u+e}(i,j) + kappa_i(n) w_{u-e}(i,j)      (:183-221, :280-342)
-//               + sum over baths b of site j, Matsubara terms m:
+//               + sum over slots e of the baths of site j:
 //                   -i cplus(n) w_{u+e}(i,j) + kappa_j(n) w_{u-e}(i,j)      (:223-259, :344-403)
-// where n is the tuple entry of u for slot e = b*M+m,
+// with n the tuple entry of u for slot e and
 //   cplus(n)   = sqrt((n+1) |c_e| / hbar)                                 (:211, :249)
 //   kappa_i(n) = sqrt(n hbar / |c_e|) (i c_e / hbar + [m==0] pf_circ[b])  (:301-337)
 //   kappa_j(n) = sqrt(n hbar / |c_e|) (-i c_e / hbar + [m==0] pf_circ[b]) (:363-398)
-// For i == j the site-i and site-j plus terms cancel exactly and the minus
-// terms combine to kappa_i + kappa_j; both are folded on the host.
+// For a diagonal element the site-i and site-j plus terms cancel exactly and
+// the minus terms combine to kappa_i + kappa_j ("kappa_d"); both are folded
+// on the host.
 //
-// Layout in HBM (state buffers): ADO-major, each ADO an N x N row-major tile of
-// double2 (re, im); ADOs in the handle's internal order.  Per-ADO tables:
-// nbr[u][0..W) = plus neighbours, nbr[u][W..2W) = minus neighbours (internal
-// index, -1 when absent, masked, or gated off as in the reference), tup[u][W]
-// tuple entries, pss[u] = pf_same_sum.
+// HBM layout ("pair layout"): an ADO is P = N(N-1)/2 + ceil(N/2) sectors of
+// 32 B.  Sector p < N(N-1)/2 holds the symmetric pair (w(i,j), w(j,i)), i < j;
+// the remaining sectors hold pairs of diagonal elements (w(2k,2k),
+// w(2k+1,2k+1)) (for odd N the last holds w(N-1,N-1) twice).  The neighbour
+// terms only ever read the "cross" of a neighbour -- row b and column b for a
+// bath b of the element's sites -- and in this layout a cross is N whole
+// sectors; both elements of a sector need the same neighbours.  For N = 8 an
+// ADO is exactly 32 sectors (1 KB): one warp per ADO, one sector per lane.
 //
-// Mapping: one thread per matrix element, G = 256 / N^2 ADOs per CTA
-// iteration, persistent grid-stride loop over ADO groups.  The group's tiles
-// are staged in shared memory for the commutator; neighbour elements are read
-// with read-only loads (L2 keeps the neighbours of nearby ADOs resident).
+// Work mapping: a team of 32*TW threads (TW = ceil(P/32) warps) owns one ADO
+// at a time, thread p of the team owns sector p.  Teams loop over ADOs
+// (grid-stride) with a two-slot shared-memory pipeline: while ADO k is
+// computed, the tile and index row of ADO k+1 arrive by cp.async; one team
+// barrier per ADO.  The tile in shared memory is row-major with a padded row
+// (N+1 elements) for conflict-free row and column reads in the commutator.
 #pragma once
 
 #include <cstdint>
@@ -38,44 +44,116 @@
 
 namespace heomk {
 
-enum Epi : int {
-    EPI_PURE = 0,      // out = L(w)
-    EPI_AXPY_SELF = 1, // out = w + beta L(w)
-    EPI_AXPY_Y = 2,    // out = y + beta L(w)   (out may alias y)
-    EPI_ACC = 3,       // out = L(w); acc = (acc_init ? w : acc) + beta L(w)
-};
+constexpr int kCtaWarps = 8;
 
-struct StageParams {
-    const double2* __restrict__ in;
-    const double2* y;
+__host__ __device__ constexpr int pairs_of(int n) { return n * (n - 1) / 2 + (n + 1) / 2; }
+__host__ __device__ constexpr int team_warps(int n) { return (pairs_of(n) + 31) / 32; }
+
+// element indices (row-major, e = i*N + j) of the two halves of sector p
+__host__ __device__ inline void pair_elements(int n, int p, int* e1, int* e2, int* i_out, int* j_out,
+                                              int* diag)
+{
+    const int noff = n * (n - 1) / 2;
+    if (p < noff) {
+        int i = 0, q = p;
+        while (q >= n - 1 - i) {
+            q -= n - 1 - i;
+            ++i;
+        }
+        const int j = i + 1 + q;
+        *e1 = i * n + j;
+        *e2 = j * n + i;
+        *i_out = i;
+        *j_out = j;
+        *diag = 0;
+    } else {
+        const int k = p - noff;
+        const int a = 2 * k;
+        const int b = (2 * k + 1 < n) ? 2 * k + 1 : a;
+        *e1 = a * n + a;
+        *e2 = b * n + b;
+        *i_out = a;
+        *j_out = b;
+        *diag = 1;
+    }
+}
+
+enum HKind : int { H_REAL_SYM = 0, H_GENERIC = 1 };
+
+struct PairParams {
+    const double2* __restrict__ in;  // [nodes][2P] (sector p = double2 pair 2p, 2p+1)
+    const double2* y;                // AXPY against y instead of in (may alias out)
     double2* out;
-    double2* acc;
+    double2* acc;                    // accumulate mode
+    double2 alpha;                   // out = alpha * x + beta * L
     double2 beta;
+    double2 acc_beta;                // acc = (acc_init ? in : acc) + acc_beta * L
     int acc_init;
-    const int32_t* __restrict__ nbr;   // [nodes][2W]
-    const uint8_t* __restrict__ tup;   // [nodes][W]
-    const double2* __restrict__ pss;   // [nodes]
+    int use_acc;
+    const int32_t* __restrict__ nbr; // [nodes][NW]: plus[W], minus[W], padded to NW (multiple of 4)
+    const uint8_t* __restrict__ tup; // [nodes][TWB] tuple bytes, padded to TWB (multiple of 16)
+    const double2* __restrict__ pss; // [nodes]
     const double* __restrict__ cplus;  // [W][LS]
-    const double2* __restrict__ kmin;  // [3][W][LS]: kappa_i, kappa_j, kappa_i + kappa_j
-    const double2* __restrict__ hs;    // [N*N]
+    const double2* __restrict__ kmin;  // [3][W][LS]: kappa_i, kappa_j, kappa_d
+    const double2* __restrict__ hs;    // [N*N] H / hbar
     const double2* __restrict__ gamma0;// [N*N]
     const int16_t* __restrict__ slots; // [N][SL], -1 padded
     int64_t nodes;
-    int W;
-    int LS;
-    int SL;
+    int W, NW, TWB, LS, SL;
 };
 
-constexpr int kThreads = 256;
+// dynamic shared memory carve-up (bytes); everything 16-B aligned
+struct PairSmem {
+    int lut;     // cplus W*LS doubles + kmin 3*W*LS double2 (+ H for generic)
+    int team;    // per team: 2 slots
+    int slot;    // per slot: tile + nbr + tup + pss
+    int tile_off, nbr_off, tup_off, pss_off;
+};
 
-// dynamic shared memory of heom_stage for G ADOs per iteration
-inline size_t stage_smem_bytes(int G, int W, int LS)
+__host__ __device__ inline PairSmem pair_smem_layout(int n, int W, int NW, int TWB, int LS)
 {
-    return (size_t)G * 16 + (size_t)3 * W * LS * 16 + (size_t)W * LS * 8 + (size_t)G * 2 * W * 4 +
-           (size_t)G * W * 4;
+    PairSmem s;
+    // 3*W*LS double2 (kappa) + N*N double2 (H) + W*LS double (cplus) + N*(N+1) double (real H)
+    const int lut = 3 * W * LS * 16 + n * n * 16 + W * LS * 8 + n * (n + 1) * 8;
+    s.lut = (lut + 15) & ~15;
+    const int tile = n * (n + 1) * 16;
+    s.tile_off = 0;
+    s.nbr_off = tile;
+    s.tup_off = s.nbr_off + ((NW * 4 + 15) & ~15);
+    s.pss_off = s.tup_off + ((TWB + 15) & ~15);
+    s.slot = s.pss_off + 16;
+    s.team = 2 * s.slot;
+    return s;
 }
 
-__device__ __forceinline__ double2 ld_ro(const double2* p) { return __ldg(p); }
+__host__ inline size_t pair_smem_bytes(int n, int W, int NW, int TWB, int LS)
+{
+    const PairSmem s = pair_smem_layout(n, W, NW, TWB, LS);
+    const int teams = kCtaWarps / team_warps(n);
+    return (size_t)s.lut + (size_t)teams * s.team;
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+template <int TW>
+__device__ __forceinline__ void team_sync(int team)
+{
+    if (TW == 1) {
+        __syncwarp();
+    } else {
+        asm volatile("bar.sync %0, %1;\n" ::"r"(team + 1), "r"(TW * 32) : "memory");
+    }
+}
 
 __device__ __forceinline__ void cmac(double2& acc, const double2 a, const double2 b)
 {
@@ -85,155 +163,229 @@ __device__ __forceinline__ void cmac(double2& acc, const double2 a, const double
     acc.y = fma(a.y, b.x, acc.y);
 }
 
-template <int N, bool REAL_H, int EPI>
-__global__ void __launch_bounds__(kThreads, 2) heom_stage(const StageParams p)
+__device__ __forceinline__ double2 ldg2(const double2* p) { return __ldg(p); }
+
+// issue the asynchronous copies of ADO u into a team slot
+template <int N>
+__device__ __forceinline__ void prefetch_ado(unsigned char* slot, const PairParams& p, const PairSmem& L,
+                                             int64_t u, int lt, int tt, int e1, int e2, bool active)
 {
-    constexpr int NN = N * N;
-    constexpr int G = kThreads / NN;
-    __shared__ double2 tile[G * NN];
-    extern __shared__ __align__(16) unsigned char dyn[];
-    // dynamic shared memory (stage_smem_bytes): pss, LUTs, nbr rows, tuple rows
-    const int W = p.W;
-    const int LS = p.LS;
-    double2* s_pss = reinterpret_cast<double2*>(dyn);                 // G
-    double2* s_kmin = s_pss + G;                                      // 3 * W * LS
-    double* s_cplus = reinterpret_cast<double*>(s_kmin + 3 * W * LS); // W * LS
-    int32_t* s_nbr = reinterpret_cast<int32_t*>(s_cplus + W * LS);    // G * 2W
-    int32_t* s_tup = s_nbr + G * 2 * W;                               // G * W
-
-    const int t = threadIdx.x;
-    for (int q = t; q < 3 * W * LS; q += kThreads) s_kmin[q] = p.kmin[q];
-    for (int q = t; q < W * LS; q += kThreads) s_cplus[q] = p.cplus[q];
-
-    const int g = t / NN;
-    const int e = t - g * NN;
-    const bool lane_ok = g < G;
-    const int i = e / N;
-    const int j = e - i * N;
-
-    // Hamiltonian row i and column j (scaled by 1/hbar) kept in registers
-    double2 hrow[N], hcol[N];
-#pragma unroll
-    for (int k = 0; k < N; ++k) {
-        hrow[k] = lane_ok ? p.hs[i * N + k] : make_double2(0.0, 0.0);
-        hcol[k] = lane_ok ? p.hs[k * N + j] : make_double2(0.0, 0.0);
+    double2* tile = reinterpret_cast<double2*>(slot + L.tile_off);
+    if (active) {
+        const double2* src = p.in + u * (2 * pairs_of(N));
+        const int pr = lt; // sector index
+        const int i1 = e1 / N, j1 = e1 - i1 * N, i2 = e2 / N, j2 = e2 - i2 * N;
+        cp_async16(tile + i1 * (N + 1) + j1, src + 2 * pr);
+        cp_async16(tile + i2 * (N + 1) + j2, src + 2 * pr + 1);
     }
-    const double2 g0 = lane_ok ? p.gamma0[e] : make_double2(0.0, 0.0);
-    const int SL = p.SL;
-    const int16_t* slot_i = p.slots + i * SL;
-    const int16_t* slot_j = p.slots + j * SL;
-    const double2* kap_i = s_kmin + (i == j ? 2 : 0) * W * LS;
-    const double2* kap_j = s_kmin + 1 * W * LS;
+    int32_t* nb = reinterpret_cast<int32_t*>(slot + L.nbr_off);
+    for (int q = lt * 4; q < p.NW; q += tt * 4) cp_async16(nb + q, p.nbr + u * p.NW + q);
+    unsigned char* tu = slot + L.tup_off;
+    for (int q = lt * 16; q < p.TWB; q += tt * 16) cp_async16(tu + q, p.tup + u * p.TWB + q);
+    if (lt == 0) cp_async16(slot + L.pss_off, p.pss + u);
+}
+
+template <int N, int HK, int SLT>
+__global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_pair_stage(const PairParams p)
+{
+    constexpr int P = pairs_of(N);
+    constexpr int TW = team_warps(N);
+    constexpr int TT = 32 * TW;
+    constexpr int TEAMS = kCtaWarps / TW;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const PairSmem L = pair_smem_layout(N, p.W, p.NW, p.TWB, p.LS);
+    const int W = p.W, LS = p.LS, SL = p.SL;
+
+    // look-up tables shared by the CTA; 16-byte arrays first (all offsets multiples of 16)
+    double2* s_kmin = reinterpret_cast<double2*>(smem);              // 3 * W * LS
+    double2* s_h = s_kmin + 3 * W * LS;                              // N * N, complex H / hbar
+    double* s_cplus = reinterpret_cast<double*>(s_h + N * N);        // W * LS
+    double* s_hr = s_cplus + W * LS;                                 // N * (N+1), real H / hbar
+    for (int q = threadIdx.x; q < W * LS; q += blockDim.x) s_cplus[q] = p.cplus[q];
+    for (int q = threadIdx.x; q < 3 * W * LS; q += blockDim.x) s_kmin[q] = p.kmin[q];
+    if (HK == H_GENERIC)
+        for (int q = threadIdx.x; q < N * N; q += blockDim.x) s_h[q] = p.hs[q];
+    else
+        for (int q = threadIdx.x; q < N * N; q += blockDim.x) s_hr[(q / N) * (N + 1) + q % N] = p.hs[q].x;
+
+    const int team = threadIdx.x / TT;
+    const int lt = threadIdx.x - team * TT;
+    const bool active = team < TEAMS && lt < P;
+    unsigned char* team_base = smem + L.lut + team * L.team;
+
+    int e1 = 0, e2 = 0, i = 0, j = 0, diag = 0;
+    if (active) pair_elements(N, lt, &e1, &e2, &i, &j, &diag);
+
+    // rows i and j of a real symmetric H (its columns equal its rows)
+    const double* hri = s_hr + i * (N + 1);
+    const double* hrj = s_hr + j * (N + 1);
+    const double2 g1 = active ? p.gamma0[e1] : make_double2(0.0, 0.0);
+    const double2 g2 = active ? p.gamma0[e2] : make_double2(0.0, 0.0);
+    int sli[SLT], slj[SLT];
+#pragma unroll
+    for (int q = 0; q < SLT; ++q) {
+        sli[q] = (active && q < SL) ? p.slots[i * SL + q] : -1;
+        slj[q] = (active && q < SL) ? p.slots[j * SL + q] : -1;
+    }
+    // coefficient tables seen by the two elements of this sector
+    const double2* kap_i1 = s_kmin + (diag ? 2 : 0) * W * LS; // element 1, slots of site i
+    const double2* kap_j1 = s_kmin + 1 * W * LS;              // element 1, slots of site j (off-diagonal)
+    const double2* kap_i2 = s_kmin + 1 * W * LS;              // element 2 = (j,i), slots of site i (its j side)
+    const double2* kap_j2 = s_kmin + (diag ? 2 : 0) * W * LS; // element 2, slots of site j
+
+    __syncthreads();
+    if (team >= TEAMS) return;
 
     const int64_t nodes = p.nodes;
-    const int64_t stride = (int64_t)gridDim.x * G;
-    for (int64_t base = (int64_t)blockIdx.x * G; base < nodes; base += stride) {
-        const int64_t u = base + g;
-        const bool ok = lane_ok && u < nodes;
-        __syncthreads(); // previous iteration finished with the shared buffers
-        double2 s = make_double2(0.0, 0.0);
-        if (ok) s = ld_ro(p.in + u * NN + e);
-        if (lane_ok) tile[g * NN + e] = s;
-        for (int q = t; q < G * 2 * W; q += kThreads) {
-            const int gg = q / (2 * W);
-            const int64_t uu = base + gg;
-            s_nbr[q] = uu < nodes ? __ldg(p.nbr + uu * 2 * W + (q - gg * 2 * W)) : -1;
-        }
-        for (int q = t; q < G * W; q += kThreads) {
-            const int gg = q / W;
-            const int64_t uu = base + gg;
-            s_tup[q] = uu < nodes ? (int32_t)__ldg(p.tup + uu * W + (q - gg * W)) : 0;
-        }
-        if (t < G) s_pss[t] = (base + t < nodes) ? ld_ro(p.pss + base + t) : make_double2(0.0, 0.0);
-        __syncthreads();
-        if (!ok) continue;
+    const int64_t stride = (int64_t)gridDim.x * TEAMS;
+    int64_t u = (int64_t)blockIdx.x * TEAMS + team;
+    int cur = 0;
+    if (u < nodes) prefetch_ado<N>(team_base, p, L, u, lt, TT, e1, e2, active);
+    cp_async_wait_all();
+    team_sync<TW>(team);
 
-        // ---- commutator: i * (w Hs - Hs w) ----
-        const double2* w = tile + g * NN;
-        double cr = 0.0, ci = 0.0;
+    for (; u < nodes; u += stride) {
+        unsigned char* slot = team_base + cur * L.slot;
+        const int64_t un = u + stride;
+        if (un < nodes) prefetch_ado<N>(team_base + (cur ^ 1) * L.slot, p, L, un, lt, TT, e1, e2, active);
+
+        if (active) {
+            const double2* t = reinterpret_cast<const double2*>(slot + L.tile_off);
+            const int32_t* nb = reinterpret_cast<const int32_t*>(slot + L.nbr_off);
+            const unsigned char* tu = slot + L.tup_off;
+            const double2 pss = *reinterpret_cast<const double2*>(slot + L.pss_off);
+            const int i1 = e1 / N, j1 = e1 - i1 * N, i2 = e2 / N, j2 = e2 - i2 * N;
+            const double2 s1 = t[i1 * (N + 1) + j1];
+            const double2 s2 = t[i2 * (N + 1) + j2];
+
+            // ---- commutator i * (w H - H w) / hbar for both elements ----
+            double c1r = 0.0, c1i = 0.0, c2r = 0.0, c2i = 0.0;
 #pragma unroll
-        for (int k = 0; k < N; ++k) {
-            const double2 a = w[i * N + k];
-            const double2 b = w[k * N + j];
-            if (REAL_H) {
-                cr = fma(a.x, hcol[k].x, cr);
-                cr = fma(-hrow[k].x, b.x, cr);
-                ci = fma(a.y, hcol[k].x, ci);
-                ci = fma(-hrow[k].x, b.y, ci);
+            for (int k = 0; k < N; ++k) {
+                const double2 a1 = t[i1 * (N + 1) + k]; // w(i1,k)
+                const double2 b1 = t[k * (N + 1) + j1]; // w(k,j1)
+                const double2 a2 = t[i2 * (N + 1) + k];
+                const double2 b2 = t[k * (N + 1) + j2];
+                if (HK == H_REAL_SYM) {
+                    // element 1 = (i1, j1): H(k,j1) = row j1, H(i1,k) = row i1
+                    // pairs: off-diagonal (i,j),(j,i): i1=i,j1=j,i2=j,j2=i; diagonal: (i,i),(j,j)
+                    const double hk_j1 = diag ? hri[k] : hrj[k];
+                    const double hi1_k = hri[k];
+                    const double hk_j2 = diag ? hrj[k] : hri[k];
+                    const double hi2_k = hrj[k];
+                    c1r = fma(a1.x, hk_j1, c1r);
+                    c1r = fma(-hi1_k, b1.x, c1r);
+                    c1i = fma(a1.y, hk_j1, c1i);
+                    c1i = fma(-hi1_k, b1.y, c1i);
+                    c2r = fma(a2.x, hk_j2, c2r);
+                    c2r = fma(-hi2_k, b2.x, c2r);
+                    c2i = fma(a2.y, hk_j2, c2i);
+                    c2i = fma(-hi2_k, b2.y, c2i);
+                } else {
+                    const double2 hkj1 = s_h[k * N + j1], hi1k = s_h[i1 * N + k];
+                    const double2 hkj2 = s_h[k * N + j2], hi2k = s_h[i2 * N + k];
+                    c1r = fma(a1.x, hkj1.x, c1r);
+                    c1r = fma(-a1.y, hkj1.y, c1r);
+                    c1i = fma(a1.x, hkj1.y, c1i);
+                    c1i = fma(a1.y, hkj1.x, c1i);
+                    c1r = fma(-hi1k.x, b1.x, c1r);
+                    c1r = fma(hi1k.y, b1.y, c1r);
+                    c1i = fma(-hi1k.x, b1.y, c1i);
+                    c1i = fma(-hi1k.y, b1.x, c1i);
+                    c2r = fma(a2.x, hkj2.x, c2r);
+                    c2r = fma(-a2.y, hkj2.y, c2r);
+                    c2i = fma(a2.x, hkj2.y, c2i);
+                    c2i = fma(a2.y, hkj2.x, c2i);
+                    c2r = fma(-hi2k.x, b2.x, c2r);
+                    c2r = fma(hi2k.y, b2.y, c2r);
+                    c2i = fma(-hi2k.x, b2.y, c2i);
+                    c2i = fma(-hi2k.y, b2.x, c2i);
+                }
+            }
+            double2 L1 = make_double2(-c1i, c1r);
+            double2 L2 = make_double2(-c2i, c2r);
+
+            // ---- same term ----
+            cmac(L1, make_double2(pss.x + g1.x, pss.y + g1.y), s1);
+            cmac(L2, make_double2(pss.x + g2.x, pss.y + g2.y), s2);
+
+            // ---- neighbours: per side all loads first, then the updates ----
+            // side 0 = slots of site i, side 1 = slots of site j
+#pragma unroll
+            for (int sd = 0; sd < 2; ++sd) {
+                double2 xp[SLT][2], xm[SLT][2];
+                int ix[SLT];
+#pragma unroll
+                for (int q = 0; q < SLT; ++q) {
+                    const int sl = sd == 0 ? sli[q] : slj[q];
+                    const int32_t vp = (sl >= 0 && !diag) ? nb[sl] : -1;
+                    const int32_t vm = sl >= 0 ? nb[W + sl] : -1;
+                    ix[q] = sl >= 0 ? (sl * LS + tu[sl]) : 0;
+                    xp[q][0] = xp[q][1] = xm[q][0] = xm[q][1] = make_double2(0.0, 0.0);
+                    if (vp >= 0) {
+                        const double2* src = p.in + (int64_t)vp * (2 * P) + 2 * lt;
+                        xp[q][0] = ldg2(src);
+                        xp[q][1] = ldg2(src + 1);
+                    }
+                    if (vm >= 0) {
+                        const double2* src = p.in + (int64_t)vm * (2 * P) + 2 * lt;
+                        xm[q][0] = ldg2(src);
+                        xm[q][1] = ldg2(src + 1);
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < SLT; ++q) {
+                    const int sl = sd == 0 ? sli[q] : slj[q];
+                    if (sl < 0) continue;
+                    const double c = diag ? 0.0 : s_cplus[ix[q]];
+                    if (sd == 0) {
+                        // site i: element 1 (i,j) i-side (+i c, kappa_i); element 2 (j,i) j-side (-i c, kappa_j)
+                        L1.x = fma(-c, xp[q][0].y, L1.x);
+                        L1.y = fma(c, xp[q][0].x, L1.y);
+                        L2.x = fma(c, xp[q][1].y, L2.x);
+                        L2.y = fma(-c, xp[q][1].x, L2.y);
+                        cmac(L1, kap_i1[ix[q]], xm[q][0]);
+                        if (!diag) cmac(L2, kap_i2[ix[q]], xm[q][1]);
+                    } else {
+                        // site j: element 1 j-side (-i c, kappa_j); element 2 i-side (+i c, kappa_i)
+                        L1.x = fma(c, xp[q][0].y, L1.x);
+                        L1.y = fma(-c, xp[q][0].x, L1.y);
+                        L2.x = fma(-c, xp[q][1].y, L2.x);
+                        L2.y = fma(c, xp[q][1].x, L2.y);
+                        if (!diag) cmac(L1, kap_j1[ix[q]], xm[q][0]);
+                        cmac(L2, kap_j2[ix[q]], xm[q][1]);
+                    }
+                }
+            }
+
+            // ---- stage write ----
+            const int64_t off = u * (2 * P) + 2 * lt;
+            double2 x1, x2;
+            if (p.y) {
+                x1 = p.y[off];
+                x2 = p.y[off + 1];
             } else {
-                cr = fma(a.x, hcol[k].x, cr);
-                cr = fma(-a.y, hcol[k].y, cr);
-                ci = fma(a.x, hcol[k].y, ci);
-                ci = fma(a.y, hcol[k].x, ci);
-                cr = fma(-hrow[k].x, b.x, cr);
-                cr = fma(hrow[k].y, b.y, cr);
-                ci = fma(-hrow[k].x, b.y, ci);
-                ci = fma(-hrow[k].y, b.x, ci);
+                x1 = s1;
+                x2 = s2;
+            }
+            double2 r1 = make_double2(p.alpha.x * x1.x - p.alpha.y * x1.y, p.alpha.x * x1.y + p.alpha.y * x1.x);
+            double2 r2 = make_double2(p.alpha.x * x2.x - p.alpha.y * x2.y, p.alpha.x * x2.y + p.alpha.y * x2.x);
+            cmac(r1, p.beta, L1);
+            cmac(r2, p.beta, L2);
+            __stcs(p.out + off, r1);
+            __stcs(p.out + off + 1, r2);
+            if (p.use_acc) {
+                double2 a1 = p.acc_init ? s1 : p.acc[off];
+                double2 a2 = p.acc_init ? s2 : p.acc[off + 1];
+                cmac(a1, p.acc_beta, L1);
+                cmac(a2, p.acc_beta, L2);
+                p.acc[off] = a1;
+                p.acc[off + 1] = a2;
             }
         }
-        double2 L = make_double2(-ci, cr);
-
-        // ---- same term ----
-        const double2 pss = s_pss[g];
-        const double2 gam = make_double2(pss.x + g0.x, pss.y + g0.y);
-        cmac(L, gam, s);
-
-        // ---- plus / minus neighbours ----
-        const int32_t* nb = s_nbr + g * 2 * W;
-        const int32_t* tu = s_tup + g * W;
-        for (int q = 0; q < SL; ++q) {
-            const int sl = slot_i[q];
-            if (sl < 0) break;
-            const int n = tu[sl];
-            if (i != j) {
-                const int32_t v = nb[sl];
-                if (v >= 0) {
-                    const double c = s_cplus[sl * LS + n];
-                    const double2 x = ld_ro(p.in + (int64_t)v * NN + e);
-                    L.x = fma(-c, x.y, L.x);
-                    L.y = fma(c, x.x, L.y);
-                }
-            }
-            const int32_t v = nb[W + sl];
-            if (v >= 0) {
-                const double2 x = ld_ro(p.in + (int64_t)v * NN + e);
-                cmac(L, kap_i[sl * LS + n], x);
-            }
-        }
-        if (i != j) {
-            for (int q = 0; q < SL; ++q) {
-                const int sl = slot_j[q];
-                if (sl < 0) break;
-                const int n = tu[sl];
-                const int32_t vp = nb[sl];
-                if (vp >= 0) {
-                    const double c = s_cplus[sl * LS + n];
-                    const double2 x = ld_ro(p.in + (int64_t)vp * NN + e);
-                    L.x = fma(c, x.y, L.x);
-                    L.y = fma(-c, x.x, L.y);
-                }
-                const int32_t vm = nb[W + sl];
-                if (vm >= 0) {
-                    const double2 x = ld_ro(p.in + (int64_t)vm * NN + e);
-                    cmac(L, kap_j[sl * LS + n], x);
-                }
-            }
-        }
-
-        // ---- stage write ----
-        const int64_t off = u * NN + e;
-        if (EPI == EPI_PURE) {
-            __stcs(p.out + off, L);
-        } else if (EPI == EPI_AXPY_SELF || EPI == EPI_AXPY_Y) {
-            double2 r = (EPI == EPI_AXPY_SELF) ? s : p.y[off];
-            cmac(r, p.beta, L);
-            __stcs(p.out + off, r);
-        } else { // EPI_ACC
-            __stcs(p.out + off, L);
-            double2 a = p.acc_init ? s : p.acc[off];
-            cmac(a, p.beta, L);
-            p.acc[off] = a;
-        }
+        cp_async_wait_all();
+        team_sync<TW>(team);
+        cur ^= 1;
     }
 }
 
@@ -262,29 +414,66 @@ __global__ void heom_weighted_add(const WaddParams p)
     }
 }
 
-// dst[int] = src[ref] for whole N x N tiles (to_internal) or the reverse.
-__global__ void heom_permute_tiles(double2* __restrict__ dst, const double2* __restrict__ src,
-                                   const int64_t* __restrict__ ref_of_int, int64_t nodes, int nn,
-                                   int to_internal)
+// Reference layout (row-major tiles in uid order) <-> pair layout in the
+// internal ADO order.  One thread per (internal ADO, sector).
+__global__ void heom_to_pairs(double2* __restrict__ dst, const double2* __restrict__ src,
+                              const int64_t* __restrict__ ref_of_int, int64_t nodes, int n)
 {
-    const int64_t total = nodes * nn;
+    const int P = pairs_of(n);
+    const int64_t total = nodes * P;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += stride) {
-        const int64_t u = q / nn;
-        const int64_t e = q - u * nn;
-        const int64_t r = ref_of_int[u];
-        if (to_internal)
-            dst[q] = src[r * nn + e];
-        else
-            dst[r * nn + e] = src[q];
+        const int64_t u = q / P;
+        const int pr = (int)(q - u * P);
+        int e1, e2, i, j, d;
+        pair_elements(n, pr, &e1, &e2, &i, &j, &d);
+        const int64_t r = ref_of_int[u] * n * n;
+        dst[2 * q] = src[r + e1];
+        dst[2 * q + 1] = src[r + e2];
     }
 }
 
-// Copy the top matrix (internal index top_int) into log row `row`.
-__global__ void heom_record_top(double2* __restrict__ log, const double2* __restrict__ y,
-                                int64_t top_int, int nn, int64_t row)
+__global__ void heom_from_pairs(double2* __restrict__ dst, const double2* __restrict__ src,
+                                const int64_t* __restrict__ ref_of_int, int64_t nodes, int n)
 {
-    for (int e = threadIdx.x; e < nn; e += blockDim.x) log[row * nn + e] = y[top_int * nn + e];
+    const int P = pairs_of(n);
+    const int64_t total = nodes * P;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += stride) {
+        const int64_t u = q / P;
+        const int pr = (int)(q - u * P);
+        int e1, e2, i, j, d;
+        pair_elements(n, pr, &e1, &e2, &i, &j, &d);
+        const int64_t r = ref_of_int[u] * n * n;
+        dst[r + e1] = src[2 * q];
+        if (e2 != e1) dst[r + e2] = src[2 * q + 1];
+    }
+}
+
+// Copy the top matrix (internal ADO top_int, pair layout) into row `row` of a
+// row-major log; also used for heom_get_top with row 0.
+__global__ void heom_record_top(double2* __restrict__ log, const double2* __restrict__ y,
+                                int64_t top_int, int n, int64_t row)
+{
+    const int P = pairs_of(n);
+    for (int pr = threadIdx.x; pr < P; pr += blockDim.x) {
+        int e1, e2, i, j, d;
+        pair_elements(n, pr, &e1, &e2, &i, &j, &d);
+        log[row * n * n + e1] = y[top_int * 2 * P + 2 * pr];
+        if (e2 != e1) log[row * n * n + e2] = y[top_int * 2 * P + 2 * pr + 1];
+    }
+}
+
+// Write a row-major top matrix into the pair layout of ADO top_int.
+__global__ void heom_write_top(double2* __restrict__ y, const double2* __restrict__ top, int64_t top_int, int n)
+{
+    const int P = pairs_of(n);
+    for (int pr = threadIdx.x; pr < P; pr += blockDim.x) {
+        int e1, e2, i, j, d;
+        pair_elements(n, pr, &e1, &e2, &i, &j, &d);
+        y[top_int * 2 * P + 2 * pr] = top[e1];
+        y[top_int * 2 * P + 2 * pr + 1] = top[e2];
+    }
 }
 
 // Sets *flag when any element is not finite.

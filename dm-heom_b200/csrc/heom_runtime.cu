@@ -19,7 +19,7 @@
 #include "heom_b200.h"
 #include "heom_kernels.cuh"
 
-using heomk::StageParams;
+using heomk::PairParams;
 
 namespace {
 
@@ -85,30 +85,29 @@ struct DevBuf {
     }
 };
 
-typedef void (*stage_fn_t)(const StageParams);
+typedef void (*stage_fn_t)(const PairParams);
 
-template <int N, bool RH>
-stage_fn_t pick_epi(int epi)
+template <int N, int HK>
+stage_fn_t pick_slt(int slt)
 {
-    switch (epi) {
-    case heomk::EPI_PURE: return heomk::heom_stage<N, RH, heomk::EPI_PURE>;
-    case heomk::EPI_AXPY_SELF: return heomk::heom_stage<N, RH, heomk::EPI_AXPY_SELF>;
-    case heomk::EPI_AXPY_Y: return heomk::heom_stage<N, RH, heomk::EPI_AXPY_Y>;
-    default: return heomk::heom_stage<N, RH, heomk::EPI_ACC>;
+    switch (slt) {
+    case 2: return heomk::heom_pair_stage<N, HK, 2>;
+    case 4: return heomk::heom_pair_stage<N, HK, 4>;
+    default: return heomk::heom_pair_stage<N, HK, 8>;
     }
 }
 
 template <int N>
-stage_fn_t pick_n(bool real_h, int epi)
+stage_fn_t pick_n(int hk, int slt)
 {
-    return real_h ? pick_epi<N, true>(epi) : pick_epi<N, false>(epi);
+    return hk == heomk::H_REAL_SYM ? pick_slt<N, heomk::H_REAL_SYM>(slt) : pick_slt<N, heomk::H_GENERIC>(slt);
 }
 
-stage_fn_t pick_stage(int n, bool real_h, int epi)
+stage_fn_t pick_stage(int n, int hk, int slt)
 {
     switch (n) {
 #define HEOM_CASE(K) \
-    case K: return pick_n<K>(real_h, epi);
+    case K: return pick_n<K>(hk, slt);
         HEOM_CASE(1) HEOM_CASE(2) HEOM_CASE(3) HEOM_CASE(4) HEOM_CASE(5) HEOM_CASE(6)
         HEOM_CASE(7) HEOM_CASE(8) HEOM_CASE(9) HEOM_CASE(10) HEOM_CASE(11) HEOM_CASE(12)
         HEOM_CASE(13) HEOM_CASE(14) HEOM_CASE(15) HEOM_CASE(16)
@@ -116,6 +115,14 @@ stage_fn_t pick_stage(int n, bool real_h, int epi)
     default: return nullptr;
     }
 }
+
+// stage write modes (runtime parameters of the one stage kernel)
+enum Epi : int {
+    EPI_PURE = 0,      // out = L(w)
+    EPI_AXPY_SELF = 1, // out = w + beta L(w)
+    EPI_AXPY_Y = 2,    // out = y + beta L(w)   (out may alias y)
+    EPI_ACC = 3,       // out = L(w); acc = (acc_init ? w : acc) + beta L(w)
+};
 
 // number of tuples over d coordinates with sum <= r
 int64_t simplex_count(int d, int r, const std::vector<std::vector<int64_t>>& binom)
@@ -150,8 +157,10 @@ struct heom_handle {
     int N = 0, M = 0, B = 0, BPS = 0, W = 0, D = 0;
     int64_t nodes = 0;
     int32_t first_non_plus = 0;
-    int LS = 0, SL = 0;
-    bool real_h = true;
+    int LS = 0, SL = 0, SLT = 2;
+    int P = 0;          // 32-byte sectors per ADO (pair layout)
+    int NW = 0, TWB = 0; // padded widths of the neighbour and tuple rows
+    int hkind = heomk::H_REAL_SYM;
 
     // host copies in reference layout
     std::vector<int32_t> coupling, tuples, plus, minus;
@@ -173,44 +182,44 @@ struct heom_handle {
     DevBuf<double2> work[5];
     DevBuf<double2> xfer;   // reference-layout staging buffer for host transfers
     DevBuf<double2> toplog;
+    DevBuf<double2> topbuf; // one row-major top matrix
     DevBuf<int> d_flag;
 
     // launch accounting
     int64_t launches = 0;
-    int stage_blocks[4] = {0, 0, 0, 0};
+    int stage_blocks[2] = {0, 0}; // per H kind
 
     // cached graph of one RK4 step
     cudaGraphExec_t step_graph = nullptr;
     double graph_dt = 0.0;
 
-    size_t state_elems() const { return (size_t)nodes * N * N; }
+    size_t state_elems() const { return (size_t)nodes * 2 * P; } // double2 per internal state
+    size_t ref_elems() const { return (size_t)nodes * N * N; }   // double2 per reference-layout state
 };
 
 namespace {
-
-int G_of(int n) { return heomk::kThreads / (n * n); }
 
 int build_neighbours(heom_handle* h)
 {
     // internal neighbour table with the reference's gating folded in:
     //   plus read only when uid < first_non_plus_id (heom_ode.cl:183) and mask[plus] != 0 (:199)
     //   minus read only when tuple > 0 (:293) and mask[minus] != 0 (:297)
-    const int W = h->W;
-    std::vector<int32_t> nbr((size_t)h->nodes * 2 * W);
-    std::vector<uint8_t> tup((size_t)h->nodes * W);
+    const int W = h->W, NW = h->NW, TWB = h->TWB;
+    std::vector<int32_t> nbr((size_t)h->nodes * NW, -1);
+    std::vector<uint8_t> tup((size_t)h->nodes * TWB, 0);
     std::vector<double2> pss(h->nodes);
     for (int64_t u = 0; u < h->nodes; ++u) {
         const int64_t r = h->ref_of_int[u];
         for (int m = 0; m < W; ++m) {
             const int32_t t = h->tuples[r * W + m];
-            tup[u * W + m] = (uint8_t)t;
+            tup[u * TWB + m] = (uint8_t)t;
             int32_t pv = -1, mv = -1;
             const int32_t pr = h->plus[r * W + m];
             if (r < h->first_non_plus && pr >= 0 && h->mask[pr]) pv = (int32_t)h->int_of_ref[pr];
             const int32_t mr = h->minus[r * W + m];
             if (t > 0 && mr >= 0 && h->mask[mr]) mv = (int32_t)h->int_of_ref[mr];
-            nbr[u * 2 * W + m] = pv;
-            nbr[u * 2 * W + W + m] = mv;
+            nbr[u * NW + m] = pv;
+            nbr[u * NW + W + m] = mv;
         }
         pss[u] = make_double2(h->pss[2 * r], h->pss[2 * r + 1]);
     }
@@ -229,11 +238,16 @@ int upload_hamiltonian(heom_handle* h)
 {
     const int N = h->N;
     std::vector<double2> hs(N * N), g0(N * N);
-    h->real_h = true;
+    bool real_sym = true;
     for (int q = 0; q < N * N; ++q) {
         hs[q] = make_double2(h->ham[2 * q] / kHbar, h->ham[2 * q + 1] / kHbar);
-        if (h->ham[2 * q + 1] != 0.0) h->real_h = false;
+        if (h->ham[2 * q + 1] != 0.0) real_sym = false;
     }
+    for (int i = 0; i < N && real_sym; ++i)
+        for (int j = 0; j < i; ++j)
+            if (h->ham[2 * (i * N + j)] != h->ham[2 * (j * N + i)]) real_sym = false;
+    // real symmetric H keeps rows i, j in registers; anything else reads H from shared memory
+    h->hkind = real_sym ? heomk::H_REAL_SYM : heomk::H_GENERIC;
     // same term (heom_ode.cl:138-168): for i != j subtract pf_same of every
     // bath coupled to site i and to site j
     for (int i = 0; i < N; ++i)
@@ -254,8 +268,7 @@ int upload_hamiltonian(heom_handle* h)
     }
     CUDA_TRY(cudaMemcpy(h->d_hs.p, hs.data(), hs.size() * 16, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(h->d_gamma0.p, g0.data(), g0.size() * 16, cudaMemcpyHostToDevice));
-    // the real/complex-H kernel variant may change: re-resolve launch shapes and graphs
-    for (int& b : h->stage_blocks) b = 0;
+    // the kernel variant may change: rebuild the cached step graph
     if (h->step_graph) {
         cudaGraphExecDestroy(h->step_graph);
         h->step_graph = nullptr;
@@ -304,9 +317,9 @@ int upload_coefficients(heom_handle* h)
     return 0;
 }
 
-StageParams base_params(const heom_handle* h)
+PairParams base_params(const heom_handle* h)
 {
-    StageParams p{};
+    PairParams p{};
     p.nbr = h->d_nbr.p;
     p.tup = h->d_tup.p;
     p.pss = h->d_pss.p;
@@ -317,28 +330,30 @@ StageParams base_params(const heom_handle* h)
     p.slots = h->d_slots.p;
     p.nodes = h->nodes;
     p.W = h->W;
+    p.NW = h->NW;
+    p.TWB = h->TWB;
     p.LS = h->LS;
     p.SL = h->SL;
     return p;
 }
 
-// resolve the launch shape of a stage variant (outside of any stream capture)
-int resolve_stage(heom_handle* h, int epi, stage_fn_t* fn_out, size_t* smem_out)
+int cta_threads(int n) { return (heomk::kCtaWarps / heomk::team_warps(n)) * heomk::team_warps(n) * 32; }
+int cta_teams(int n) { return heomk::kCtaWarps / heomk::team_warps(n); }
+
+// resolve the launch shape of the stage kernel (outside of any stream capture)
+int resolve_stage(heom_handle* h, stage_fn_t* fn_out, size_t* smem_out)
 {
-    stage_fn_t fn = pick_stage(h->N, h->real_h, epi);
+    stage_fn_t fn = pick_stage(h->N, h->hkind, h->SLT);
     if (!fn) return fail(HEOM_E_UNSUPPORTED, "states = %d not supported", h->N);
-    const int G = G_of(h->N);
-    const size_t smem = heomk::stage_smem_bytes(G, h->W, h->LS);
-    int& blocks = h->stage_blocks[epi];
+    const size_t smem = heomk::pair_smem_bytes(h->N, h->W, h->NW, h->TWB, h->LS);
+    int& blocks = h->stage_blocks[h->hkind];
     if (blocks == 0) {
-        if (smem > 48 * 1024)
-            CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)smem));
+        if (smem > 227 * 1024) return fail(HEOM_E_UNSUPPORTED, "stage kernel needs %zu B of shared memory", smem);
+        CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;
-        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn,
-                                                               heomk::kThreads, smem));
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn, cta_threads(h->N), smem));
         if (per_sm < 1) return fail(HEOM_E_UNSUPPORTED, "stage kernel cannot be resident");
-        const int64_t groups = (h->nodes + G - 1) / G;
+        const int64_t groups = (h->nodes + cta_teams(h->N) - 1) / cta_teams(h->N);
         blocks = (int)std::min<int64_t>(groups, (int64_t)per_sm * h->sm_count);
     }
     *fn_out = fn;
@@ -351,16 +366,35 @@ int launch_stage(heom_handle* h, int epi, const double2* in, const double2* y, d
 {
     stage_fn_t fn = nullptr;
     size_t smem = 0;
-    if (int rc = resolve_stage(h, epi, &fn, &smem)) return rc;
-    StageParams p = base_params(h);
+    if (int rc = resolve_stage(h, &fn, &smem)) return rc;
+    PairParams p = base_params(h);
     p.in = in;
-    p.y = y;
     p.out = out;
-    p.acc = acc;
-    p.beta = beta;
-    p.acc_init = acc_init;
-    const int blocks = h->stage_blocks[epi];
-    fn<<<blocks, heomk::kThreads, smem, h->stream>>>(p);
+    switch (epi) {
+    case EPI_PURE:
+        p.alpha = make_double2(0.0, 0.0);
+        p.beta = make_double2(1.0, 0.0);
+        break;
+    case EPI_AXPY_SELF:
+        p.alpha = make_double2(1.0, 0.0);
+        p.beta = beta;
+        break;
+    case EPI_AXPY_Y:
+        p.y = y;
+        p.alpha = make_double2(1.0, 0.0);
+        p.beta = beta;
+        break;
+    default: // EPI_ACC
+        p.alpha = make_double2(0.0, 0.0);
+        p.beta = make_double2(1.0, 0.0);
+        p.acc = acc;
+        p.use_acc = 1;
+        p.acc_beta = beta;
+        p.acc_init = acc_init;
+        break;
+    }
+    const int blocks = h->stage_blocks[h->hkind];
+    fn<<<blocks, cta_threads(h->N), smem, h->stream>>>(p);
     h->launches++;
     CUDA_TRY(cudaGetLastError());
     return 0;
@@ -407,7 +441,7 @@ int enqueue_step(heom_handle* h, double dt)
         double2* outs[4] = {a, b, a, y};
         for (int k = 0; k < 4; ++k) {
             const double2 beta = make_double2(dt * kProdBeta[k][0], dt * kProdBeta[k][1]);
-            if (int rc = launch_stage(h, heomk::EPI_AXPY_SELF, ins[k], nullptr, outs[k], nullptr, beta, 0))
+            if (int rc = launch_stage(h, EPI_AXPY_SELF, ins[k], nullptr, outs[k], nullptr, beta, 0))
                 return rc;
         }
         return 0;
@@ -416,10 +450,10 @@ int enqueue_step(heom_handle* h, double dt)
         double2* a = h->work[0].p;
         double2* b = h->work[1].p;
         const double c[4] = {dt / 4.0, dt / 3.0, dt / 2.0, dt};
-        if (int rc = launch_stage(h, heomk::EPI_AXPY_SELF, y, nullptr, a, nullptr, make_double2(c[0], 0.0), 0)) return rc;
-        if (int rc = launch_stage(h, heomk::EPI_AXPY_Y, a, y, b, nullptr, make_double2(c[1], 0.0), 0)) return rc;
-        if (int rc = launch_stage(h, heomk::EPI_AXPY_Y, b, y, a, nullptr, make_double2(c[2], 0.0), 0)) return rc;
-        if (int rc = launch_stage(h, heomk::EPI_AXPY_Y, a, y, y, nullptr, make_double2(c[3], 0.0), 0)) return rc;
+        if (int rc = launch_stage(h, EPI_AXPY_SELF, y, nullptr, a, nullptr, make_double2(c[0], 0.0), 0)) return rc;
+        if (int rc = launch_stage(h, EPI_AXPY_Y, a, y, b, nullptr, make_double2(c[1], 0.0), 0)) return rc;
+        if (int rc = launch_stage(h, EPI_AXPY_Y, b, y, a, nullptr, make_double2(c[2], 0.0), 0)) return rc;
+        if (int rc = launch_stage(h, EPI_AXPY_Y, a, y, y, nullptr, make_double2(c[3], 0.0), 0)) return rc;
         return 0;
     }
     default: { // HEOM_RK4_REFERENCE
@@ -431,13 +465,13 @@ int enqueue_step(heom_handle* h, double dt)
         const double2* ks[4] = {k1, k2, k3, k4};
         const double a2[1] = {0.5}, a3[2] = {0.0, 0.5}, a4[3] = {0.0, 0.0, 1.0};
         const double bb[4] = {1.0 / 6, 1.0 / 3, 1.0 / 3, 1.0 / 6};
-        if (int rc = launch_stage(h, heomk::EPI_PURE, y, nullptr, k1, nullptr, zero, 0)) return rc;
+        if (int rc = launch_stage(h, EPI_PURE, y, nullptr, k1, nullptr, zero, 0)) return rc;
         if (int rc = launch_wadd(h, 1, dt, st, y, a2, ks)) return rc;
-        if (int rc = launch_stage(h, heomk::EPI_PURE, st, nullptr, k2, nullptr, zero, 0)) return rc;
+        if (int rc = launch_stage(h, EPI_PURE, st, nullptr, k2, nullptr, zero, 0)) return rc;
         if (int rc = launch_wadd(h, 2, dt, st, y, a3, ks)) return rc;
-        if (int rc = launch_stage(h, heomk::EPI_PURE, st, nullptr, k3, nullptr, zero, 0)) return rc;
+        if (int rc = launch_stage(h, EPI_PURE, st, nullptr, k3, nullptr, zero, 0)) return rc;
         if (int rc = launch_wadd(h, 3, dt, st, y, a4, ks)) return rc;
-        if (int rc = launch_stage(h, heomk::EPI_PURE, st, nullptr, k4, nullptr, zero, 0)) return rc;
+        if (int rc = launch_stage(h, EPI_PURE, st, nullptr, k4, nullptr, zero, 0)) return rc;
         return launch_wadd(h, 4, dt, y, y, bb, ks);
     }
     }
@@ -473,11 +507,9 @@ int run_steps(heom_handle* h, double dt, int64_t steps)
     }
     if (!h->step_graph) {
         // make sure launch shapes are resolved outside of capture
-        for (int e = 0; e < 4; ++e) {
-            stage_fn_t fn = nullptr;
-            size_t smem = 0;
-            if (int rc = resolve_stage(h, e, &fn, &smem)) return rc;
-        }
+        stage_fn_t fn = nullptr;
+        size_t smem = 0;
+        if (int rc = resolve_stage(h, &fn, &smem)) return rc;
         cudaGraph_t graph = nullptr;
         const int64_t saved = h->launches;
         CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
@@ -576,12 +608,11 @@ void build_order(heom_handle* h)
 
 int to_internal(heom_handle* h, double2* dst, const double* host)
 {
-    const size_t bytes = h->state_elems() * sizeof(double2);
+    const size_t bytes = h->ref_elems() * sizeof(double2);
     CUDA_TRY(cudaMemcpyAsync(h->xfer.p, host, bytes, cudaMemcpyHostToDevice, h->stream));
-    const int64_t total = (int64_t)h->state_elems();
+    const int64_t total = h->nodes * h->P;
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, h->sm_count * 16));
-    heomk::heom_permute_tiles<<<blocks, 256, 0, h->stream>>>(dst, h->xfer.p, h->d_ref_of_int.p, h->nodes,
-                                                              h->N * h->N, 1);
+    heomk::heom_to_pairs<<<blocks, 256, 0, h->stream>>>(dst, h->xfer.p, h->d_ref_of_int.p, h->nodes, h->N);
     h->launches++;
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -590,11 +621,10 @@ int to_internal(heom_handle* h, double2* dst, const double* host)
 
 int from_internal(heom_handle* h, double* host, const double2* src)
 {
-    const size_t bytes = h->state_elems() * sizeof(double2);
-    const int64_t total = (int64_t)h->state_elems();
+    const size_t bytes = h->ref_elems() * sizeof(double2);
+    const int64_t total = h->nodes * h->P;
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, h->sm_count * 16));
-    heomk::heom_permute_tiles<<<blocks, 256, 0, h->stream>>>(h->xfer.p, src, h->d_ref_of_int.p, h->nodes,
-                                                              h->N * h->N, 0);
+    heomk::heom_from_pairs<<<blocks, 256, 0, h->stream>>>(h->xfer.p, src, h->d_ref_of_int.p, h->nodes, h->N);
     h->launches++;
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(host, h->xfer.p, bytes, cudaMemcpyDeviceToHost, h->stream));
@@ -648,6 +678,11 @@ int heom_create(const heom_instance_desc* d, const heom_options* opt, heom_handl
     h->first_non_plus = d->first_non_plus_id;
     h->LS = h->D + 1;
     h->SL = h->BPS * h->M;
+    if (h->SL > 8) return fail(HEOM_E_UNSUPPORTED, "baths_per_state * matsubaras = %d > 8", h->SL);
+    h->SLT = h->SL <= 2 ? 2 : h->SL <= 4 ? 4 : 8;
+    h->P = heomk::pairs_of(h->N);
+    h->NW = (2 * h->W + 3) & ~3;
+    h->TWB = (h->W + 15) & ~15;
     const int64_t nw = h->nodes * h->W;
     h->coupling.assign(d->baths_coupling, d->baths_coupling + h->N * h->BPS);
     h->tuples.assign(d->ado_tuples, d->ado_tuples + nw);
@@ -674,7 +709,8 @@ int heom_create(const heom_instance_desc* d, const heom_options* opt, heom_handl
     h->y.borrowed = true;
     if (int rc = h->y.data.alloc(h->state_elems())) return rc;
     CUDA_TRY(cudaMemset(h->y.data.p, 0, h->state_elems() * sizeof(double2)));
-    if (int rc = h->xfer.alloc(h->state_elems())) return rc;
+    if (int rc = h->xfer.alloc(h->ref_elems())) return rc;
+    if (int rc = h->topbuf.alloc((size_t)h->N * h->N)) return rc;
     if (int rc = h->d_flag.alloc(1)) return rc;
     *out = h.release();
     return 0;
@@ -758,18 +794,18 @@ int heom_solve(heom_handle* h, double, double, const heom_buffer* in, heom_buffe
     switch (mode) {
     case HEOM_SOLVE_PURE:
         if (!out || out->owner != h || out == in) return fail(HEOM_E_ARG, "bad output buffer");
-        rc = launch_stage(h, heomk::EPI_PURE, in->data.p, nullptr, out->data.p, nullptr,
+        rc = launch_stage(h, EPI_PURE, in->data.p, nullptr, out->data.p, nullptr,
                           make_double2(0.0, 0.0), 0);
         break;
     case HEOM_SOLVE_ACCUMULATE:
         if (!out || out->owner != h || out == in || !acc || acc->owner != h || acc == in || acc == out)
             return fail(HEOM_E_ARG, "bad output/accumulation buffer");
-        rc = launch_stage(h, heomk::EPI_ACC, in->data.p, nullptr, out->data.p, acc->data.p,
+        rc = launch_stage(h, EPI_ACC, in->data.p, nullptr, out->data.p, acc->data.p,
                           make_double2(acc_coeff, 0.0), acc_init ? 1 : 0);
         break;
     case HEOM_SOLVE_SUBDIAGONAL:
         if (!acc || acc->owner != h || acc == in) return fail(HEOM_E_ARG, "bad accumulation buffer");
-        rc = launch_stage(h, heomk::EPI_AXPY_SELF, in->data.p, nullptr, acc->data.p, nullptr,
+        rc = launch_stage(h, EPI_AXPY_SELF, in->data.p, nullptr, acc->data.p, nullptr,
                           make_double2(out_coeff, 0.0), 0);
         break;
     default: return fail(HEOM_E_ARG, "unknown solve mode %d", mode);
@@ -814,7 +850,10 @@ int heom_set_top(heom_handle* h, const double* top)
     if (!h || !top) return fail(HEOM_E_ARG, "NULL argument");
     CUDA_TRY(cudaSetDevice(h->device));
     const size_t nn = (size_t)h->N * h->N;
-    CUDA_TRY(cudaMemcpyAsync(h->y.data.p + h->top_int * nn, top, nn * 16, cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(cudaMemcpyAsync(h->topbuf.p, top, nn * 16, cudaMemcpyHostToDevice, h->stream));
+    heomk::heom_write_top<<<1, 128, 0, h->stream>>>(h->y.data.p, h->topbuf.p, h->top_int, h->N);
+    h->launches++;
+    CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     return 0;
 }
@@ -824,7 +863,10 @@ int heom_get_top(heom_handle* h, double* top)
     if (!h || !top) return fail(HEOM_E_ARG, "NULL argument");
     CUDA_TRY(cudaSetDevice(h->device));
     const size_t nn = (size_t)h->N * h->N;
-    CUDA_TRY(cudaMemcpyAsync(top, h->y.data.p + h->top_int * nn, nn * 16, cudaMemcpyDeviceToHost, h->stream));
+    heomk::heom_record_top<<<1, 128, 0, h->stream>>>(h->topbuf.p, h->y.data.p, h->top_int, h->N, 0);
+    h->launches++;
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(top, h->topbuf.p, nn * 16, cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     return 0;
 }
@@ -866,12 +908,12 @@ int heom_propagate(heom_handle* h, double dt, int64_t steps, int64_t observe_eve
     const int nn = h->N * h->N;
     if ((int64_t)h->toplog.n < rows * nn)
         if (int rc = h->toplog.alloc(rows * nn)) return rc;
-    heomk::heom_record_top<<<1, 256, 0, h->stream>>>(h->toplog.p, h->y.data.p, h->top_int, nn, 0);
+    heomk::heom_record_top<<<1, 128, 0, h->stream>>>(h->toplog.p, h->y.data.p, h->top_int, h->N, 0);
     h->launches++;
     CUDA_TRY(cudaGetLastError());
     for (int64_t r = 1; r < rows; ++r) {
         if (int rc = run_steps(h, dt, observe_every)) return rc;
-        heomk::heom_record_top<<<1, 256, 0, h->stream>>>(h->toplog.p, h->y.data.p, h->top_int, nn, r);
+        heomk::heom_record_top<<<1, 128, 0, h->stream>>>(h->toplog.p, h->y.data.p, h->top_int, h->N, r);
         h->launches++;
         CUDA_TRY(cudaGetLastError());
     }
