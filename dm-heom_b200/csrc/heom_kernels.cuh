@@ -389,6 +389,325 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_pair_stage(const PairP
     }
 }
 
+// ---------------------------------------------------------------------------
+// N <= 8: one warp per ADO, commutator on the FP64 tensor pipe.
+//
+// The tile is zero-padded to 8 x 8.  For k-slice s in {0, 1} lane l = 4r + t
+// needs the MMA operands A = w(r, 4s+t) (for w H) and B = w(4s+t, r) (for
+// H w): the two halves of one pair sector, read from the staged tile.  Eight
+// m8n8k4 MMAs (real H; sixteen for complex H) give C = w H - H w at
+// (r, 2t), (r, 2t+1); the result goes through a swizzled row-major tile to the
+// lane that owns the sector.  The sector order (pair_tables.inc) makes both
+// the operand reads and the exchange reads free of bank conflicts.
+//
+// Pipeline: per warp two slots, each filled by 1-D TMA bulk copies (tile,
+// neighbour row, tuple row, pf_same_sum) that complete on the slot's
+// mbarrier; the copies of ADO k+1 fly while ADO k is computed.  Every wait is
+// bounded; on expiry the kernel sets *p.err and the warp stops.
+// ---------------------------------------------------------------------------
+
+struct LaneTab {
+    signed char e1[32], e2[32]; // owned sector: element indices (row-major)
+    signed char fs[32][2];      // operand sector of k-slice s (-1: zero padding)
+    signed char ha[32][2];      // half of that sector holding A = w(r, 4s+t)
+};
+
+struct DmmaParams {
+    PairParams p;
+    LaneTab lt;
+    int* err;
+};
+
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void ld256(const double2* src, double2& a, double2& b)
+{
+    asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];\n"
+                 : "=d"(a.x), "=d"(a.y), "=d"(b.x), "=d"(b.y)
+                 : "l"(src));
+}
+
+__device__ __forceinline__ void ld256_cg(const double2* src, double2& a, double2& b)
+{
+    asm volatile("ld.global.v4.f64 {%0,%1,%2,%3}, [%4];\n"
+                 : "=d"(a.x), "=d"(a.y), "=d"(b.x), "=d"(b.y)
+                 : "l"(src));
+}
+
+__device__ __forceinline__ void st256_cs(double2* dst, double2 a, double2 b)
+{
+    asm volatile("st.global.cs.v4.f64 [%0], {%1,%2,%3,%4};\n" ::"l"(dst), "d"(a.x), "d"(a.y), "d"(b.x),
+                 "d"(b.y)
+                 : "memory");
+}
+
+__device__ __forceinline__ void st256(double2* dst, double2 a, double2 b)
+{
+    asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};\n" ::"l"(dst), "d"(a.x), "d"(a.y), "d"(b.x), "d"(b.y)
+                 : "memory");
+}
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect(uint64_t* bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// bounded wait for the phase `parity` of an mbarrier; false on expiry
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity)
+{
+    const unsigned a = smem_addr(bar);
+    for (int it = 0; it < (1 << 24); ++it) {
+        unsigned done;
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                     " selp.u32 %0, 1, 0, p;\n}\n"
+                     : "=r"(done)
+                     : "r"(a), "r"(parity)
+                     : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ int swz(int r) { return ((r & 1) << 2) | (r & 1) | (((r >> 1) & 1) << 1); }
+
+// bytes of one pipeline slot and of a warp's shared area for the DMMA kernel
+__host__ __device__ inline int dmma_slot_bytes(int P, int NW, int TWB)
+{
+    return P * 32 + ((NW * 4 + 15) & ~15) + ((TWB + 15) & ~15) + 16;
+}
+__host__ __device__ inline int dmma_warp_bytes(int P, int NW, int TWB)
+{
+    return 2 * dmma_slot_bytes(P, NW, TWB) + 64 * 16 /* exchange tile */ + 16 /* 2 mbarriers */;
+}
+__host__ inline size_t dmma_smem_bytes(int P, int W, int NW, int TWB, int LS)
+{
+    const size_t lut = (size_t)3 * W * LS * 16 + (size_t)W * LS * 8;
+    return ((lut + 15) & ~(size_t)15) + (size_t)kCtaWarps * dmma_warp_bytes(P, NW, TWB);
+}
+
+template <int N, int HK, int SLT>
+__global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_dmma_stage(const DmmaParams dp)
+{
+    static_assert(N <= 8, "DMMA stage handles N <= 8");
+    constexpr int P = pairs_of(N);
+    const PairParams& p = dp.p;
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int W = p.W, LS = p.LS, SL = p.SL;
+
+    double2* s_kmin = reinterpret_cast<double2*>(smem);        // 3 * W * LS
+    double* s_cplus = reinterpret_cast<double*>(s_kmin + 3 * W * LS); // W * LS
+    for (int q = threadIdx.x; q < W * LS; q += blockDim.x) s_cplus[q] = p.cplus[q];
+    for (int q = threadIdx.x; q < 3 * W * LS; q += blockDim.x) s_kmin[q] = p.kmin[q];
+    const int lut = ((3 * W * LS * 16 + W * LS * 8) + 15) & ~15;
+
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int slot_b = dmma_slot_bytes(P, p.NW, p.TWB);
+    unsigned char* wbase = smem + lut + warp * dmma_warp_bytes(P, p.NW, p.TWB);
+    double2* xch = reinterpret_cast<double2*>(wbase + 2 * slot_b);      // 8 x 8 swizzled
+    uint64_t* bars = reinterpret_cast<uint64_t*>(wbase + 2 * slot_b + 64 * 16);
+    const int tile_b = P * 32;
+    const int nbr_off = tile_b;
+    const int tup_off = nbr_off + ((p.NW * 4 + 15) & ~15);
+    const int pss_off = tup_off + ((p.TWB + 15) & ~15);
+    const unsigned tx_bytes = (unsigned)(tile_b + p.NW * 4 + p.TWB + 16);
+
+    // lane tables
+    const bool owner = lane < P;
+    const int e1 = owner ? dp.lt.e1[lane] : 0, e2 = owner ? dp.lt.e2[lane] : 0;
+    const int i1 = e1 / N, j1 = e1 - i1 * N, i2 = e2 / N, j2 = e2 - i2 * N;
+    const int diag = (i1 == j1);
+    const int si = i1, sj = j1; // sites of the element pair (diagonal: the two diagonal sites are i1 and i2)
+    const int fs0 = dp.lt.fs[lane][0], fs1 = dp.lt.fs[lane][1];
+    const int ha0 = dp.lt.ha[lane][0], ha1 = dp.lt.ha[lane][1];
+    const int r = lane >> 2, t = lane & 3;
+    const int xr1 = 8 * i1 + (j1 ^ swz(i1)), xr2 = 8 * i2 + (j2 ^ swz(i2));
+    const int xw0 = 8 * r + ((2 * t) ^ swz(r)), xw1 = 8 * r + ((2 * t + 1) ^ swz(r));
+
+    // operand fragments of H / hbar (zero outside the N x N block)
+    double hb_r[2], hb_i[2], ha_r[2], ha_i[2];
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+        const int k = 4 * s + t;
+        const bool in = (r < N && k < N);
+        const double2 hkr = in ? p.hs[k * N + r] : make_double2(0.0, 0.0); // B operand of w H: H(k, r)
+        const double2 hrk = in ? p.hs[r * N + k] : make_double2(0.0, 0.0); // A operand of H w: H(r, k)
+        hb_r[s] = hkr.x;
+        hb_i[s] = hkr.y;
+        ha_r[s] = -hrk.x;
+        ha_i[s] = -hrk.y;
+    }
+    const double2 g1 = owner ? p.gamma0[e1] : make_double2(0.0, 0.0);
+    const double2 g2 = owner ? p.gamma0[e2] : make_double2(0.0, 0.0);
+    int sli[SLT], slj[SLT];
+#pragma unroll
+    for (int q = 0; q < SLT; ++q) {
+        // diagonal sectors: element 1 = (i1,i1) uses the slots of site i1, element 2 = (i2,i2) those of i2
+        const int a = si, b = diag ? i2 : sj;
+        sli[q] = (owner && q < SL) ? p.slots[a * SL + q] : -1;
+        slj[q] = (owner && q < SL) ? p.slots[b * SL + q] : -1;
+    }
+    const double2* kap_i1 = s_kmin + (diag ? 2 : 0) * W * LS;
+    const double2* kap_j1 = s_kmin + 1 * W * LS;
+    const double2* kap_i2 = s_kmin + 1 * W * LS;
+    const double2* kap_j2 = s_kmin + (diag ? 2 : 0) * W * LS;
+
+    if (lane == 0) {
+        mbar_init(&bars[0]);
+        mbar_init(&bars[1]);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+
+    const int64_t nodes = p.nodes;
+    const int64_t stride = (int64_t)gridDim.x * kCtaWarps;
+    int64_t u = (int64_t)blockIdx.x * kCtaWarps + warp;
+    unsigned ph0 = 0u, ph1 = 0u; // mbarrier phase parity of slot 0 / slot 1
+
+    auto issue = [&](int64_t v, int sl) {
+        unsigned char* slot = wbase + sl * slot_b;
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        mbar_expect(&bars[sl], tx_bytes);
+        bulk_g2s(slot, p.in + v * (2 * P), tile_b, &bars[sl]);
+        bulk_g2s(slot + nbr_off, p.nbr + v * p.NW, p.NW * 4, &bars[sl]);
+        bulk_g2s(slot + tup_off, p.tup + v * p.TWB, p.TWB, &bars[sl]);
+        bulk_g2s(slot + pss_off, p.pss + v, 16, &bars[sl]);
+    };
+    if (u < nodes && lane == 0) issue(u, 0);
+    int cur = 0;
+    bool failed = false;
+    for (; u < nodes; u += stride) {
+        const int64_t un = u + stride;
+        if (un < nodes && lane == 0) issue(un, cur ^ 1);
+        if (!mbar_wait(&bars[cur], cur ? ph1 : ph0)) {
+            failed = true;
+            break;
+        }
+        if (cur) ph1 ^= 1u; else ph0 ^= 1u;
+        const unsigned char* slot = wbase + cur * slot_b;
+        const double2* tile = reinterpret_cast<const double2*>(slot);
+        const int32_t* nb = reinterpret_cast<const int32_t*>(slot + nbr_off);
+        const unsigned char* tu = slot + tup_off;
+        const double2 pss = *reinterpret_cast<const double2*>(slot + pss_off);
+
+        // ---- commutator on the tensor pipe ----
+        double cr0 = 0.0, cr1 = 0.0, ci0 = 0.0, ci1 = 0.0;
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            const int fs = s == 0 ? fs0 : fs1;
+            const int ha = s == 0 ? ha0 : ha1;
+            double2 A = make_double2(0.0, 0.0), B = A;
+            if (fs >= 0) {
+                A = tile[2 * fs + ha];
+                B = (r == 4 * s + t) ? A : tile[2 * fs + (ha ^ 1)];
+            }
+            dmma(cr0, cr1, A.x, hb_r[s]); // Re(w) Re(H)
+            dmma(ci0, ci1, A.y, hb_r[s]); // Im(w) Re(H)
+            dmma(cr0, cr1, ha_r[s], B.x); // -Re(H) Re(w)
+            dmma(ci0, ci1, ha_r[s], B.y); // -Re(H) Im(w)
+            if (HK == H_GENERIC) {
+                dmma(cr0, cr1, -A.y, hb_i[s]); // -Im(w) Im(H)
+                dmma(ci0, ci1, A.x, hb_i[s]);  //  Re(w) Im(H)
+                dmma(cr0, cr1, -ha_i[s], B.y); // +Im(H) Im(w)
+                dmma(ci0, ci1, ha_i[s], B.x);  // -Im(H) Re(w)
+            }
+        }
+        xch[xw0] = make_double2(cr0, ci0);
+        xch[xw1] = make_double2(cr1, ci1);
+        __syncwarp();
+
+        if (owner) {
+            const double2 c1 = xch[xr1], c2 = xch[xr2];
+            const double2 s1 = tile[2 * lane], s2 = tile[2 * lane + 1];
+            double2 L1 = make_double2(-c1.y, c1.x); // i * (w H - H w) / hbar
+            double2 L2 = make_double2(-c2.y, c2.x);
+            cmac(L1, make_double2(pss.x + g1.x, pss.y + g1.y), s1);
+            cmac(L2, make_double2(pss.x + g2.x, pss.y + g2.y), s2);
+
+#pragma unroll
+            for (int sd = 0; sd < 2; ++sd) {
+                double2 xp[SLT][2], xm[SLT][2];
+                int ix[SLT];
+#pragma unroll
+                for (int q = 0; q < SLT; ++q) {
+                    const int sl = sd == 0 ? sli[q] : slj[q];
+                    const int32_t vp = (sl >= 0 && !diag) ? nb[sl] : -1;
+                    const int32_t vm = sl >= 0 ? nb[W + sl] : -1;
+                    ix[q] = sl >= 0 ? (sl * LS + tu[sl]) : 0;
+                    xp[q][0] = xp[q][1] = xm[q][0] = xm[q][1] = make_double2(0.0, 0.0);
+                    if (vp >= 0) ld256(p.in + (int64_t)vp * (2 * P) + 2 * lane, xp[q][0], xp[q][1]);
+                    if (vm >= 0) ld256(p.in + (int64_t)vm * (2 * P) + 2 * lane, xm[q][0], xm[q][1]);
+                }
+#pragma unroll
+                for (int q = 0; q < SLT; ++q) {
+                    const int sl = sd == 0 ? sli[q] : slj[q];
+                    if (sl < 0) continue;
+                    const double c = diag ? 0.0 : s_cplus[ix[q]];
+                    if (sd == 0) {
+                        L1.x = fma(-c, xp[q][0].y, L1.x);
+                        L1.y = fma(c, xp[q][0].x, L1.y);
+                        L2.x = fma(c, xp[q][1].y, L2.x);
+                        L2.y = fma(-c, xp[q][1].x, L2.y);
+                        cmac(L1, kap_i1[ix[q]], xm[q][0]);
+                        if (!diag) cmac(L2, kap_i2[ix[q]], xm[q][1]);
+                    } else {
+                        L1.x = fma(c, xp[q][0].y, L1.x);
+                        L1.y = fma(-c, xp[q][0].x, L1.y);
+                        L2.x = fma(-c, xp[q][1].y, L2.x);
+                        L2.y = fma(c, xp[q][1].x, L2.y);
+                        if (!diag) cmac(L1, kap_j1[ix[q]], xm[q][0]);
+                        cmac(L2, kap_j2[ix[q]], xm[q][1]);
+                    }
+                }
+            }
+
+            const int64_t off = u * (2 * P) + 2 * lane;
+            double2 x1 = s1, x2 = s2;
+            if (p.y) ld256_cg(p.y + off, x1, x2);
+            double2 o1 = make_double2(p.alpha.x * x1.x - p.alpha.y * x1.y, p.alpha.x * x1.y + p.alpha.y * x1.x);
+            double2 o2 = make_double2(p.alpha.x * x2.x - p.alpha.y * x2.y, p.alpha.x * x2.y + p.alpha.y * x2.x);
+            cmac(o1, p.beta, L1);
+            cmac(o2, p.beta, L2);
+            st256_cs(p.out + off, o1, o2);
+            if (p.use_acc) {
+                double2 a1 = s1, a2 = s2;
+                if (!p.acc_init) ld256_cg(p.acc + off, a1, a2);
+                cmac(a1, p.acc_beta, L1);
+                cmac(a2, p.acc_beta, L2);
+                st256(p.acc + off, a1, a2);
+            }
+        }
+        __syncwarp();
+        cur ^= 1;
+    }
+    if (failed) {
+        if (lane == 0) atomicExch(dp.err, 1);
+        // let copies still in flight land before the warp leaves (bounded)
+        mbar_wait(&bars[cur ^ 1], cur ? ph0 : ph1);
+    }
+}
+
 // out = y + h * sum_l c_l k_l over doubles, terms with c_l == 0 skipped, in
 // the operation order of rk_weighted_add.cl:78-95 (no contraction).
 struct WaddParams {
@@ -415,64 +734,58 @@ __global__ void heom_weighted_add(const WaddParams p)
 }
 
 // Reference layout (row-major tiles in uid order) <-> pair layout in the
-// internal ADO order.  One thread per (internal ADO, sector).
+// internal ADO order.  pe[2p], pe[2p+1] = element indices of the halves of
+// sector p (equal for the padding half).  One thread per (ADO, sector).
 __global__ void heom_to_pairs(double2* __restrict__ dst, const double2* __restrict__ src,
-                              const int64_t* __restrict__ ref_of_int, int64_t nodes, int n)
+                              const int64_t* __restrict__ ref_of_int, const int16_t* __restrict__ pe,
+                              int64_t nodes, int n, int P)
 {
-    const int P = pairs_of(n);
     const int64_t total = nodes * P;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += stride) {
         const int64_t u = q / P;
         const int pr = (int)(q - u * P);
-        int e1, e2, i, j, d;
-        pair_elements(n, pr, &e1, &e2, &i, &j, &d);
         const int64_t r = ref_of_int[u] * n * n;
-        dst[2 * q] = src[r + e1];
-        dst[2 * q + 1] = src[r + e2];
+        dst[2 * q] = src[r + pe[2 * pr]];
+        dst[2 * q + 1] = src[r + pe[2 * pr + 1]];
     }
 }
 
 __global__ void heom_from_pairs(double2* __restrict__ dst, const double2* __restrict__ src,
-                                const int64_t* __restrict__ ref_of_int, int64_t nodes, int n)
+                                const int64_t* __restrict__ ref_of_int, const int16_t* __restrict__ pe,
+                                int64_t nodes, int n, int P)
 {
-    const int P = pairs_of(n);
     const int64_t total = nodes * P;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += stride) {
         const int64_t u = q / P;
         const int pr = (int)(q - u * P);
-        int e1, e2, i, j, d;
-        pair_elements(n, pr, &e1, &e2, &i, &j, &d);
         const int64_t r = ref_of_int[u] * n * n;
+        const int e1 = pe[2 * pr], e2 = pe[2 * pr + 1];
         dst[r + e1] = src[2 * q];
         if (e2 != e1) dst[r + e2] = src[2 * q + 1];
     }
 }
 
 // Copy the top matrix (internal ADO top_int, pair layout) into row `row` of a
-// row-major log; also used for heom_get_top with row 0.
+// row-major log.
 __global__ void heom_record_top(double2* __restrict__ log, const double2* __restrict__ y,
-                                int64_t top_int, int n, int64_t row)
+                                const int16_t* __restrict__ pe, int64_t top_int, int n, int P, int64_t row)
 {
-    const int P = pairs_of(n);
     for (int pr = threadIdx.x; pr < P; pr += blockDim.x) {
-        int e1, e2, i, j, d;
-        pair_elements(n, pr, &e1, &e2, &i, &j, &d);
+        const int e1 = pe[2 * pr], e2 = pe[2 * pr + 1];
         log[row * n * n + e1] = y[top_int * 2 * P + 2 * pr];
         if (e2 != e1) log[row * n * n + e2] = y[top_int * 2 * P + 2 * pr + 1];
     }
 }
 
 // Write a row-major top matrix into the pair layout of ADO top_int.
-__global__ void heom_write_top(double2* __restrict__ y, const double2* __restrict__ top, int64_t top_int, int n)
+__global__ void heom_write_top(double2* __restrict__ y, const double2* __restrict__ top,
+                               const int16_t* __restrict__ pe, int64_t top_int, int P)
 {
-    const int P = pairs_of(n);
     for (int pr = threadIdx.x; pr < P; pr += blockDim.x) {
-        int e1, e2, i, j, d;
-        pair_elements(n, pr, &e1, &e2, &i, &j, &d);
-        y[top_int * 2 * P + 2 * pr] = top[e1];
-        y[top_int * 2 * P + 2 * pr + 1] = top[e2];
+        y[top_int * 2 * P + 2 * pr] = top[pe[2 * pr]];
+        y[top_int * 2 * P + 2 * pr + 1] = top[pe[2 * pr + 1]];
     }
 }
 

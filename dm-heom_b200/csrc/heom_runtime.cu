@@ -19,6 +19,10 @@
 #include "heom_b200.h"
 #include "heom_kernels.cuh"
 
+namespace {
+#include "pair_tables.inc"
+}
+
 using heomk::PairParams;
 
 namespace {
@@ -86,6 +90,7 @@ struct DevBuf {
 };
 
 typedef void (*stage_fn_t)(const PairParams);
+typedef void (*dmma_fn_t)(const heomk::DmmaParams);
 
 template <int N, int HK>
 stage_fn_t pick_slt(int slt)
@@ -103,14 +108,43 @@ stage_fn_t pick_n(int hk, int slt)
     return hk == heomk::H_REAL_SYM ? pick_slt<N, heomk::H_REAL_SYM>(slt) : pick_slt<N, heomk::H_GENERIC>(slt);
 }
 
+// SIMT pair kernel: N = 9..16
 stage_fn_t pick_stage(int n, int hk, int slt)
 {
     switch (n) {
 #define HEOM_CASE(K) \
     case K: return pick_n<K>(hk, slt);
-        HEOM_CASE(1) HEOM_CASE(2) HEOM_CASE(3) HEOM_CASE(4) HEOM_CASE(5) HEOM_CASE(6)
-        HEOM_CASE(7) HEOM_CASE(8) HEOM_CASE(9) HEOM_CASE(10) HEOM_CASE(11) HEOM_CASE(12)
+        HEOM_CASE(9) HEOM_CASE(10) HEOM_CASE(11) HEOM_CASE(12)
         HEOM_CASE(13) HEOM_CASE(14) HEOM_CASE(15) HEOM_CASE(16)
+#undef HEOM_CASE
+    default: return nullptr;
+    }
+}
+
+template <int N, int HK>
+dmma_fn_t pick_dslt(int slt)
+{
+    switch (slt) {
+    case 2: return heomk::heom_dmma_stage<N, HK, 2>;
+    case 4: return heomk::heom_dmma_stage<N, HK, 4>;
+    default: return heomk::heom_dmma_stage<N, HK, 8>;
+    }
+}
+
+template <int N>
+dmma_fn_t pick_dn(int hk, int slt)
+{
+    return hk == heomk::H_REAL_SYM ? pick_dslt<N, heomk::H_REAL_SYM>(slt) : pick_dslt<N, heomk::H_GENERIC>(slt);
+}
+
+// tensor-pipe kernel: N = 1..8
+dmma_fn_t pick_dmma(int n, int hk, int slt)
+{
+    switch (n) {
+#define HEOM_CASE(K) \
+    case K: return pick_dn<K>(hk, slt);
+        HEOM_CASE(1) HEOM_CASE(2) HEOM_CASE(3) HEOM_CASE(4) HEOM_CASE(5) HEOM_CASE(6)
+        HEOM_CASE(7) HEOM_CASE(8)
 #undef HEOM_CASE
     default: return nullptr;
     }
@@ -176,6 +210,10 @@ struct heom_handle {
     DevBuf<double> d_cplus;
     DevBuf<int16_t> d_slots;
     DevBuf<int64_t> d_ref_of_int;
+    DevBuf<int16_t> d_pair;          // [P][2] element indices of the sector halves
+    std::vector<int16_t> pair_tab;   // host copy
+    heomk::LaneTab lane_tab{};       // DMMA kernel lane tables (N <= 8)
+    DevBuf<int> d_err;               // set by a stage kernel whose pipeline wait expired
 
     // propagation state + stage buffers
     heom_buffer y;
@@ -188,6 +226,7 @@ struct heom_handle {
     // launch accounting
     int64_t launches = 0;
     int stage_blocks[2] = {0, 0}; // per H kind
+    size_t stage_smem = 0;
 
     // cached graph of one RK4 step
     cudaGraphExec_t step_graph = nullptr;
@@ -341,32 +380,42 @@ int cta_threads(int n) { return (heomk::kCtaWarps / heomk::team_warps(n)) * heom
 int cta_teams(int n) { return heomk::kCtaWarps / heomk::team_warps(n); }
 
 // resolve the launch shape of the stage kernel (outside of any stream capture)
-int resolve_stage(heom_handle* h, stage_fn_t* fn_out, size_t* smem_out)
+int resolve_stage(heom_handle* h, const void** fn_out)
 {
-    stage_fn_t fn = pick_stage(h->N, h->hkind, h->SLT);
+    const void* fn = nullptr;
+    size_t smem = 0;
+    int threads = 0;
+    if (h->N <= 8) {
+        fn = (const void*)pick_dmma(h->N, h->hkind, h->SLT);
+        smem = heomk::dmma_smem_bytes(h->P, h->W, h->NW, h->TWB, h->LS);
+        threads = heomk::kCtaWarps * 32;
+    } else {
+        fn = (const void*)pick_stage(h->N, h->hkind, h->SLT);
+        smem = heomk::pair_smem_bytes(h->N, h->W, h->NW, h->TWB, h->LS);
+        threads = cta_threads(h->N);
+    }
     if (!fn) return fail(HEOM_E_UNSUPPORTED, "states = %d not supported", h->N);
-    const size_t smem = heomk::pair_smem_bytes(h->N, h->W, h->NW, h->TWB, h->LS);
     int& blocks = h->stage_blocks[h->hkind];
     if (blocks == 0) {
         if (smem > 227 * 1024) return fail(HEOM_E_UNSUPPORTED, "stage kernel needs %zu B of shared memory", smem);
-        CUDA_TRY(cudaFuncSetAttribute((const void*)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         int per_sm = 0;
-        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn, cta_threads(h->N), smem));
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
         if (per_sm < 1) return fail(HEOM_E_UNSUPPORTED, "stage kernel cannot be resident");
-        const int64_t groups = (h->nodes + cta_teams(h->N) - 1) / cta_teams(h->N);
+        const int teams = h->N <= 8 ? heomk::kCtaWarps : cta_teams(h->N);
+        const int64_t groups = (h->nodes + teams - 1) / teams;
         blocks = (int)std::min<int64_t>(groups, (int64_t)per_sm * h->sm_count);
     }
+    h->stage_smem = smem;
     *fn_out = fn;
-    *smem_out = smem;
     return 0;
 }
 
 int launch_stage(heom_handle* h, int epi, const double2* in, const double2* y, double2* out,
                  double2* acc, double2 beta, int acc_init)
 {
-    stage_fn_t fn = nullptr;
-    size_t smem = 0;
-    if (int rc = resolve_stage(h, &fn, &smem)) return rc;
+    const void* fn = nullptr;
+    if (int rc = resolve_stage(h, &fn)) return rc;
     PairParams p = base_params(h);
     p.in = in;
     p.out = out;
@@ -394,7 +443,15 @@ int launch_stage(heom_handle* h, int epi, const double2* in, const double2* y, d
         break;
     }
     const int blocks = h->stage_blocks[h->hkind];
-    fn<<<blocks, cta_threads(h->N), smem, h->stream>>>(p);
+    if (h->N <= 8) {
+        heomk::DmmaParams dp;
+        dp.p = p;
+        dp.lt = h->lane_tab;
+        dp.err = h->d_err.p;
+        ((dmma_fn_t)fn)<<<blocks, heomk::kCtaWarps * 32, h->stage_smem, h->stream>>>(dp);
+    } else {
+        ((stage_fn_t)fn)<<<blocks, cta_threads(h->N), h->stage_smem, h->stream>>>(p);
+    }
     h->launches++;
     CUDA_TRY(cudaGetLastError());
     return 0;
@@ -507,9 +564,8 @@ int run_steps(heom_handle* h, double dt, int64_t steps)
     }
     if (!h->step_graph) {
         // make sure launch shapes are resolved outside of capture
-        stage_fn_t fn = nullptr;
-        size_t smem = 0;
-        if (int rc = resolve_stage(h, &fn, &smem)) return rc;
+        const void* fn = nullptr;
+        if (int rc = resolve_stage(h, &fn)) return rc;
         cudaGraph_t graph = nullptr;
         const int64_t saved = h->launches;
         CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
@@ -566,6 +622,48 @@ int check_desc(const heom_instance_desc* d)
     return 0;
 }
 
+// sector tables of the pair layout: the searched order for N <= 8
+// (pair_tables.inc), the canonical order of heomk::pair_elements above
+int build_pair_tables(heom_handle* h)
+{
+    const int N = h->N, P = h->P;
+    h->pair_tab.assign(2 * P, 0);
+    for (int p = 0; p < P; ++p) {
+        int e1, e2, i, j, d;
+        if (N <= 8) {
+            e1 = kPairE1[N][p];
+            e2 = kPairE2[N][p];
+        } else {
+            heomk::pair_elements(N, p, &e1, &e2, &i, &j, &d);
+        }
+        h->pair_tab[2 * p] = (int16_t)e1;
+        h->pair_tab[2 * p + 1] = (int16_t)e2;
+    }
+    if (N <= 8) {
+        heomk::LaneTab& lt = h->lane_tab;
+        for (int l = 0; l < 32; ++l) {
+            lt.e1[l] = (signed char)(l < P ? h->pair_tab[2 * l] : 0);
+            lt.e2[l] = (signed char)(l < P ? h->pair_tab[2 * l + 1] : 0);
+            const int r = l >> 2, t = l & 3;
+            for (int s = 0; s < 2; ++s) {
+                const int k = 4 * s + t;
+                lt.fs[l][s] = -1;
+                lt.ha[l][s] = 0;
+                if (r >= N || k >= N) continue;
+                const int e = r * N + k;
+                for (int p = 0; p < P; ++p) {
+                    if (h->pair_tab[2 * p] == e) { lt.fs[l][s] = (signed char)p; lt.ha[l][s] = 0; break; }
+                    if (h->pair_tab[2 * p + 1] == e) { lt.fs[l][s] = (signed char)p; lt.ha[l][s] = 1; break; }
+                }
+                if (lt.fs[l][s] < 0) return fail(HEOM_E_UNSUPPORTED, "pair table misses element %d", e);
+            }
+        }
+    }
+    if (int rc = h->d_pair.alloc(2 * P)) return rc;
+    CUDA_TRY(cudaMemcpy(h->d_pair.p, h->pair_tab.data(), 2 * P * sizeof(int16_t), cudaMemcpyHostToDevice));
+    return 0;
+}
+
 // internal order: lexicographic rank of the tuple when the tuples form the
 // complete hierarchy, else the reference order
 void build_order(heom_handle* h)
@@ -612,7 +710,8 @@ int to_internal(heom_handle* h, double2* dst, const double* host)
     CUDA_TRY(cudaMemcpyAsync(h->xfer.p, host, bytes, cudaMemcpyHostToDevice, h->stream));
     const int64_t total = h->nodes * h->P;
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, h->sm_count * 16));
-    heomk::heom_to_pairs<<<blocks, 256, 0, h->stream>>>(dst, h->xfer.p, h->d_ref_of_int.p, h->nodes, h->N);
+    heomk::heom_to_pairs<<<blocks, 256, 0, h->stream>>>(dst, h->xfer.p, h->d_ref_of_int.p, h->d_pair.p, h->nodes,
+                                                         h->N, h->P);
     h->launches++;
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -624,11 +723,24 @@ int from_internal(heom_handle* h, double* host, const double2* src)
     const size_t bytes = h->ref_elems() * sizeof(double2);
     const int64_t total = h->nodes * h->P;
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, h->sm_count * 16));
-    heomk::heom_from_pairs<<<blocks, 256, 0, h->stream>>>(h->xfer.p, src, h->d_ref_of_int.p, h->nodes, h->N);
+    heomk::heom_from_pairs<<<blocks, 256, 0, h->stream>>>(h->xfer.p, src, h->d_ref_of_int.p, h->d_pair.p, h->nodes,
+                                                           h->N, h->P);
     h->launches++;
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(host, h->xfer.p, bytes, cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+// a stage kernel whose bounded pipeline wait expired leaves a flag behind
+int check_kernel_error(heom_handle* h)
+{
+    int err = 0;
+    CUDA_TRY(cudaMemcpy(&err, h->d_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) {
+        cudaMemset(h->d_err.p, 0, sizeof(int));
+        return fail(HEOM_E_CUDA, "stage kernel pipeline wait expired (results of this call are invalid)");
+    }
     return 0;
 }
 
@@ -699,6 +811,7 @@ int heom_create(const heom_instance_desc* d, const heom_options* opt, heom_handl
         if (!(std::hypot(h->cbk[2 * q], h->cbk[2 * q + 1]) > 0.0))
             return fail(HEOM_E_TABLE, "cbk[%d] is zero or not finite", q);
 
+    if (int rc = build_pair_tables(h.get())) return rc;
     build_order(h.get());
     if (int rc = h->d_ref_of_int.alloc(h->nodes)) return rc;
     CUDA_TRY(cudaMemcpy(h->d_ref_of_int.p, h->ref_of_int.data(), h->nodes * 8, cudaMemcpyHostToDevice));
@@ -712,6 +825,8 @@ int heom_create(const heom_instance_desc* d, const heom_options* opt, heom_handl
     if (int rc = h->xfer.alloc(h->ref_elems())) return rc;
     if (int rc = h->topbuf.alloc((size_t)h->N * h->N)) return rc;
     if (int rc = h->d_flag.alloc(1)) return rc;
+    if (int rc = h->d_err.alloc(1)) return rc;
+    CUDA_TRY(cudaMemset(h->d_err.p, 0, sizeof(int)));
     *out = h.release();
     return 0;
 }
@@ -812,7 +927,7 @@ int heom_solve(heom_handle* h, double, double, const heom_buffer* in, heom_buffe
     }
     if (rc) return rc;
     CUDA_TRY(cudaStreamSynchronize(h->stream));
-    return 0;
+    return check_kernel_error(h);
 }
 
 int heom_weighted_add(heom_handle* h, int n, double step, heom_buffer* out, const heom_buffer* y,
@@ -851,7 +966,7 @@ int heom_set_top(heom_handle* h, const double* top)
     CUDA_TRY(cudaSetDevice(h->device));
     const size_t nn = (size_t)h->N * h->N;
     CUDA_TRY(cudaMemcpyAsync(h->topbuf.p, top, nn * 16, cudaMemcpyHostToDevice, h->stream));
-    heomk::heom_write_top<<<1, 128, 0, h->stream>>>(h->y.data.p, h->topbuf.p, h->top_int, h->N);
+    heomk::heom_write_top<<<1, 128, 0, h->stream>>>(h->y.data.p, h->topbuf.p, h->d_pair.p, h->top_int, h->P);
     h->launches++;
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -863,7 +978,7 @@ int heom_get_top(heom_handle* h, double* top)
     if (!h || !top) return fail(HEOM_E_ARG, "NULL argument");
     CUDA_TRY(cudaSetDevice(h->device));
     const size_t nn = (size_t)h->N * h->N;
-    heomk::heom_record_top<<<1, 128, 0, h->stream>>>(h->topbuf.p, h->y.data.p, h->top_int, h->N, 0);
+    heomk::heom_record_top<<<1, 128, 0, h->stream>>>(h->topbuf.p, h->y.data.p, h->d_pair.p, h->top_int, h->N, h->P, 0);
     h->launches++;
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(top, h->topbuf.p, nn * 16, cudaMemcpyDeviceToHost, h->stream));
@@ -890,7 +1005,7 @@ int heom_synchronize(heom_handle* h)
     if (!h) return fail(HEOM_E_ARG, "NULL handle");
     CUDA_TRY(cudaSetDevice(h->device));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
-    return 0;
+    return check_kernel_error(h);
 }
 
 int heom_rk4_steps(heom_handle* h, double dt, int64_t steps)
@@ -908,12 +1023,12 @@ int heom_propagate(heom_handle* h, double dt, int64_t steps, int64_t observe_eve
     const int nn = h->N * h->N;
     if ((int64_t)h->toplog.n < rows * nn)
         if (int rc = h->toplog.alloc(rows * nn)) return rc;
-    heomk::heom_record_top<<<1, 128, 0, h->stream>>>(h->toplog.p, h->y.data.p, h->top_int, h->N, 0);
+    heomk::heom_record_top<<<1, 128, 0, h->stream>>>(h->toplog.p, h->y.data.p, h->d_pair.p, h->top_int, h->N, h->P, 0);
     h->launches++;
     CUDA_TRY(cudaGetLastError());
     for (int64_t r = 1; r < rows; ++r) {
         if (int rc = run_steps(h, dt, observe_every)) return rc;
-        heomk::heom_record_top<<<1, 128, 0, h->stream>>>(h->toplog.p, h->y.data.p, h->top_int, h->N, r);
+        heomk::heom_record_top<<<1, 128, 0, h->stream>>>(h->toplog.p, h->y.data.p, h->d_pair.p, h->top_int, h->N, h->P, r);
         h->launches++;
         CUDA_TRY(cudaGetLastError());
     }
@@ -927,6 +1042,7 @@ int heom_propagate(heom_handle* h, double dt, int64_t steps, int64_t observe_eve
     int flag = 0;
     CUDA_TRY(cudaMemcpyAsync(&flag, h->d_flag.p, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (int rc = check_kernel_error(h)) return rc;
     if (flag) return fail(HEOM_E_NONFINITE, "non-finite value in the hierarchy state after propagation");
     return 0;
 }

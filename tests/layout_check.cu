@@ -3,6 +3,9 @@
 // Prints one line per problem: "bad ..." for any violation, then "ok N".
 #include <cstdio>
 #include "heom_kernels.cuh"
+#include "pair_tables.inc"
+
+static int swz_h(int r) { return ((r & 1) << 2) | (r & 1) | (((r >> 1) & 1) << 1); }
 
 int main()
 {
@@ -34,6 +37,57 @@ int main()
                     L.pss_off - L.tup_off < TWB || L.slot - L.pss_off < 16) { printf("bad sizes n=%d W=%d\n", n, W); ++bad; }
                 if (NW % 4 || NW < 2 * W || TWB % 16 || TWB < W) { printf("bad pads W=%d\n", W); ++bad; }
                 ++checked;
+            }
+    }
+    // searched sector tables for N <= 8: coverage, and for N = 8 conflict-free
+    // operand and exchange reads of the tensor-pipe kernel
+    for (int n = 1; n <= 8; ++n) {
+        const int P = heomk::pairs_of(n);
+        int seen[64] = {0};
+        for (int p = 0; p < P; ++p) {
+            const int e1 = kPairE1[n][p], e2 = kPairE2[n][p];
+            if (e1 < 0 || e1 >= n * n || e2 < 0 || e2 >= n * n) { printf("bad table range n=%d\n", n); ++bad; continue; }
+            const int i1 = e1 / n, j1 = e1 % n, i2 = e2 / n, j2 = e2 % n;
+            const bool d1 = i1 == j1, d2 = i2 == j2;
+            if (d1 != d2 || (!d1 && !(i1 == j2 && j1 == i2))) { printf("bad pair n=%d p=%d\n", n, p); ++bad; }
+            seen[e1]++;
+            if (e2 != e1) seen[e2]++;
+        }
+        for (int e = 0; e < n * n; ++e)
+            if (seen[e] != 1) { printf("bad table coverage n=%d e=%d\n", n, e); ++bad; }
+        for (int W = 1; W <= 64; ++W) {
+            const int NW = (2 * W + 3) & ~3, TWB = (W + 15) & ~15;
+            const int sb = heomk::dmma_slot_bytes(P, NW, TWB), wb = heomk::dmma_warp_bytes(P, NW, TWB);
+            if (sb % 16 || wb % 16 || sb < P * 32 + NW * 4 + TWB + 16) { printf("bad dmma slot n=%d W=%d\n", n, W); ++bad; }
+            if (heomk::dmma_smem_bytes(P, W, NW, TWB, 41) > 227 * 1024) { printf("dmma smem too big n=%d W=%d\n", n, W); ++bad; }
+        }
+    }
+    {
+        const int n = 8;
+        int sec[64], half[64];
+        for (int p = 0; p < 32; ++p) {
+            sec[kPairE1[n][p]] = p; half[kPairE1[n][p]] = 0;
+            sec[kPairE2[n][p]] = p; half[kPairE2[n][p]] = 1;
+        }
+        for (int q = 0; q < 4; ++q)
+            for (int s = 0; s < 2; ++s)
+                for (int which = 0; which < 2; ++which) {
+                    int used[8] = {0};
+                    for (int rr = 2 * q; rr <= 2 * q + 1; ++rr)
+                        for (int t = 0; t < 4; ++t) {
+                            const int col = 4 * s + t;
+                            if (which == 1 && rr == col) continue;
+                            const int e = which == 0 ? rr * n + col : col * n + rr;
+                            if (used[(2 * sec[e] + half[e]) % 8]++) { printf("bank conflict operand q=%d s=%d\n", q, s); ++bad; }
+                        }
+                }
+        for (int k = 0; k < 4; ++k)
+            for (int which = 0; which < 2; ++which) {
+                int used[8] = {0};
+                for (int p = 8 * k; p < 8 * k + 8; ++p) {
+                    const int e = which == 0 ? kPairE1[n][p] : kPairE2[n][p];
+                    if (used[((e % n) ^ swz_h(e / n)) % 8]++) { printf("bank conflict exchange k=%d\n", k); ++bad; }
+                }
             }
     }
     printf("%s %ld\n", bad ? "FAILED" : "ok", checked);
