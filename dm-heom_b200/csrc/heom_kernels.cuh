@@ -412,9 +412,21 @@ struct LaneTab {
     signed char ha[32][2];      // half of that sector holding A = w(r, 4s+t)
 };
 
+// Factored bath coefficients: cplus(n) = chat * sqrt(n+1), kappa(n) = khat * sqrt(n)
+// (heom_ode.cl:211,249 and :321,383).  Per-slot constants are stored at
+// position pos(slot) = m * B + b (slot = b*M + m) so that the lanes of a warp,
+// which read the same m for different baths, hit different banks.
+struct CoefTabs {
+    const double* chat;   // [W] at pos(slot)
+    const double2* khat;  // [3][W] at pos(slot): kappa_i, kappa_j, kappa_i + kappa_j (n = 1)
+    const double* sq;     // [D+2]: sqrt(n)
+    const int16_t* pos;   // [W] slot -> position
+};
+
 struct DmmaParams {
     PairParams p;
     LaneTab lt;
+    CoefTabs ct;
     int* err;
 };
 
@@ -500,10 +512,14 @@ __host__ __device__ inline int dmma_warp_bytes(int P, int NW, int TWB)
 {
     return 2 * dmma_slot_bytes(P, NW, TWB) + 64 * 16 /* exchange tile */ + 16 /* 2 mbarriers */;
 }
+// shared look-up tables of the DMMA kernel: khat 3*W double2, chat W doubles, sqrt LS+1 doubles
+__host__ __device__ inline int dmma_lut_bytes(int W, int LS)
+{
+    return ((3 * W * 16 + W * 8 + (LS + 1) * 8) + 15) & ~15;
+}
 __host__ inline size_t dmma_smem_bytes(int P, int W, int NW, int TWB, int LS)
 {
-    const size_t lut = (size_t)3 * W * LS * 16 + (size_t)W * LS * 8;
-    return ((lut + 15) & ~(size_t)15) + (size_t)kCtaWarps * dmma_warp_bytes(P, NW, TWB);
+    return (size_t)dmma_lut_bytes(W, LS) + (size_t)kCtaWarps * dmma_warp_bytes(P, NW, TWB);
 }
 
 template <int N, int HK, int SLT>
@@ -515,11 +531,13 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_dmma_stage(const DmmaP
     extern __shared__ __align__(128) unsigned char smem[];
     const int W = p.W, LS = p.LS, SL = p.SL;
 
-    double2* s_kmin = reinterpret_cast<double2*>(smem);        // 3 * W * LS
-    double* s_cplus = reinterpret_cast<double*>(s_kmin + 3 * W * LS); // W * LS
-    for (int q = threadIdx.x; q < W * LS; q += blockDim.x) s_cplus[q] = p.cplus[q];
-    for (int q = threadIdx.x; q < 3 * W * LS; q += blockDim.x) s_kmin[q] = p.kmin[q];
-    const int lut = ((3 * W * LS * 16 + W * LS * 8) + 15) & ~15;
+    double2* s_kh = reinterpret_cast<double2*>(smem);            // 3 * W
+    double* s_ch = reinterpret_cast<double*>(s_kh + 3 * W);       // W
+    double* s_sq = s_ch + W;                                      // LS + 1
+    for (int q = threadIdx.x; q < 3 * W; q += blockDim.x) s_kh[q] = dp.ct.khat[q];
+    for (int q = threadIdx.x; q < W; q += blockDim.x) s_ch[q] = dp.ct.chat[q];
+    for (int q = threadIdx.x; q <= LS; q += blockDim.x) s_sq[q] = dp.ct.sq[q];
+    const int lut = dmma_lut_bytes(W, LS);
 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -560,18 +578,20 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_dmma_stage(const DmmaP
     }
     const double2 g1 = owner ? p.gamma0[e1] : make_double2(0.0, 0.0);
     const double2 g2 = owner ? p.gamma0[e2] : make_double2(0.0, 0.0);
-    int sli[SLT], slj[SLT];
+    int sli[SLT], slj[SLT], pi[SLT], pj[SLT];
 #pragma unroll
     for (int q = 0; q < SLT; ++q) {
         // diagonal sectors: element 1 = (i1,i1) uses the slots of site i1, element 2 = (i2,i2) those of i2
         const int a = si, b = diag ? i2 : sj;
         sli[q] = (owner && q < SL) ? p.slots[a * SL + q] : -1;
         slj[q] = (owner && q < SL) ? p.slots[b * SL + q] : -1;
+        pi[q] = sli[q] >= 0 ? dp.ct.pos[sli[q]] : 0;
+        pj[q] = slj[q] >= 0 ? dp.ct.pos[slj[q]] : 0;
     }
-    const double2* kap_i1 = s_kmin + (diag ? 2 : 0) * W * LS;
-    const double2* kap_j1 = s_kmin + 1 * W * LS;
-    const double2* kap_i2 = s_kmin + 1 * W * LS;
-    const double2* kap_j2 = s_kmin + (diag ? 2 : 0) * W * LS;
+    const double2* kap_i1 = s_kh + (diag ? 2 : 0) * W;
+    const double2* kap_j1 = s_kh + 1 * W;
+    const double2* kap_i2 = s_kh + 1 * W;
+    const double2* kap_j2 = s_kh + (diag ? 2 : 0) * W;
 
     if (lane == 0) {
         mbar_init(&bars[0]);
@@ -639,7 +659,10 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_dmma_stage(const DmmaP
 
         if (owner) {
             const double2 c1 = xch[xr1], c2 = xch[xr2];
-            const double2 s1 = tile[2 * lane], s2 = tile[2 * lane + 1];
+            // read the halves in a staggered order (conflict-free quarter warps)
+            const int h0 = (lane >> 2) & 1;
+            const double2 sa = tile[2 * lane + h0], sb = tile[2 * lane + (h0 ^ 1)];
+            const double2 s1 = h0 ? sb : sa, s2 = h0 ? sa : sb;
             double2 L1 = make_double2(-c1.y, c1.x); // i * (w H - H w) / hbar
             double2 L2 = make_double2(-c2.y, c2.x);
             cmac(L1, make_double2(pss.x + g1.x, pss.y + g1.y), s1);
@@ -648,13 +671,13 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_dmma_stage(const DmmaP
 #pragma unroll
             for (int sd = 0; sd < 2; ++sd) {
                 double2 xp[SLT][2], xm[SLT][2];
-                int ix[SLT];
+                int nn[SLT];
 #pragma unroll
                 for (int q = 0; q < SLT; ++q) {
                     const int sl = sd == 0 ? sli[q] : slj[q];
                     const int32_t vp = (sl >= 0 && !diag) ? nb[sl] : -1;
                     const int32_t vm = sl >= 0 ? nb[W + sl] : -1;
-                    ix[q] = sl >= 0 ? (sl * LS + tu[sl]) : 0;
+                    nn[q] = sl >= 0 ? tu[sl] : 0;
                     xp[q][0] = xp[q][1] = xm[q][0] = xm[q][1] = make_double2(0.0, 0.0);
                     if (vp >= 0) ld256(p.in + (int64_t)vp * (2 * P) + 2 * lane, xp[q][0], xp[q][1]);
                     if (vm >= 0) ld256(p.in + (int64_t)vm * (2 * P) + 2 * lane, xm[q][0], xm[q][1]);
@@ -663,21 +686,26 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_dmma_stage(const DmmaP
                 for (int q = 0; q < SLT; ++q) {
                     const int sl = sd == 0 ? sli[q] : slj[q];
                     if (sl < 0) continue;
-                    const double c = diag ? 0.0 : s_cplus[ix[q]];
+                    const int ps = sd == 0 ? pi[q] : pj[q];
+                    const double sqn = s_sq[nn[q]];
+                    const double c = diag ? 0.0 : s_ch[ps] * s_sq[nn[q] + 1];
+                    // minus neighbours scale as sqrt(n); fold it into the neighbour value
+                    const double2 m1 = make_double2(xm[q][0].x * sqn, xm[q][0].y * sqn);
+                    const double2 m2 = make_double2(xm[q][1].x * sqn, xm[q][1].y * sqn);
                     if (sd == 0) {
                         L1.x = fma(-c, xp[q][0].y, L1.x);
                         L1.y = fma(c, xp[q][0].x, L1.y);
                         L2.x = fma(c, xp[q][1].y, L2.x);
                         L2.y = fma(-c, xp[q][1].x, L2.y);
-                        cmac(L1, kap_i1[ix[q]], xm[q][0]);
-                        if (!diag) cmac(L2, kap_i2[ix[q]], xm[q][1]);
+                        cmac(L1, kap_i1[ps], m1);
+                        if (!diag) cmac(L2, kap_i2[ps], m2);
                     } else {
                         L1.x = fma(c, xp[q][0].y, L1.x);
                         L1.y = fma(-c, xp[q][0].x, L1.y);
                         L2.x = fma(-c, xp[q][1].y, L2.x);
                         L2.y = fma(c, xp[q][1].x, L2.y);
-                        if (!diag) cmac(L1, kap_j1[ix[q]], xm[q][0]);
-                        cmac(L2, kap_j2[ix[q]], xm[q][1]);
+                        if (!diag) cmac(L1, kap_j1[ps], m1);
+                        cmac(L2, kap_j2[ps], m2);
                     }
                 }
             }

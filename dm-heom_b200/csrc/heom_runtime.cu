@@ -209,6 +209,9 @@ struct heom_handle {
     DevBuf<double2> d_pss, d_kmin, d_hs, d_gamma0;
     DevBuf<double> d_cplus;
     DevBuf<int16_t> d_slots;
+    DevBuf<double> d_chat, d_sq;     // factored coefficients (DMMA kernel)
+    DevBuf<double2> d_khat;
+    DevBuf<int16_t> d_pos;
     DevBuf<int64_t> d_ref_of_int;
     DevBuf<int16_t> d_pair;          // [P][2] element indices of the sector halves
     std::vector<int16_t> pair_tab;   // host copy
@@ -347,6 +350,35 @@ int upload_coefficients(heom_handle* h)
             for (int m = 0; m < M; ++m) slots[s * h->SL + q++] = (int16_t)(bs * M + m);
         }
     }
+    // factored form: cplus(n) = chat sqrt(n+1), kappa(n) = khat sqrt(n), stored at pos(slot) = m*B + b
+    {
+        std::vector<double> chat(W, 0.0), sq(LS + 1, 0.0);
+        std::vector<double2> khat((size_t)3 * W, make_double2(0.0, 0.0));
+        std::vector<int16_t> pos(W, 0);
+        for (int sl = 0; sl < W; ++sl) {
+            const int b = sl / M, m = sl - b * M;
+            const int ps = m * h->B + b;
+            pos[sl] = (int16_t)ps;
+            const double cr = h->cbk[2 * sl], ci = h->cbk[2 * sl + 1];
+            const double qr = m == 0 ? h->pf_circ[2 * b] : 0.0;
+            const double qi = m == 0 ? h->pf_circ[2 * b + 1] : 0.0;
+            const double habs = std::hypot(cr, ci);
+            chat[ps] = std::sqrt(habs / kHbar);
+            const double sc = std::sqrt(kHbar / habs);
+            khat[0 * W + ps] = make_double2(sc * (-ci / kHbar + qr), sc * (cr / kHbar + qi));
+            khat[1 * W + ps] = make_double2(sc * (ci / kHbar + qr), sc * (-cr / kHbar + qi));
+            khat[2 * W + ps] = make_double2(2.0 * sc * qr, 2.0 * sc * qi);
+        }
+        for (int n = 0; n <= LS; ++n) sq[n] = std::sqrt((double)n);
+        if (int rc = h->d_chat.alloc(W)) return rc;
+        if (int rc = h->d_khat.alloc(3 * W)) return rc;
+        if (int rc = h->d_sq.alloc(LS + 1)) return rc;
+        if (int rc = h->d_pos.alloc(W)) return rc;
+        CUDA_TRY(cudaMemcpy(h->d_chat.p, chat.data(), W * 8, cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaMemcpy(h->d_khat.p, khat.data(), 3 * W * 16, cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaMemcpy(h->d_sq.p, sq.data(), (LS + 1) * 8, cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaMemcpy(h->d_pos.p, pos.data(), W * 2, cudaMemcpyHostToDevice));
+    }
     if (int rc = h->d_cplus.alloc(cplus.size())) return rc;
     if (int rc = h->d_kmin.alloc(kmin.size())) return rc;
     if (int rc = h->d_slots.alloc(slots.size())) return rc;
@@ -447,6 +479,10 @@ int launch_stage(heom_handle* h, int epi, const double2* in, const double2* y, d
         heomk::DmmaParams dp;
         dp.p = p;
         dp.lt = h->lane_tab;
+        dp.ct.chat = h->d_chat.p;
+        dp.ct.khat = h->d_khat.p;
+        dp.ct.sq = h->d_sq.p;
+        dp.ct.pos = h->d_pos.p;
         dp.err = h->d_err.p;
         ((dmma_fn_t)fn)<<<blocks, heomk::kCtaWarps * 32, h->stage_smem, h->stream>>>(dp);
     } else {
