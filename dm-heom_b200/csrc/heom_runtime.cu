@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -768,6 +769,42 @@ int from_internal(heom_handle* h, double* host, const double2* src)
     return 0;
 }
 
+// ---------------------------------------------------------------------------
+// Static scratch for heom_rk4_steps_noalloc: three state-sized buffers (the
+// caller's state converted to the pair layout, and the two stage buffers of
+// the product-form RK4 step).  The array is part of this module, so every GPU
+// that loads the library holds it until the process exits.
+// ---------------------------------------------------------------------------
+constexpr size_t kNoAllocBufferBytes = size_t(16) << 20; // per buffer
+constexpr int kNoAllocBuffers = 3;
+constexpr int kNoAllocMaxDevices = 128;
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+} // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBuffers * kNoAllocBufferBytes];
+
+namespace {
+
+// Device address of the static scratch on `device`, which the caller has made
+// current.  Resolved once per device: in host code the array's name is only a
+// host-side stand-in, so kernels are always given this address.
+int noalloc_scratch(int device, unsigned char** out)
+{
+    if (device < 0 || device >= kNoAllocMaxDevices) return fail(HEOM_E_ARG, "device ordinal %d out of range", device);
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[device]) {
+        void* ptr = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess || !ptr)
+            return fail(HEOM_E_CUDA, "cudaGetSymbolAddress of the static scratch failed: %s", cudaGetErrorString(e));
+        g_noalloc_addr[device] = ptr;
+    }
+    *out = static_cast<unsigned char*>(g_noalloc_addr[device]);
+    return 0;
+}
+
 // a stage kernel whose bounded pipeline wait expired leaves a flag behind
 int check_kernel_error(heom_handle* h)
 {
@@ -1081,6 +1118,45 @@ int heom_propagate(heom_handle* h, double dt, int64_t steps, int64_t observe_eve
     if (int rc = check_kernel_error(h)) return rc;
     if (flag) return fail(HEOM_E_NONFINITE, "non-finite value in the hierarchy state after propagation");
     return 0;
+}
+
+int heom_rk4_steps_noalloc(heom_handle* h, double* d_state, double dt, int64_t steps)
+{
+    if (!h || !d_state || steps < 0 || !(dt > 0.0)) return fail(HEOM_E_ARG, "bad argument");
+    if (reinterpret_cast<uintptr_t>(d_state) % 16 != 0) return fail(HEOM_E_ARG, "d_state must be 16-byte aligned");
+    const size_t need = h->state_elems() * sizeof(double2);
+    if (need > kNoAllocBufferBytes)
+        return fail(HEOM_E_UNSUPPORTED,
+                    "heom_rk4_steps_noalloc: this hierarchy needs %zu bytes per state buffer; the static scratch "
+                    "holds %zu bytes per buffer (use heom_rk4_steps)",
+                    need, kNoAllocBufferBytes);
+    CUDA_TRY(cudaSetDevice(h->device));
+    unsigned char* base = nullptr;
+    if (int rc = noalloc_scratch(h->device, &base)) return rc;
+    double2* y = reinterpret_cast<double2*>(base);
+    double2* a = reinterpret_cast<double2*>(base + kNoAllocBufferBytes);
+    double2* b = reinterpret_cast<double2*>(base + 2 * kNoAllocBufferBytes);
+    // every element of y, a and b is written before it is read in this call, so
+    // what an earlier call left in the array needs no clearing
+    const int64_t total = h->nodes * h->P;
+    const int cblocks = (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, h->sm_count * 16));
+    heomk::heom_to_pairs<<<cblocks, 256, 0, h->stream>>>(y, reinterpret_cast<const double2*>(d_state),
+                                                          h->d_ref_of_int.p, h->d_pair.p, h->nodes, h->N, h->P);
+    h->launches++;
+    CUDA_TRY(cudaGetLastError());
+    const double2* ins[4] = {y, a, b, a};
+    double2* outs[4] = {a, b, a, y};
+    for (int64_t s = 0; s < steps; ++s)
+        for (int k = 0; k < 4; ++k) {
+            const double2 beta = make_double2(dt * kProdBeta[k][0], dt * kProdBeta[k][1]);
+            if (int rc = launch_stage(h, EPI_AXPY_SELF, ins[k], nullptr, outs[k], nullptr, beta, 0)) return rc;
+        }
+    heomk::heom_from_pairs<<<cblocks, 256, 0, h->stream>>>(reinterpret_cast<double2*>(d_state), y,
+                                                            h->d_ref_of_int.p, h->d_pair.p, h->nodes, h->N, h->P);
+    h->launches++;
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return check_kernel_error(h);
 }
 
 void* heom_stream(heom_handle* h) { return h ? (void*)h->stream : nullptr; }

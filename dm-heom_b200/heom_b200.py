@@ -35,7 +35,7 @@ EXPORTS = [
     "heom_synchronize", "heom_stream", "heom_matrices", "heom_states", "heom_kernel_launches",
     "heom_tables_build", "heom_tables_view", "heom_tables_free", "heom_create_from_system",
     "heom_config_load", "heom_config_free", "heom_config_system", "heom_config_rho_init",
-    "heom_config_get", "heom_tables_mask",
+    "heom_config_get", "heom_tables_mask", "heom_rk4_steps_noalloc",
 ]
 
 
@@ -116,6 +116,7 @@ def lib():
         L.heom_config_system.argtypes = [vp, C.POINTER(SystemDesc)]
         L.heom_config_rho_init.argtypes = [vp, vp]
         L.heom_config_get.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_size_t]
+        L.heom_rk4_steps_noalloc.argtypes = [vp, vp, dbl, i64]
         _lib = L
     return _lib
 
@@ -252,6 +253,10 @@ class Heom:
     # -- stepping ------------------------------------------------------------
     def rk4_steps(self, dt, steps):
         _check(lib().heom_rk4_steps(self.h, dt, steps))
+
+    def rk4_steps_noalloc(self, d_state_ptr, dt, steps):
+        """heom_rk4_steps_noalloc on a caller-owned device buffer (reference layout)."""
+        _check(lib().heom_rk4_steps_noalloc(self.h, C.c_void_p(d_state_ptr), dt, steps))
 
     def rk4_steps_async(self, dt, steps):
         _check(lib().heom_rk4_steps_async(self.h, dt, steps))

@@ -172,6 +172,25 @@ int heom_propagate(heom_handle* h, double dt, int64_t steps, int64_t observe_eve
  * stream and returns; heom_synchronize waits for it. */
 int heom_rk4_steps_async(heom_handle* h, double dt, int64_t steps);
 int heom_synchronize(heom_handle* h);
+/* Advance a hierarchy state that the caller keeps in its own device memory by
+ * `steps` RK4 steps of size dt, without allocating anything.  No counterpart
+ * in the reference.  It is for callers that cannot call cudaMalloc while they
+ * step: code living inside another runtime's device-memory arena, or a
+ * latency-critical loop that must not take cudaMalloc's implicit device
+ * synchronisation.
+ *   d_state: device pointer, 16-byte aligned, to matrices * states * states
+ *            complex doubles in the reference layout (uid order, row-major,
+ *            interleaved re/im); read and overwritten with the result.
+ * The handle's tables are used (create the handle beforehand); the stages use
+ * the product-form RK4 whatever the handle's scheme.  Scratch comes from a
+ * static device array of 3 x 16 MiB built into the library and held on every
+ * GPU that loads it until exit; hierarchies whose state needs more than
+ * 16 MiB in the library's layout are rejected with HEOM_E_UNSUPPORTED.  The
+ * first call on a device resolves the array's device address: make that first
+ * call before any stream capture.  All calls share the array, so calls that
+ * overlap on the GPU (other threads, other handles on the same device) race.
+ * Blocking: returns once the result is in d_state. */
+int heom_rk4_steps_noalloc(heom_handle* h, double* d_state, double dt, int64_t steps);
 /* The handle's CUDA stream (a cudaStream_t), for event timing by callers. */
 void* heom_stream(heom_handle* h);
 
