@@ -78,8 +78,6 @@ __host__ __device__ inline void pair_elements(int n, int p, int* e1, int* e2, in
     }
 }
 
-enum HKind : int { H_REAL_SYM = 0, H_GENERIC = 1 };
-
 struct PairParams {
     const double2* __restrict__ in;  // [nodes][2P] (sector p = double2 pair 2p, 2p+1)
     const double2* y;                // AXPY against y instead of in (may alias out)
@@ -95,40 +93,48 @@ struct PairParams {
     const double2* __restrict__ pss; // [nodes]
     const double* __restrict__ cplus;  // [W][LS]
     const double2* __restrict__ kmin;  // [3][W][LS]: kappa_i, kappa_j, kappa_d
-    const double2* __restrict__ hs;    // [N*N] H / hbar
+    const double2* __restrict__ hs;    // [n_inst][N*N] H / hbar (complex H, SIMT kernel)
+    const double* __restrict__ hr;     // [n_inst][N*(N+1)] real symmetric H / hbar, padded rows (SIMT kernel)
+    const double* __restrict__ hfrag;  // [n_inst][8][32] MMA operand fragments of H / hbar (DMMA kernel)
+    const int32_t* __restrict__ inst;  // [nodes] instance of each ADO; NULL when the handle holds one instance
     const double2* __restrict__ gamma0;// [N*N]
     const int16_t* __restrict__ slots; // [N][SL], -1 padded
     int64_t nodes;
     int W, NW, TWB, LS, SL;
 };
 
+enum HKind : int { H_REAL_SYM = 0, H_GENERIC = 1 };
+
+// bytes of one instance's Hamiltonian as the SIMT kernel stages it
+__host__ __device__ constexpr int pair_h_bytes(int n, int hk) { return hk == H_REAL_SYM ? n * (n + 1) * 8 : n * n * 16; }
+
 // dynamic shared memory carve-up (bytes); everything 16-B aligned
 struct PairSmem {
-    int lut;     // cplus W*LS doubles + kmin 3*W*LS double2 (+ H for generic)
+    int lut;     // kmin 3*W*LS double2 + cplus W*LS doubles
     int team;    // per team: 2 slots
-    int slot;    // per slot: tile + nbr + tup + pss
-    int tile_off, nbr_off, tup_off, pss_off;
+    int slot;    // per slot: tile + nbr + tup + pss + H of the slot's instance
+    int tile_off, nbr_off, tup_off, pss_off, h_off;
 };
 
-__host__ __device__ inline PairSmem pair_smem_layout(int n, int W, int NW, int TWB, int LS)
+__host__ __device__ inline PairSmem pair_smem_layout(int n, int W, int NW, int TWB, int LS, int hk)
 {
     PairSmem s;
-    // 3*W*LS double2 (kappa) + N*N double2 (H) + W*LS double (cplus) + N*(N+1) double (real H)
-    const int lut = 3 * W * LS * 16 + n * n * 16 + W * LS * 8 + n * (n + 1) * 8;
+    const int lut = 3 * W * LS * 16 + W * LS * 8;
     s.lut = (lut + 15) & ~15;
     const int tile = n * (n + 1) * 16;
     s.tile_off = 0;
     s.nbr_off = tile;
     s.tup_off = s.nbr_off + ((NW * 4 + 15) & ~15);
     s.pss_off = s.tup_off + ((TWB + 15) & ~15);
-    s.slot = s.pss_off + 16;
+    s.h_off = s.pss_off + 16;
+    s.slot = s.h_off + ((pair_h_bytes(n, hk) + 15) & ~15);
     s.team = 2 * s.slot;
     return s;
 }
 
-__host__ inline size_t pair_smem_bytes(int n, int W, int NW, int TWB, int LS)
+__host__ inline size_t pair_smem_bytes(int n, int W, int NW, int TWB, int LS, int hk)
 {
-    const PairSmem s = pair_smem_layout(n, W, NW, TWB, LS);
+    const PairSmem s = pair_smem_layout(n, W, NW, TWB, LS, hk);
     const int teams = kCtaWarps / team_warps(n);
     return (size_t)s.lut + (size_t)teams * s.team;
 }
@@ -165,11 +171,19 @@ __device__ __forceinline__ void cmac(double2& acc, const double2 a, const double
 
 __device__ __forceinline__ double2 ldg2(const double2* p) { return __ldg(p); }
 
-// issue the asynchronous copies of ADO u into a team slot
-template <int N>
+// issue the asynchronous copies of ADO u into a team slot; hinst >= 0 also
+// copies the Hamiltonian of instance hinst (the slot holds another instance's)
+template <int N, int HK>
 __device__ __forceinline__ void prefetch_ado(unsigned char* slot, const PairParams& p, const PairSmem& L,
-                                             int64_t u, int lt, int tt, int e1, int e2, bool active)
+                                             int64_t u, int lt, int tt, int e1, int e2, bool active, int hinst)
 {
+    if (hinst >= 0) {
+        constexpr int hb = pair_h_bytes(N, HK);
+        const unsigned char* hsrc =
+            HK == H_REAL_SYM ? reinterpret_cast<const unsigned char*>(p.hr + (size_t)hinst * N * (N + 1))
+                             : reinterpret_cast<const unsigned char*>(p.hs + (size_t)hinst * N * N);
+        for (int q = lt * 16; q < hb; q += tt * 16) cp_async16(slot + L.h_off + q, hsrc + q);
+    }
     double2* tile = reinterpret_cast<double2*>(slot + L.tile_off);
     if (active) {
         const double2* src = p.in + u * (2 * pairs_of(N));
@@ -193,20 +207,14 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_pair_stage(const PairP
     constexpr int TT = 32 * TW;
     constexpr int TEAMS = kCtaWarps / TW;
     extern __shared__ __align__(16) unsigned char smem[];
-    const PairSmem L = pair_smem_layout(N, p.W, p.NW, p.TWB, p.LS);
+    const PairSmem L = pair_smem_layout(N, p.W, p.NW, p.TWB, p.LS, HK);
     const int W = p.W, LS = p.LS, SL = p.SL;
 
     // look-up tables shared by the CTA; 16-byte arrays first (all offsets multiples of 16)
     double2* s_kmin = reinterpret_cast<double2*>(smem);              // 3 * W * LS
-    double2* s_h = s_kmin + 3 * W * LS;                              // N * N, complex H / hbar
-    double* s_cplus = reinterpret_cast<double*>(s_h + N * N);        // W * LS
-    double* s_hr = s_cplus + W * LS;                                 // N * (N+1), real H / hbar
+    double* s_cplus = reinterpret_cast<double*>(s_kmin + 3 * W * LS); // W * LS
     for (int q = threadIdx.x; q < W * LS; q += blockDim.x) s_cplus[q] = p.cplus[q];
     for (int q = threadIdx.x; q < 3 * W * LS; q += blockDim.x) s_kmin[q] = p.kmin[q];
-    if (HK == H_GENERIC)
-        for (int q = threadIdx.x; q < N * N; q += blockDim.x) s_h[q] = p.hs[q];
-    else
-        for (int q = threadIdx.x; q < N * N; q += blockDim.x) s_hr[(q / N) * (N + 1) + q % N] = p.hs[q].x;
 
     const int team = threadIdx.x / TT;
     const int lt = threadIdx.x - team * TT;
@@ -216,9 +224,6 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_pair_stage(const PairP
     int e1 = 0, e2 = 0, i = 0, j = 0, diag = 0;
     if (active) pair_elements(N, lt, &e1, &e2, &i, &j, &diag);
 
-    // rows i and j of a real symmetric H (its columns equal its rows)
-    const double* hri = s_hr + i * (N + 1);
-    const double* hrj = s_hr + j * (N + 1);
     const double2 g1 = active ? p.gamma0[e1] : make_double2(0.0, 0.0);
     const double2 g2 = active ? p.gamma0[e2] : make_double2(0.0, 0.0);
     int sli[SLT], slj[SLT];
@@ -240,16 +245,32 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_pair_stage(const PairP
     const int64_t stride = (int64_t)gridDim.x * TEAMS;
     int64_t u = (int64_t)blockIdx.x * TEAMS + team;
     int cur = 0;
-    if (u < nodes) prefetch_ado<N>(team_base, p, L, u, lt, TT, e1, e2, active);
+    // instance whose Hamiltonian each slot holds (team-uniform)
+    int hin0 = -1, hin1 = -1;
+    if (u < nodes) {
+        const int iu = p.inst ? p.inst[u] : 0;
+        prefetch_ado<N, HK>(team_base, p, L, u, lt, TT, e1, e2, active, iu);
+        hin0 = iu;
+    }
     cp_async_wait_all();
     team_sync<TW>(team);
 
     for (; u < nodes; u += stride) {
         unsigned char* slot = team_base + cur * L.slot;
         const int64_t un = u + stride;
-        if (un < nodes) prefetch_ado<N>(team_base + (cur ^ 1) * L.slot, p, L, un, lt, TT, e1, e2, active);
+        if (un < nodes) {
+            const int iu = p.inst ? p.inst[un] : 0;
+            int& held = cur ? hin0 : hin1;
+            prefetch_ado<N, HK>(team_base + (cur ^ 1) * L.slot, p, L, un, lt, TT, e1, e2, active,
+                                iu != held ? iu : -1);
+            held = iu;
+        }
 
         if (active) {
+            // rows i and j of a real symmetric H (its columns equal its rows), or the complex H
+            const double* hri = reinterpret_cast<const double*>(slot + L.h_off) + i * (N + 1);
+            const double* hrj = reinterpret_cast<const double*>(slot + L.h_off) + j * (N + 1);
+            const double2* s_h = reinterpret_cast<const double2*>(slot + L.h_off);
             const double2* t = reinterpret_cast<const double2*>(slot + L.tile_off);
             const int32_t* nb = reinterpret_cast<const int32_t*>(slot + L.nbr_off);
             const unsigned char* tu = slot + L.tup_off;
@@ -522,7 +543,9 @@ __host__ inline size_t dmma_smem_bytes(int P, int W, int NW, int TWB, int LS)
     return (size_t)dmma_lut_bytes(W, LS) + (size_t)kCtaWarps * dmma_warp_bytes(P, NW, TWB);
 }
 
-template <int N, int HK, int SLT>
+// MI: the handle holds several instances (p.inst set); each ADO's instance
+// selects its H fragments, reloaded whenever the instance changes
+template <int N, int HK, int SLT, bool MI>
 __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_dmma_stage(const DmmaParams dp)
 {
     static_assert(N <= 8, "DMMA stage handles N <= 8");
@@ -563,19 +586,24 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_dmma_stage(const DmmaP
     const int xr1 = 8 * i1 + (j1 ^ swz(i1)), xr2 = 8 * i2 + (j2 ^ swz(i2));
     const int xw0 = 8 * r + ((2 * t) ^ swz(r)), xw1 = 8 * r + ((2 * t + 1) ^ swz(r));
 
-    // operand fragments of H / hbar (zero outside the N x N block)
+    // operand fragments of H / hbar for k-slice s (zero outside the N x N block):
+    //   hb = H(4s+t, r) (B operand of w H), ha = -H(r, 4s+t) (A operand of -H w);
+    // packed per instance as [re hb s0, s1 | im hb | re ha | im ha][lane]
     double hb_r[2], hb_i[2], ha_r[2], ha_i[2];
+    auto load_frag = [&](int ci, double* br, double* bi, double* ar, double* ai) {
+        const double* f = dp.p.hfrag + (size_t)ci * 256 + lane;
 #pragma unroll
-    for (int s = 0; s < 2; ++s) {
-        const int k = 4 * s + t;
-        const bool in = (r < N && k < N);
-        const double2 hkr = in ? p.hs[k * N + r] : make_double2(0.0, 0.0); // B operand of w H: H(k, r)
-        const double2 hrk = in ? p.hs[r * N + k] : make_double2(0.0, 0.0); // A operand of H w: H(r, k)
-        hb_r[s] = hkr.x;
-        hb_i[s] = hkr.y;
-        ha_r[s] = -hrk.x;
-        ha_i[s] = -hrk.y;
-    }
+        for (int s = 0; s < 2; ++s) {
+            br[s] = __ldg(f + 32 * s);
+            ar[s] = __ldg(f + 32 * (4 + s));
+            if (HK == H_GENERIC) {
+                bi[s] = __ldg(f + 32 * (2 + s));
+                ai[s] = __ldg(f + 32 * (6 + s));
+            } else {
+                bi[s] = ai[s] = 0.0;
+            }
+        }
+    };
     const double2 g1 = owner ? p.gamma0[e1] : make_double2(0.0, 0.0);
     const double2 g2 = owner ? p.gamma0[e2] : make_double2(0.0, 0.0);
     int sli[SLT], slj[SLT], pi[SLT], pj[SLT];
@@ -604,6 +632,9 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_dmma_stage(const DmmaP
     const int64_t stride = (int64_t)gridDim.x * kCtaWarps;
     int64_t u = (int64_t)blockIdx.x * kCtaWarps + warp;
     unsigned ph0 = 0u, ph1 = 0u; // mbarrier phase parity of slot 0 / slot 1
+    // instance of the current ADO (warp-uniform); its fragments are in hb_* / ha_*
+    int ci = (MI && u < nodes) ? __ldg(p.inst + u) : 0;
+    load_frag(ci, hb_r, hb_i, ha_r, ha_i);
 
     auto issue = [&](int64_t v, int sl) {
         unsigned char* slot = wbase + sl * slot_b;
@@ -620,6 +651,13 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_dmma_stage(const DmmaP
     for (; u < nodes; u += stride) {
         const int64_t un = u + stride;
         if (un < nodes && lane == 0) issue(un, cur ^ 1);
+        // the next ADO's instance and, when it differs, its fragments (used from the next iteration)
+        int ni = ci;
+        double nb_r[2], nb_i[2], na_r[2], na_i[2];
+        if (MI && un < nodes) {
+            ni = __ldg(p.inst + un);
+            if (ni != ci) load_frag(ni, nb_r, nb_i, na_r, na_i);
+        }
         if (!mbar_wait(&bars[cur], cur ? ph1 : ph0)) {
             failed = true;
             break;
@@ -728,6 +766,16 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_dmma_stage(const DmmaP
         }
         __syncwarp();
         cur ^= 1;
+        if (MI && ni != ci) {
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {
+                hb_r[s] = nb_r[s];
+                hb_i[s] = nb_i[s];
+                ha_r[s] = na_r[s];
+                ha_i[s] = na_i[s];
+            }
+            ci = ni;
+        }
     }
     if (failed) {
         if (lane == 0) atomicExch(dp.err, 1);
@@ -762,58 +810,70 @@ __global__ void heom_weighted_add(const WaddParams p)
 }
 
 // Reference layout (row-major tiles in uid order) <-> pair layout in the
-// internal ADO order.  pe[2p], pe[2p+1] = element indices of the halves of
-// sector p (equal for the padding half).  One thread per (ADO, sector).
-__global__ void heom_to_pairs(double2* __restrict__ dst, const double2* __restrict__ src,
-                              const int64_t* __restrict__ ref_of_int, const int16_t* __restrict__ pe,
-                              int64_t nodes, int n, int P)
+// internal ADO order, over the reference ADOs [r0, r0 + count) whose tiles
+// are (or go) back to back in `ref`.  pe[2p], pe[2p+1] = element indices of
+// the halves of sector p (equal for the padding half).  One thread per
+// (ADO, sector): the pair side is written / read as whole 32-byte sectors.
+__global__ void heom_to_pairs(double2* __restrict__ dst, const double2* __restrict__ ref,
+                              const int64_t* __restrict__ int_of_ref, const int16_t* __restrict__ pe,
+                              int64_t r0, int64_t count, int n, int P)
 {
-    const int64_t total = nodes * P;
+    const int64_t total = count * P;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += stride) {
-        const int64_t u = q / P;
-        const int pr = (int)(q - u * P);
-        const int64_t r = ref_of_int[u] * n * n;
-        dst[2 * q] = src[r + pe[2 * pr]];
-        dst[2 * q + 1] = src[r + pe[2 * pr + 1]];
+        const int64_t r = q / P;
+        const int pr = (int)(q - r * P);
+        const int64_t u = int_of_ref[r0 + r];
+        const double2* src = ref + r * n * n;
+        dst[(u * P + pr) * 2] = src[pe[2 * pr]];
+        dst[(u * P + pr) * 2 + 1] = src[pe[2 * pr + 1]];
     }
 }
 
-__global__ void heom_from_pairs(double2* __restrict__ dst, const double2* __restrict__ src,
-                                const int64_t* __restrict__ ref_of_int, const int16_t* __restrict__ pe,
-                                int64_t nodes, int n, int P)
+__global__ void heom_from_pairs(double2* __restrict__ ref, const double2* __restrict__ src,
+                                const int64_t* __restrict__ int_of_ref, const int16_t* __restrict__ pe,
+                                int64_t r0, int64_t count, int n, int P)
 {
-    const int64_t total = nodes * P;
+    const int64_t total = count * P;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total; q += stride) {
-        const int64_t u = q / P;
-        const int pr = (int)(q - u * P);
-        const int64_t r = ref_of_int[u] * n * n;
+        const int64_t r = q / P;
+        const int pr = (int)(q - r * P);
+        const int64_t u = int_of_ref[r0 + r];
+        double2* dst = ref + r * n * n;
         const int e1 = pe[2 * pr], e2 = pe[2 * pr + 1];
-        dst[r + e1] = src[2 * q];
-        if (e2 != e1) dst[r + e2] = src[2 * q + 1];
+        dst[e1] = src[(u * P + pr) * 2];
+        if (e2 != e1) dst[e2] = src[(u * P + pr) * 2 + 1];
     }
 }
 
-// Copy the top matrix (internal ADO top_int, pair layout) into row `row` of a
-// row-major log.
+// Copy the top matrix of every instance (block k: internal ADO tops[k], pair
+// layout) into row `row` of a row-major log [rows][n_inst][n*n].
 __global__ void heom_record_top(double2* __restrict__ log, const double2* __restrict__ y,
-                                const int16_t* __restrict__ pe, int64_t top_int, int n, int P, int64_t row)
+                                const int16_t* __restrict__ pe, const int64_t* __restrict__ tops, int n, int P,
+                                int64_t row)
 {
+    const int k = blockIdx.x;
+    const int64_t u = tops[k];
+    double2* dst = log + (row * gridDim.x + k) * n * n;
     for (int pr = threadIdx.x; pr < P; pr += blockDim.x) {
         const int e1 = pe[2 * pr], e2 = pe[2 * pr + 1];
-        log[row * n * n + e1] = y[top_int * 2 * P + 2 * pr];
-        if (e2 != e1) log[row * n * n + e2] = y[top_int * 2 * P + 2 * pr + 1];
+        dst[e1] = y[(u * P + pr) * 2];
+        if (e2 != e1) dst[e2] = y[(u * P + pr) * 2 + 1];
     }
 }
 
-// Write a row-major top matrix into the pair layout of ADO top_int.
+// Write row-major top matrices top[k] ([n_inst][n*n]) into the pair layout
+// of each instance's top ADO (block k).
 __global__ void heom_write_top(double2* __restrict__ y, const double2* __restrict__ top,
-                               const int16_t* __restrict__ pe, int64_t top_int, int P)
+                               const int16_t* __restrict__ pe, const int64_t* __restrict__ tops, int n, int P)
 {
+    const int k = blockIdx.x;
+    const int64_t u = tops[k];
+    const double2* src = top + (int64_t)k * n * n;
     for (int pr = threadIdx.x; pr < P; pr += blockDim.x) {
-        y[top_int * 2 * P + 2 * pr] = top[pe[2 * pr]];
-        y[top_int * 2 * P + 2 * pr + 1] = top[pe[2 * pr + 1]];
+        y[(u * P + pr) * 2] = src[pe[2 * pr]];
+        y[(u * P + pr) * 2 + 1] = src[pe[2 * pr + 1]];
     }
 }
 

@@ -122,28 +122,35 @@ stage_fn_t pick_stage(int n, int hk, int slt)
     }
 }
 
-template <int N, int HK>
+template <int N, int HK, bool MI>
 dmma_fn_t pick_dslt(int slt)
 {
     switch (slt) {
-    case 2: return heomk::heom_dmma_stage<N, HK, 2>;
-    case 4: return heomk::heom_dmma_stage<N, HK, 4>;
-    default: return heomk::heom_dmma_stage<N, HK, 8>;
+    case 2: return heomk::heom_dmma_stage<N, HK, 2, MI>;
+    case 4: return heomk::heom_dmma_stage<N, HK, 4, MI>;
+    default: return heomk::heom_dmma_stage<N, HK, 8, MI>;
     }
 }
 
-template <int N>
-dmma_fn_t pick_dn(int hk, int slt)
+template <int N, bool MI>
+dmma_fn_t pick_dhk(int hk, int slt)
 {
-    return hk == heomk::H_REAL_SYM ? pick_dslt<N, heomk::H_REAL_SYM>(slt) : pick_dslt<N, heomk::H_GENERIC>(slt);
+    return hk == heomk::H_REAL_SYM ? pick_dslt<N, heomk::H_REAL_SYM, MI>(slt)
+                                   : pick_dslt<N, heomk::H_GENERIC, MI>(slt);
+}
+
+template <int N>
+dmma_fn_t pick_dn(int hk, int slt, bool multi)
+{
+    return multi ? pick_dhk<N, true>(hk, slt) : pick_dhk<N, false>(hk, slt);
 }
 
 // tensor-pipe kernel: N = 1..8
-dmma_fn_t pick_dmma(int n, int hk, int slt)
+dmma_fn_t pick_dmma(int n, int hk, int slt, bool multi)
 {
     switch (n) {
 #define HEOM_CASE(K) \
-    case K: return pick_dn<K>(hk, slt);
+    case K: return pick_dn<K>(hk, slt, multi);
         HEOM_CASE(1) HEOM_CASE(2) HEOM_CASE(3) HEOM_CASE(4) HEOM_CASE(5) HEOM_CASE(6)
         HEOM_CASE(7) HEOM_CASE(8)
 #undef HEOM_CASE
@@ -188,32 +195,41 @@ struct heom_handle {
     cudaStream_t stream = nullptr;
     int sm_count = 0;
 
-    // instance sizes
-    int N = 0, M = 0, B = 0, BPS = 0, W = 0, D = 0;
-    int64_t nodes = 0;
-    int32_t first_non_plus = 0;
+    // sizes shared by every instance of the handle
+    int N = 0, M = 0, B = 0, BPS = 0, W = 0, D = 0; // D = largest depth
+    int64_t nodes = 0;                              // ADOs of all instances
     int LS = 0, SL = 0, SLT = 2;
     int P = 0;          // 32-byte sectors per ADO (pair layout)
     int NW = 0, TWB = 0; // padded widths of the neighbour and tuple rows
     int hkind = heomk::H_REAL_SYM;
 
-    // host copies in reference layout
+    // instances: ADOs [inst_base[k], inst_base[k+1]) in both the reference
+    // and the internal order belong to instance k
+    int n_inst = 1;
+    std::vector<int64_t> inst_base;
+    std::vector<int32_t> inst_depth, inst_fnp; // depth and first_non_plus_id per instance
+
+    // host copies in reference layout, instances back to back (plus / minus
+    // hold indices into the concatenation)
     std::vector<int32_t> coupling, tuples, plus, minus;
     std::vector<double> ham, pss, pf_same, pf_circ, cbk, cbk_sqrt;
     std::vector<uint8_t> mask;
     std::vector<int64_t> int_of_ref, ref_of_int;
-    int64_t top_int = 0;
+    std::vector<int64_t> top_int; // internal index of each instance's top ADO
 
     // device tables
     DevBuf<int32_t> d_nbr;
     DevBuf<uint8_t> d_tup;
     DevBuf<double2> d_pss, d_kmin, d_hs, d_gamma0;
+    DevBuf<double> d_hr, d_hfrag;    // per-instance H for the SIMT / DMMA kernels
+    DevBuf<int32_t> d_inst;          // instance of each internal ADO (n_inst > 1)
+    DevBuf<int64_t> d_top;
     DevBuf<double> d_cplus;
     DevBuf<int16_t> d_slots;
     DevBuf<double> d_chat, d_sq;     // factored coefficients (DMMA kernel)
     DevBuf<double2> d_khat;
     DevBuf<int16_t> d_pos;
-    DevBuf<int64_t> d_ref_of_int;
+    DevBuf<int64_t> d_int_of_ref;
     DevBuf<int16_t> d_pair;          // [P][2] element indices of the sector halves
     std::vector<int16_t> pair_tab;   // host copy
     heomk::LaneTab lane_tab{};       // DMMA kernel lane tables (N <= 8)
@@ -222,14 +238,16 @@ struct heom_handle {
     // propagation state + stage buffers
     heom_buffer y;
     DevBuf<double2> work[5];
-    DevBuf<double2> xfer;   // reference-layout staging buffer for host transfers
+    DevBuf<double2> xfer;   // reference-layout staging buffer for host transfers (xfer_ados ADOs)
+    int64_t xfer_ados = 0;
     DevBuf<double2> toplog;
-    DevBuf<double2> topbuf; // one row-major top matrix
+    DevBuf<double2> topbuf; // row-major top matrices of all instances
     DevBuf<int> d_flag;
 
-    // launch accounting
+    // launch accounting and shape
     int64_t launches = 0;
-    int stage_blocks[2] = {0, 0}; // per H kind
+    int per_sm[2] = {0, 0};  // resident stage CTAs per SM, per H kind
+    int grid_override = 0;   // stage grid chosen by an autotuner (0: one full wave)
     size_t stage_smem = 0;
 
     // cached graph of one RK4 step
@@ -251,45 +269,75 @@ int build_neighbours(heom_handle* h)
     std::vector<int32_t> nbr((size_t)h->nodes * NW, -1);
     std::vector<uint8_t> tup((size_t)h->nodes * TWB, 0);
     std::vector<double2> pss(h->nodes);
-    for (int64_t u = 0; u < h->nodes; ++u) {
-        const int64_t r = h->ref_of_int[u];
-        for (int m = 0; m < W; ++m) {
-            const int32_t t = h->tuples[r * W + m];
-            tup[u * TWB + m] = (uint8_t)t;
-            int32_t pv = -1, mv = -1;
-            const int32_t pr = h->plus[r * W + m];
-            if (r < h->first_non_plus && pr >= 0 && h->mask[pr]) pv = (int32_t)h->int_of_ref[pr];
-            const int32_t mr = h->minus[r * W + m];
-            if (t > 0 && mr >= 0 && h->mask[mr]) mv = (int32_t)h->int_of_ref[mr];
-            nbr[u * NW + m] = pv;
-            nbr[u * NW + W + m] = mv;
+    std::vector<int32_t> inst(h->n_inst > 1 ? h->nodes : 0);
+    for (int k = 0; k < h->n_inst; ++k) {
+        const int64_t base = h->inst_base[k];
+        for (int64_t r = base; r < h->inst_base[k + 1]; ++r) {
+            const int64_t u = h->int_of_ref[r];
+            const bool has_plus = r - base < h->inst_fnp[k];
+            for (int m = 0; m < W; ++m) {
+                const int32_t t = h->tuples[r * W + m];
+                tup[u * TWB + m] = (uint8_t)t;
+                int32_t pv = -1, mv = -1;
+                const int32_t pr = h->plus[r * W + m];
+                if (has_plus && pr >= 0 && h->mask[pr]) pv = (int32_t)h->int_of_ref[pr];
+                const int32_t mr = h->minus[r * W + m];
+                if (t > 0 && mr >= 0 && h->mask[mr]) mv = (int32_t)h->int_of_ref[mr];
+                nbr[u * NW + m] = pv;
+                nbr[u * NW + W + m] = mv;
+            }
+            pss[u] = make_double2(h->pss[2 * r], h->pss[2 * r + 1]);
+            if (h->n_inst > 1) inst[u] = k;
         }
-        pss[u] = make_double2(h->pss[2 * r], h->pss[2 * r + 1]);
     }
     if (!h->d_nbr.p) {
         if (int rc = h->d_nbr.alloc(nbr.size())) return rc;
         if (int rc = h->d_tup.alloc(tup.size())) return rc;
         if (int rc = h->d_pss.alloc(pss.size())) return rc;
+        if (h->n_inst > 1)
+            if (int rc = h->d_inst.alloc(inst.size())) return rc;
     }
     CUDA_TRY(cudaMemcpy(h->d_nbr.p, nbr.data(), nbr.size() * 4, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(h->d_tup.p, tup.data(), tup.size(), cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(h->d_pss.p, pss.data(), pss.size() * 16, cudaMemcpyHostToDevice));
+    if (h->n_inst > 1) CUDA_TRY(cudaMemcpy(h->d_inst.p, inst.data(), inst.size() * 4, cudaMemcpyHostToDevice));
     return 0;
 }
 
 int upload_hamiltonian(heom_handle* h)
 {
-    const int N = h->N;
-    std::vector<double2> hs(N * N), g0(N * N);
+    const int N = h->N, K = h->n_inst;
+    std::vector<double2> hs((size_t)K * N * N), g0(N * N);
+    std::vector<double> hr((size_t)K * N * (N + 1), 0.0);
+    std::vector<double> frag(N <= 8 ? (size_t)K * 256 : 0, 0.0);
     bool real_sym = true;
-    for (int q = 0; q < N * N; ++q) {
-        hs[q] = make_double2(h->ham[2 * q] / kHbar, h->ham[2 * q + 1] / kHbar);
-        if (h->ham[2 * q + 1] != 0.0) real_sym = false;
+    for (int k = 0; k < K; ++k) {
+        const double* hk = h->ham.data() + (size_t)k * 2 * N * N;
+        for (int q = 0; q < N * N; ++q) {
+            hs[(size_t)k * N * N + q] = make_double2(hk[2 * q] / kHbar, hk[2 * q + 1] / kHbar);
+            if (hk[2 * q + 1] != 0.0) real_sym = false;
+            hr[(size_t)k * N * (N + 1) + (q / N) * (N + 1) + q % N] = hk[2 * q] / kHbar;
+        }
+        for (int i = 0; i < N && real_sym; ++i)
+            for (int j = 0; j < i; ++j)
+                if (hk[2 * (i * N + j)] != hk[2 * (j * N + i)]) real_sym = false;
+        // MMA operand fragments, lane l = 4r + t, k-slice s: column 4s+t
+        for (int l = 0; l < 32 && N <= 8; ++l) {
+            const int r = l >> 2, t = l & 3;
+            for (int sl = 0; sl < 2; ++sl) {
+                const int c = 4 * sl + t;
+                if (r >= N || c >= N) continue;
+                const double2 hcr = hs[(size_t)k * N * N + c * N + r]; // H(c, r)
+                const double2 hrc = hs[(size_t)k * N * N + r * N + c]; // H(r, c)
+                double* f = frag.data() + (size_t)k * 256 + l;
+                f[32 * (0 + sl)] = hcr.x;
+                f[32 * (2 + sl)] = hcr.y;
+                f[32 * (4 + sl)] = -hrc.x;
+                f[32 * (6 + sl)] = -hrc.y;
+            }
+        }
     }
-    for (int i = 0; i < N && real_sym; ++i)
-        for (int j = 0; j < i; ++j)
-            if (h->ham[2 * (i * N + j)] != h->ham[2 * (j * N + i)]) real_sym = false;
-    // real symmetric H keeps rows i, j in registers; anything else reads H from shared memory
+    // real symmetric H (every instance) takes the cheaper kernel variants
     h->hkind = real_sym ? heomk::H_REAL_SYM : heomk::H_GENERIC;
     // same term (heom_ode.cl:138-168): for i != j subtract pf_same of every
     // bath coupled to site i and to site j
@@ -306,10 +354,14 @@ int upload_hamiltonian(heom_handle* h)
             g0[i * N + j] = make_double2(gr, gi);
         }
     if (!h->d_hs.p) {
-        if (int rc = h->d_hs.alloc(N * N)) return rc;
+        if (int rc = h->d_hs.alloc(hs.size())) return rc;
+        if (int rc = h->d_hr.alloc(hr.size())) return rc;
+        if (int rc = h->d_hfrag.alloc(frag.size())) return rc;
         if (int rc = h->d_gamma0.alloc(N * N)) return rc;
     }
     CUDA_TRY(cudaMemcpy(h->d_hs.p, hs.data(), hs.size() * 16, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(h->d_hr.p, hr.data(), hr.size() * 8, cudaMemcpyHostToDevice));
+    if (!frag.empty()) CUDA_TRY(cudaMemcpy(h->d_hfrag.p, frag.data(), frag.size() * 8, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(h->d_gamma0.p, g0.data(), g0.size() * 16, cudaMemcpyHostToDevice));
     // the kernel variant may change: rebuild the cached step graph
     if (h->step_graph) {
@@ -398,6 +450,9 @@ PairParams base_params(const heom_handle* h)
     p.cplus = h->d_cplus.p;
     p.kmin = h->d_kmin.p;
     p.hs = h->d_hs.p;
+    p.hr = h->d_hr.p;
+    p.hfrag = h->d_hfrag.p;
+    p.inst = h->n_inst > 1 ? h->d_inst.p : nullptr;
     p.gamma0 = h->d_gamma0.p;
     p.slots = h->d_slots.p;
     p.nodes = h->nodes;
@@ -409,36 +464,58 @@ PairParams base_params(const heom_handle* h)
     return p;
 }
 
+// The dynamic shared-memory limit is an attribute of the kernel function,
+// shared by every handle that launches it (with its own sizes): it only grows.
+std::mutex g_smem_mu;
+std::vector<std::pair<int, std::pair<const void*, size_t>>> g_smem_allowed; // (device, (function, bytes))
+
+int allow_dynamic_smem(const void* fn, size_t smem)
+{
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(g_smem_mu);
+    for (auto& e : g_smem_allowed)
+        if (e.first == dev && e.second.first == fn) {
+            if (e.second.second >= smem) return 0;
+            CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            e.second.second = smem;
+            return 0;
+        }
+    CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    g_smem_allowed.push_back({dev, {fn, smem}});
+    return 0;
+}
+
 int cta_threads(int n) { return (heomk::kCtaWarps / heomk::team_warps(n)) * heomk::team_warps(n) * 32; }
 int cta_teams(int n) { return heomk::kCtaWarps / heomk::team_warps(n); }
 
 // resolve the launch shape of the stage kernel (outside of any stream capture)
-int resolve_stage(heom_handle* h, const void** fn_out)
+int resolve_stage(heom_handle* h, const void** fn_out, int* blocks_out = nullptr)
 {
     const void* fn = nullptr;
     size_t smem = 0;
     int threads = 0;
     if (h->N <= 8) {
-        fn = (const void*)pick_dmma(h->N, h->hkind, h->SLT);
+        fn = (const void*)pick_dmma(h->N, h->hkind, h->SLT, h->n_inst > 1);
         smem = heomk::dmma_smem_bytes(h->P, h->W, h->NW, h->TWB, h->LS);
         threads = heomk::kCtaWarps * 32;
     } else {
         fn = (const void*)pick_stage(h->N, h->hkind, h->SLT);
-        smem = heomk::pair_smem_bytes(h->N, h->W, h->NW, h->TWB, h->LS);
+        smem = heomk::pair_smem_bytes(h->N, h->W, h->NW, h->TWB, h->LS, h->hkind);
         threads = cta_threads(h->N);
     }
     if (!fn) return fail(HEOM_E_UNSUPPORTED, "states = %d not supported", h->N);
-    int& blocks = h->stage_blocks[h->hkind];
-    if (blocks == 0) {
+    int& per_sm = h->per_sm[h->hkind];
+    if (per_sm == 0) {
         if (smem > 227 * 1024) return fail(HEOM_E_UNSUPPORTED, "stage kernel needs %zu B of shared memory", smem);
-        CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        int per_sm = 0;
+        if (int rc = allow_dynamic_smem(fn, smem)) return rc;
         CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
         if (per_sm < 1) return fail(HEOM_E_UNSUPPORTED, "stage kernel cannot be resident");
-        const int teams = h->N <= 8 ? heomk::kCtaWarps : cta_teams(h->N);
-        const int64_t groups = (h->nodes + teams - 1) / teams;
-        blocks = (int)std::min<int64_t>(groups, (int64_t)per_sm * h->sm_count);
     }
+    const int teams = h->N <= 8 ? heomk::kCtaWarps : cta_teams(h->N);
+    const int64_t groups = (h->nodes + teams - 1) / teams;
+    const int64_t want = h->grid_override > 0 ? h->grid_override : (int64_t)per_sm * h->sm_count;
+    if (blocks_out) *blocks_out = (int)std::max<int64_t>(1, std::min<int64_t>(groups, want));
     h->stage_smem = smem;
     *fn_out = fn;
     return 0;
@@ -448,7 +525,8 @@ int launch_stage(heom_handle* h, int epi, const double2* in, const double2* y, d
                  double2* acc, double2 beta, int acc_init)
 {
     const void* fn = nullptr;
-    if (int rc = resolve_stage(h, &fn)) return rc;
+    int blocks = 0;
+    if (int rc = resolve_stage(h, &fn, &blocks)) return rc;
     PairParams p = base_params(h);
     p.in = in;
     p.out = out;
@@ -475,7 +553,6 @@ int launch_stage(heom_handle* h, int epi, const double2* in, const double2* y, d
         p.acc_init = acc_init;
         break;
     }
-    const int blocks = h->stage_blocks[h->hkind];
     if (h->N <= 8) {
         heomk::DmmaParams dp;
         dp.p = p;
@@ -517,8 +594,10 @@ int launch_wadd(heom_handle* h, int n, double step, double2* out, const double2*
 int ensure_work(heom_handle* h, int count)
 {
     for (int q = 0; q < count; ++q)
-        if (!h->work[q].p)
+        if (!h->work[q].p) {
             if (int rc = h->work[q].alloc(h->state_elems())) return rc;
+            CUDA_TRY(cudaMemset(h->work[q].p, 0, h->state_elems() * sizeof(double2)));
+        }
     return 0;
 }
 
@@ -659,6 +738,24 @@ int check_desc(const heom_instance_desc* d)
     return 0;
 }
 
+// instances of one handle share states, baths, their coupling and bath
+// tables; depth, hierarchy tables and Hamiltonian may differ
+int check_same_class(const heom_instance_desc* a, const heom_instance_desc* b)
+{
+    if (a->states != b->states || a->matsubaras != b->matsubaras || a->baths != b->baths ||
+        a->baths_per_state != b->baths_per_state || a->ado_width != b->ado_width)
+        return fail(HEOM_E_ARG, "sizes differ");
+    auto same = [](const void* x, const void* y, size_t bytes) { return std::memcmp(x, y, bytes) == 0; };
+    if (!same(a->baths_coupling, b->baths_coupling, sizeof(int32_t) * a->states * a->baths_per_state))
+        return fail(HEOM_E_ARG, "baths_coupling differs");
+    if (!same(a->pf_same, b->pf_same, sizeof(double) * 2 * a->baths) ||
+        !same(a->pf_circ, b->pf_circ, sizeof(double) * 2 * a->baths) ||
+        !same(a->cbk, b->cbk, sizeof(double) * 2 * a->baths * a->matsubaras) ||
+        !same(a->cbk_sqrt, b->cbk_sqrt, sizeof(double) * a->baths * a->matsubaras))
+        return fail(HEOM_E_ARG, "bath tables differ");
+    return 0;
+}
+
 // sector tables of the pair layout: the searched order for N <= 8
 // (pair_tables.inc), the canonical order of heomk::pair_elements above
 int build_pair_tables(heom_handle* h)
@@ -701,30 +798,31 @@ int build_pair_tables(heom_handle* h)
     return 0;
 }
 
-// internal order: lexicographic rank of the tuple when the tuples form the
-// complete hierarchy, else the reference order
+// internal order, per instance: lexicographic rank of the tuple when the
+// instance's tuples form the complete hierarchy, else the reference order
 void build_order(heom_handle* h)
 {
-    const int W = h->W, D = h->D;
-    const int64_t nodes = h->nodes;
-    h->int_of_ref.assign(nodes, 0);
-    h->ref_of_int.assign(nodes, 0);
-    bool lex = h->opt.ado_order == HEOM_ORDER_LEX;
-    if (lex) {
-        std::vector<std::vector<int64_t>> binom(W + D + 2, std::vector<int64_t>(W + 2, 0));
-        for (int a = 0; a < W + D + 2; ++a) {
-            binom[a][0] = 1;
-            for (int b = 1; b <= std::min(a, W + 1); ++b)
-                binom[a][b] = binom[a - 1][b - 1] + (b <= a - 1 ? binom[a - 1][b] : 0);
-        }
-        if (binom[W + D][W] != nodes) lex = false;
+    const int W = h->W;
+    h->int_of_ref.assign(h->nodes, 0);
+    h->ref_of_int.assign(h->nodes, 0);
+    h->top_int.assign(h->n_inst, 0);
+    std::vector<std::vector<int64_t>> binom(W + h->D + 2, std::vector<int64_t>(W + 2, 0));
+    for (int a = 0; a < W + h->D + 2; ++a) {
+        binom[a][0] = 1;
+        for (int b = 1; b <= std::min(a, W + 1); ++b)
+            binom[a][b] = binom[a - 1][b - 1] + (b <= a - 1 ? binom[a - 1][b] : 0);
+    }
+    for (int k = 0; k < h->n_inst; ++k) {
+        const int D = h->inst_depth[k];
+        const int64_t base = h->inst_base[k], nodes = h->inst_base[k + 1] - base;
+        bool lex = h->opt.ado_order == HEOM_ORDER_LEX && binom[W + D][W] == nodes;
         std::vector<char> seen(lex ? nodes : 0, 0);
         for (int64_t r = 0; lex && r < nodes; ++r) {
             int64_t rank = 0;
             int prefix = 0;
-            for (int k = 0; k < W; ++k) {
-                const int t = h->tuples[r * W + k];
-                for (int x = 0; x < t; ++x) rank += simplex_count(W - 1 - k, D - prefix - x, binom);
+            for (int m = 0; m < W; ++m) {
+                const int t = h->tuples[(base + r) * W + m];
+                for (int x = 0; x < t; ++x) rank += simplex_count(W - 1 - m, D - prefix - x, binom);
                 prefix += t;
             }
             if (prefix > D || rank < 0 || rank >= nodes || seen[rank]) {
@@ -732,39 +830,50 @@ void build_order(heom_handle* h)
                 break;
             }
             seen[rank] = 1;
-            h->int_of_ref[r] = rank;
+            h->int_of_ref[base + r] = base + rank;
         }
+        if (!lex)
+            for (int64_t r = 0; r < nodes; ++r) h->int_of_ref[base + r] = base + r;
+        h->top_int[k] = h->int_of_ref[base];
     }
-    if (!lex)
-        for (int64_t r = 0; r < nodes; ++r) h->int_of_ref[r] = r;
-    for (int64_t r = 0; r < nodes; ++r) h->ref_of_int[h->int_of_ref[r]] = r;
-    h->top_int = h->int_of_ref[0];
+    for (int64_t r = 0; r < h->nodes; ++r) h->ref_of_int[h->int_of_ref[r]] = r;
 }
 
+int conv_blocks(const heom_handle* h, int64_t count)
+{
+    const int64_t total = count * h->P;
+    return (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, (int64_t)h->sm_count * 16));
+}
+
+// host reference-layout state (all instances) -> pair layout, in chunks of xfer_ados ADOs
 int to_internal(heom_handle* h, double2* dst, const double* host)
 {
-    const size_t bytes = h->ref_elems() * sizeof(double2);
-    CUDA_TRY(cudaMemcpyAsync(h->xfer.p, host, bytes, cudaMemcpyHostToDevice, h->stream));
-    const int64_t total = h->nodes * h->P;
-    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, h->sm_count * 16));
-    heomk::heom_to_pairs<<<blocks, 256, 0, h->stream>>>(dst, h->xfer.p, h->d_ref_of_int.p, h->d_pair.p, h->nodes,
-                                                         h->N, h->P);
-    h->launches++;
-    CUDA_TRY(cudaGetLastError());
+    const int64_t nn = (int64_t)h->N * h->N;
+    for (int64_t r0 = 0; r0 < h->nodes; r0 += h->xfer_ados) {
+        const int64_t count = std::min<int64_t>(h->xfer_ados, h->nodes - r0);
+        CUDA_TRY(cudaMemcpyAsync(h->xfer.p, host + r0 * nn * 2, count * nn * sizeof(double2),
+                                 cudaMemcpyHostToDevice, h->stream));
+        heomk::heom_to_pairs<<<conv_blocks(h, count), 256, 0, h->stream>>>(dst, h->xfer.p, h->d_int_of_ref.p,
+                                                                             h->d_pair.p, r0, count, h->N, h->P);
+        h->launches++;
+        CUDA_TRY(cudaGetLastError());
+    }
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     return 0;
 }
 
 int from_internal(heom_handle* h, double* host, const double2* src)
 {
-    const size_t bytes = h->ref_elems() * sizeof(double2);
-    const int64_t total = h->nodes * h->P;
-    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, h->sm_count * 16));
-    heomk::heom_from_pairs<<<blocks, 256, 0, h->stream>>>(h->xfer.p, src, h->d_ref_of_int.p, h->d_pair.p, h->nodes,
-                                                           h->N, h->P);
-    h->launches++;
-    CUDA_TRY(cudaGetLastError());
-    CUDA_TRY(cudaMemcpyAsync(host, h->xfer.p, bytes, cudaMemcpyDeviceToHost, h->stream));
+    const int64_t nn = (int64_t)h->N * h->N;
+    for (int64_t r0 = 0; r0 < h->nodes; r0 += h->xfer_ados) {
+        const int64_t count = std::min<int64_t>(h->xfer_ados, h->nodes - r0);
+        heomk::heom_from_pairs<<<conv_blocks(h, count), 256, 0, h->stream>>>(h->xfer.p, src, h->d_int_of_ref.p,
+                                                                               h->d_pair.p, r0, count, h->N, h->P);
+        h->launches++;
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaMemcpyAsync(host + r0 * nn * 2, h->xfer.p, count * nn * sizeof(double2),
+                                 cudaMemcpyDeviceToHost, h->stream));
+    }
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     return 0;
 }
@@ -834,9 +943,24 @@ void heom_default_options(heom_options* opt)
 
 int heom_create(const heom_instance_desc* d, const heom_options* opt, heom_handle** out)
 {
+    return heom_create_batch(d, 1, opt, out);
+}
+
+int heom_create_batch(const heom_instance_desc* descs, int32_t count, const heom_options* opt, heom_handle** out)
+{
     if (!out) return fail(HEOM_E_ARG, "out is NULL");
     *out = nullptr;
-    if (int rc = check_desc(d)) return rc;
+    if (!descs || count < 1) return fail(HEOM_E_ARG, "descs is NULL or count < 1");
+    for (int k = 0; k < count; ++k) {
+        if (int rc = check_desc(&descs[k])) {
+            if (count > 1) g_last_error = "instance " + std::to_string(k) + ": " + g_last_error;
+            return rc;
+        }
+        if (int rc = check_same_class(&descs[0], &descs[k]))
+            return fail(rc, "instance %d does not share states, baths and Matsubara terms with instance 0: %s", k,
+                        g_last_error.c_str());
+    }
+    const heom_instance_desc* d = &descs[0];
     std::unique_ptr<heom_handle> h(new heom_handle());
     heom_default_options(&h->opt);
     if (opt) h->opt = *opt;
@@ -858,9 +982,18 @@ int heom_create(const heom_instance_desc* d, const heom_options* opt, heom_handl
     h->B = d->baths;
     h->BPS = d->baths_per_state;
     h->W = d->ado_width;
-    h->D = d->ado_depth;
-    h->nodes = d->matrices;
-    h->first_non_plus = d->first_non_plus_id;
+    h->n_inst = count;
+    h->inst_base.assign(count + 1, 0);
+    h->D = 0;
+    for (int k = 0; k < count; ++k) {
+        h->inst_base[k + 1] = h->inst_base[k] + descs[k].matrices;
+        h->inst_depth.push_back(descs[k].ado_depth);
+        h->inst_fnp.push_back(descs[k].first_non_plus_id);
+        h->D = std::max(h->D, descs[k].ado_depth);
+    }
+    h->nodes = h->inst_base[count];
+    if (h->nodes > INT32_MAX) return fail(HEOM_E_UNSUPPORTED, "%lld ADOs in one handle (at most 2^31 - 1)",
+                                          (long long)h->nodes);
     h->LS = h->D + 1;
     h->SL = h->BPS * h->M;
     if (h->SL > 8) return fail(HEOM_E_UNSUPPORTED, "baths_per_state * matsubaras = %d > 8", h->SL);
@@ -868,17 +1001,28 @@ int heom_create(const heom_instance_desc* d, const heom_options* opt, heom_handl
     h->P = heomk::pairs_of(h->N);
     h->NW = (2 * h->W + 3) & ~3;
     h->TWB = (h->W + 15) & ~15;
-    const int64_t nw = h->nodes * h->W;
+    const int W = h->W;
     h->coupling.assign(d->baths_coupling, d->baths_coupling + h->N * h->BPS);
-    h->tuples.assign(d->ado_tuples, d->ado_tuples + nw);
-    h->plus.assign(d->ado_plus, d->ado_plus + nw);
-    h->minus.assign(d->ado_minus, d->ado_minus + nw);
-    h->ham.assign(d->hamiltonian, d->hamiltonian + 2 * h->N * h->N);
-    h->pss.assign(d->pf_same_sum, d->pf_same_sum + 2 * h->nodes);
     h->pf_same.assign(d->pf_same, d->pf_same + 2 * h->B);
     h->pf_circ.assign(d->pf_circ, d->pf_circ + 2 * h->B);
     h->cbk.assign(d->cbk, d->cbk + 2 * h->B * h->M);
     h->cbk_sqrt.assign(d->cbk_sqrt, d->cbk_sqrt + h->B * h->M);
+    h->tuples.resize((size_t)h->nodes * W);
+    h->plus.resize((size_t)h->nodes * W);
+    h->minus.resize((size_t)h->nodes * W);
+    h->pss.resize((size_t)h->nodes * 2);
+    h->ham.resize((size_t)count * 2 * h->N * h->N);
+    for (int k = 0; k < count; ++k) {
+        const heom_instance_desc* e = &descs[k];
+        const int64_t base = h->inst_base[k], nw = e->matrices * W;
+        std::copy(e->ado_tuples, e->ado_tuples + nw, h->tuples.begin() + base * W);
+        for (int64_t q = 0; q < nw; ++q) {
+            h->plus[base * W + q] = e->ado_plus[q] == HEOM_INVALID_UID ? -1 : (int32_t)(base + e->ado_plus[q]);
+            h->minus[base * W + q] = e->ado_minus[q] == HEOM_INVALID_UID ? -1 : (int32_t)(base + e->ado_minus[q]);
+        }
+        std::copy(e->pf_same_sum, e->pf_same_sum + 2 * e->matrices, h->pss.begin() + 2 * base);
+        std::copy(e->hamiltonian, e->hamiltonian + 2 * h->N * h->N, h->ham.begin() + (size_t)k * 2 * h->N * h->N);
+    }
     h->mask.assign(h->nodes, 1);
     for (int q = 0; q < h->B * h->M; ++q)
         if (!(std::hypot(h->cbk[2 * q], h->cbk[2 * q + 1]) > 0.0))
@@ -886,8 +1030,10 @@ int heom_create(const heom_instance_desc* d, const heom_options* opt, heom_handl
 
     if (int rc = build_pair_tables(h.get())) return rc;
     build_order(h.get());
-    if (int rc = h->d_ref_of_int.alloc(h->nodes)) return rc;
-    CUDA_TRY(cudaMemcpy(h->d_ref_of_int.p, h->ref_of_int.data(), h->nodes * 8, cudaMemcpyHostToDevice));
+    if (int rc = h->d_int_of_ref.alloc(h->nodes)) return rc;
+    CUDA_TRY(cudaMemcpy(h->d_int_of_ref.p, h->int_of_ref.data(), h->nodes * 8, cudaMemcpyHostToDevice));
+    if (int rc = h->d_top.alloc(count)) return rc;
+    CUDA_TRY(cudaMemcpy(h->d_top.p, h->top_int.data(), count * 8, cudaMemcpyHostToDevice));
     if (int rc = build_neighbours(h.get())) return rc;
     if (int rc = upload_coefficients(h.get())) return rc;
     if (int rc = upload_hamiltonian(h.get())) return rc;
@@ -895,8 +1041,11 @@ int heom_create(const heom_instance_desc* d, const heom_options* opt, heom_handl
     h->y.borrowed = true;
     if (int rc = h->y.data.alloc(h->state_elems())) return rc;
     CUDA_TRY(cudaMemset(h->y.data.p, 0, h->state_elems() * sizeof(double2)));
-    if (int rc = h->xfer.alloc(h->ref_elems())) return rc;
-    if (int rc = h->topbuf.alloc((size_t)h->N * h->N)) return rc;
+    // host transfers go through a staging buffer of at most 64 MiB
+    const int64_t nn = (int64_t)h->N * h->N;
+    h->xfer_ados = std::max<int64_t>(1, std::min<int64_t>(h->nodes, (int64_t(64) << 20) / (nn * 16)));
+    if (int rc = h->xfer.alloc((size_t)h->xfer_ados * nn)) return rc;
+    if (int rc = h->topbuf.alloc((size_t)count * nn)) return rc;
     if (int rc = h->d_flag.alloc(1)) return rc;
     if (int rc = h->d_err.alloc(1)) return rc;
     CUDA_TRY(cudaMemset(h->d_err.p, 0, sizeof(int)));
@@ -921,7 +1070,18 @@ int heom_set_hamiltonian(heom_handle* h, const double* ham)
     if (!h || !ham) return fail(HEOM_E_ARG, "NULL argument");
     CUDA_TRY(cudaSetDevice(h->device));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
-    h->ham.assign(ham, ham + 2 * h->N * h->N);
+    h->ham.assign(ham, ham + (size_t)h->n_inst * 2 * h->N * h->N);
+    return upload_hamiltonian(h);
+}
+
+int heom_set_instance_hamiltonian(heom_handle* h, int32_t inst, const double* ham)
+{
+    if (!h || !ham) return fail(HEOM_E_ARG, "NULL argument");
+    if (inst < 0 || inst >= h->n_inst) return fail(HEOM_E_ARG, "instance %d out of range", inst);
+    CUDA_TRY(cudaSetDevice(h->device));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    const size_t nn2 = (size_t)2 * h->N * h->N;
+    std::copy(ham, ham + nn2, h->ham.begin() + inst * nn2);
     return upload_hamiltonian(h);
 }
 
@@ -1037,9 +1197,10 @@ int heom_set_top(heom_handle* h, const double* top)
 {
     if (!h || !top) return fail(HEOM_E_ARG, "NULL argument");
     CUDA_TRY(cudaSetDevice(h->device));
-    const size_t nn = (size_t)h->N * h->N;
+    const size_t nn = (size_t)h->N * h->N * h->n_inst;
     CUDA_TRY(cudaMemcpyAsync(h->topbuf.p, top, nn * 16, cudaMemcpyHostToDevice, h->stream));
-    heomk::heom_write_top<<<1, 128, 0, h->stream>>>(h->y.data.p, h->topbuf.p, h->d_pair.p, h->top_int, h->P);
+    heomk::heom_write_top<<<h->n_inst, 128, 0, h->stream>>>(h->y.data.p, h->topbuf.p, h->d_pair.p, h->d_top.p, h->N,
+                                                            h->P);
     h->launches++;
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -1050,8 +1211,39 @@ int heom_get_top(heom_handle* h, double* top)
 {
     if (!h || !top) return fail(HEOM_E_ARG, "NULL argument");
     CUDA_TRY(cudaSetDevice(h->device));
+    const size_t nn = (size_t)h->N * h->N * h->n_inst;
+    heomk::heom_record_top<<<h->n_inst, 128, 0, h->stream>>>(h->topbuf.p, h->y.data.p, h->d_pair.p, h->d_top.p, h->N,
+                                                             h->P, 0);
+    h->launches++;
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(top, h->topbuf.p, nn * 16, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int heom_set_instance_top(heom_handle* h, int32_t inst, const double* top)
+{
+    if (!h || !top) return fail(HEOM_E_ARG, "NULL argument");
+    if (inst < 0 || inst >= h->n_inst) return fail(HEOM_E_ARG, "instance %d out of range", inst);
+    CUDA_TRY(cudaSetDevice(h->device));
     const size_t nn = (size_t)h->N * h->N;
-    heomk::heom_record_top<<<1, 128, 0, h->stream>>>(h->topbuf.p, h->y.data.p, h->d_pair.p, h->top_int, h->N, h->P, 0);
+    CUDA_TRY(cudaMemcpyAsync(h->topbuf.p, top, nn * 16, cudaMemcpyHostToDevice, h->stream));
+    heomk::heom_write_top<<<1, 128, 0, h->stream>>>(h->y.data.p, h->topbuf.p, h->d_pair.p, h->d_top.p + inst, h->N,
+                                                    h->P);
+    h->launches++;
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int heom_get_instance_top(heom_handle* h, int32_t inst, double* top)
+{
+    if (!h || !top) return fail(HEOM_E_ARG, "NULL argument");
+    if (inst < 0 || inst >= h->n_inst) return fail(HEOM_E_ARG, "instance %d out of range", inst);
+    CUDA_TRY(cudaSetDevice(h->device));
+    const size_t nn = (size_t)h->N * h->N;
+    heomk::heom_record_top<<<1, 128, 0, h->stream>>>(h->topbuf.p, h->y.data.p, h->d_pair.p, h->d_top.p + inst, h->N,
+                                                     h->P, 0);
     h->launches++;
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(top, h->topbuf.p, nn * 16, cudaMemcpyDeviceToHost, h->stream));
@@ -1093,15 +1285,17 @@ int heom_propagate(heom_handle* h, double dt, int64_t steps, int64_t observe_eve
         return fail(HEOM_E_ARG, "bad argument (steps must be a multiple of observe_every)");
     CUDA_TRY(cudaSetDevice(h->device));
     const int64_t rows = steps / observe_every + 1;
-    const int nn = h->N * h->N;
+    const int64_t nn = (int64_t)h->N * h->N * h->n_inst;
     if ((int64_t)h->toplog.n < rows * nn)
         if (int rc = h->toplog.alloc(rows * nn)) return rc;
-    heomk::heom_record_top<<<1, 128, 0, h->stream>>>(h->toplog.p, h->y.data.p, h->d_pair.p, h->top_int, h->N, h->P, 0);
+    heomk::heom_record_top<<<h->n_inst, 128, 0, h->stream>>>(h->toplog.p, h->y.data.p, h->d_pair.p, h->d_top.p, h->N,
+                                                             h->P, 0);
     h->launches++;
     CUDA_TRY(cudaGetLastError());
     for (int64_t r = 1; r < rows; ++r) {
         if (int rc = run_steps(h, dt, observe_every)) return rc;
-        heomk::heom_record_top<<<1, 128, 0, h->stream>>>(h->toplog.p, h->y.data.p, h->d_pair.p, h->top_int, h->N, h->P, r);
+        heomk::heom_record_top<<<h->n_inst, 128, 0, h->stream>>>(h->toplog.p, h->y.data.p, h->d_pair.p, h->d_top.p,
+                                                                 h->N, h->P, r);
         h->launches++;
         CUDA_TRY(cudaGetLastError());
     }
@@ -1138,10 +1332,9 @@ int heom_rk4_steps_noalloc(heom_handle* h, double* d_state, double dt, int64_t s
     double2* b = reinterpret_cast<double2*>(base + 2 * kNoAllocBufferBytes);
     // every element of y, a and b is written before it is read in this call, so
     // what an earlier call left in the array needs no clearing
-    const int64_t total = h->nodes * h->P;
-    const int cblocks = (int)std::max<int64_t>(1, std::min<int64_t>((total + 255) / 256, h->sm_count * 16));
+    const int cblocks = conv_blocks(h, h->nodes);
     heomk::heom_to_pairs<<<cblocks, 256, 0, h->stream>>>(y, reinterpret_cast<const double2*>(d_state),
-                                                          h->d_ref_of_int.p, h->d_pair.p, h->nodes, h->N, h->P);
+                                                          h->d_int_of_ref.p, h->d_pair.p, 0, h->nodes, h->N, h->P);
     h->launches++;
     CUDA_TRY(cudaGetLastError());
     const double2* ins[4] = {y, a, b, a};
@@ -1152,7 +1345,7 @@ int heom_rk4_steps_noalloc(heom_handle* h, double* d_state, double dt, int64_t s
             if (int rc = launch_stage(h, EPI_AXPY_SELF, ins[k], nullptr, outs[k], nullptr, beta, 0)) return rc;
         }
     heomk::heom_from_pairs<<<cblocks, 256, 0, h->stream>>>(reinterpret_cast<double2*>(d_state), y,
-                                                            h->d_ref_of_int.p, h->d_pair.p, h->nodes, h->N, h->P);
+                                                            h->d_int_of_ref.p, h->d_pair.p, 0, h->nodes, h->N, h->P);
     h->launches++;
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -1163,5 +1356,515 @@ void* heom_stream(heom_handle* h) { return h ? (void*)h->stream : nullptr; }
 int64_t heom_matrices(const heom_handle* h) { return h ? h->nodes : 0; }
 int32_t heom_states(const heom_handle* h) { return h ? h->N : 0; }
 int64_t heom_kernel_launches(const heom_handle* h) { return h ? h->launches : 0; }
+int32_t heom_instances(const heom_handle* h) { return h ? h->n_inst : 0; }
+int64_t heom_instance_matrices(const heom_handle* h, int32_t inst)
+{
+    return (h && inst >= 0 && inst < h->n_inst) ? h->inst_base[inst + 1] - h->inst_base[inst] : 0;
+}
+int64_t heom_instance_offset(const heom_handle* h, int32_t inst)
+{
+    return (h && inst >= 0 && inst < h->n_inst) ? h->inst_base[inst] : -1;
+}
+
+} // extern "C"
+
+// ---------------------------------------------------------------------------
+// Ensembles: classes of batch handles stepped together.  One RK4 step is one
+// CUDA graph: a fork on the ensemble's stream, every class's stage launches on
+// the class's own stream (concurrent branches), a join.  The stage grid of
+// every class is chosen by timing candidate shapes (ens_autotune).
+// ---------------------------------------------------------------------------
+
+struct heom_ensemble {
+    heom_options opt{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<heom_handle*> cls;
+    std::vector<int32_t> cls_of, idx_of; // per instance
+    std::vector<int64_t> top_off;        // per instance, doubles into a row of tops
+    int64_t row_len = 0;
+    cudaEvent_t fork = nullptr;
+    std::vector<cudaEvent_t> join;
+    cudaGraphExec_t step_graph = nullptr;
+    double graph_dt = 0.0;
+    bool tuned = false;
+    double tuned_us = 0.0;
+
+    ~heom_ensemble()
+    {
+        if (stream) cudaStreamSynchronize(stream);
+        if (step_graph) cudaGraphExecDestroy(step_graph);
+        for (heom_handle* c : cls) heom_destroy(c);
+        if (fork) cudaEventDestroy(fork);
+        for (cudaEvent_t ev : join) cudaEventDestroy(ev);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+// group instances into classes that can share a batch handle (first-fit, in order)
+void group_classes(const heom_instance_desc* descs, int32_t count, std::vector<std::vector<int32_t>>& groups)
+{
+    groups.clear();
+    for (int32_t k = 0; k < count; ++k) {
+        bool placed = false;
+        for (auto& g : groups)
+            if (check_same_class(&descs[g[0]], &descs[k]) == 0) {
+                g.push_back(k);
+                placed = true;
+                break;
+            }
+        if (!placed) groups.push_back({k});
+    }
+    g_last_error.clear();
+}
+
+// device bytes of one batch handle of these instances
+size_t class_footprint(const heom_instance_desc* descs, const std::vector<int32_t>& members, int scheme)
+{
+    const heom_instance_desc& d = descs[members[0]];
+    int64_t nodes = 0;
+    for (int32_t k : members) nodes += descs[k].matrices;
+    const int P = heomk::pairs_of(d.states);
+    const int W = d.ado_width;
+    const size_t state = (size_t)nodes * P * 32;
+    const int buffers = 1 + (scheme == HEOM_RK4_REFERENCE ? 5 : 2);
+    const size_t per_ado = (size_t)((2 * W + 3) & ~3) * 4 + ((W + 15) & ~15) + 16 + 8 + (members.size() > 1 ? 4 : 0);
+    const size_t nn16 = (size_t)d.states * d.states * 16;
+    const size_t xfer = std::min<size_t>((size_t)nodes * nn16, (size_t(64) << 20) + nn16);
+    return state * buffers + per_ado * nodes + xfer + members.size() * (nn16 * 3 + 2048);
+}
+
+int ens_enqueue_step(heom_ensemble* e, double dt)
+{
+    CUDA_TRY(cudaEventRecord(e->fork, e->stream));
+    for (size_t c = 0; c < e->cls.size(); ++c) {
+        heom_handle* h = e->cls[c];
+        CUDA_TRY(cudaStreamWaitEvent(h->stream, e->fork, 0));
+        if (int rc = enqueue_step(h, dt)) return rc;
+        CUDA_TRY(cudaEventRecord(e->join[c], h->stream));
+        CUDA_TRY(cudaStreamWaitEvent(e->stream, e->join[c], 0));
+    }
+    return 0;
+}
+
+void ens_drop_graph(heom_ensemble* e)
+{
+    if (e->step_graph) {
+        cudaGraphExecDestroy(e->step_graph);
+        e->step_graph = nullptr;
+    }
+}
+
+// one stage of every class (stage buffers only) as a graph, for timing
+int ens_probe_graph(heom_ensemble* e, cudaGraphExec_t* out)
+{
+    std::vector<int64_t> saved;
+    for (heom_handle* h : e->cls) saved.push_back(h->launches);
+    cudaGraph_t graph = nullptr;
+    CUDA_TRY(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = 0;
+    cudaError_t ce = cudaEventRecord(e->fork, e->stream);
+    for (size_t c = 0; c < e->cls.size() && !rc && ce == cudaSuccess; ++c) {
+        heom_handle* h = e->cls[c];
+        ce = cudaStreamWaitEvent(h->stream, e->fork, 0);
+        if (ce == cudaSuccess)
+            rc = launch_stage(h, EPI_AXPY_SELF, h->work[0].p, nullptr, h->work[1].p, nullptr,
+                              make_double2(1e-30, 0.0), 0);
+        if (!rc && ce == cudaSuccess) ce = cudaEventRecord(e->join[c], h->stream);
+        if (!rc && ce == cudaSuccess) ce = cudaStreamWaitEvent(e->stream, e->join[c], 0);
+    }
+    cudaError_t ce2 = cudaStreamEndCapture(e->stream, &graph);
+    for (size_t c = 0; c < e->cls.size(); ++c) e->cls[c]->launches = saved[c];
+    if (rc || ce != cudaSuccess || ce2 != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        if (rc) return rc;
+        return fail(HEOM_E_CUDA, "probe capture failed: %s",
+                    cudaGetErrorString(ce != cudaSuccess ? ce : ce2));
+    }
+    ce = cudaGraphInstantiate(out, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return fail(HEOM_E_CUDA, "probe instantiate failed: %s", cudaGetErrorString(ce));
+    return 0;
+}
+
+std::mutex g_tune_mu;
+std::vector<std::pair<std::string, std::vector<int>>> g_tune_cache;
+
+std::string ens_signature(const heom_ensemble* e)
+{
+    std::string sig;
+    for (const heom_handle* h : e->cls) {
+        char buf[160];
+        snprintf(buf, sizeof buf, "%d:%d:%d:%d:%lld:%d:%d|", h->sm_count, h->N, h->W, h->LS, (long long)h->nodes,
+                 h->hkind, h->SLT);
+        sig += buf;
+    }
+    return sig;
+}
+
+int ens_autotune(heom_ensemble* e, double* best_us)
+{
+    const size_t C = e->cls.size();
+    std::vector<int> full(C), groups(C);
+    std::vector<double> work(C);
+    double total = 0.0;
+    for (size_t c = 0; c < C; ++c) {
+        heom_handle* h = e->cls[c];
+        if (int rc = prepare_scheme(h)) return rc;
+        h->grid_override = 0;
+        const void* fn = nullptr;
+        int blocks = 0;
+        if (int rc = resolve_stage(h, &fn, &blocks)) return rc;
+        full[c] = h->per_sm[h->hkind] * h->sm_count;
+        groups[c] = blocks;
+        work[c] = (double)h->nodes * h->P;
+        total += work[c];
+    }
+    const std::string sig = ens_signature(e);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        for (auto& entry : g_tune_cache)
+            if (entry.first == sig) {
+                for (size_t c = 0; c < C; ++c) e->cls[c]->grid_override = entry.second[c];
+                e->tuned = true;
+                ens_drop_graph(e);
+                if (best_us) *best_us = e->tuned_us;
+                return 0;
+            }
+    }
+    // candidates: every class a full wave; shares of one wave in proportion to
+    // the class's bytes (classes run side by side), scaled by 1/2, 1, 2
+    std::vector<std::vector<int>> cand;
+    cand.push_back(full);
+    std::vector<int> half(C);
+    for (size_t c = 0; c < C; ++c) half[c] = std::max(1, full[c] / 2);
+    cand.push_back(half);
+    for (double f : {0.5, 1.0, 2.0}) {
+        std::vector<int> v(C);
+        for (size_t c = 0; c < C; ++c) v[c] = std::max(1, (int)std::ceil(f * full[c] * work[c] / total));
+        cand.push_back(v);
+    }
+    // identical launch shapes (after the cap at one block per ADO group) are timed once
+    for (auto& v : cand)
+        for (size_t c = 0; c < C; ++c) v[c] = std::min(v[c], std::max(groups[c], 1));
+    std::sort(cand.begin(), cand.end());
+    cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    CUDA_TRY(cudaEventCreate(&t0));
+    CUDA_TRY(cudaEventCreate(&t1));
+    double best = 1e300;
+    size_t pick = 0;
+    int rc = 0;
+    for (size_t q = 0; q < cand.size() && !rc; ++q) {
+        for (size_t c = 0; c < C; ++c) e->cls[c]->grid_override = cand[q][c];
+        cudaGraphExec_t g = nullptr;
+        if ((rc = ens_probe_graph(e, &g))) break;
+        const int warm = 2, reps = 5;
+        cudaError_t ce = cudaSuccess;
+        for (int r = 0; r < warm && ce == cudaSuccess; ++r) ce = cudaGraphLaunch(g, e->stream);
+        if (ce == cudaSuccess) ce = cudaEventRecord(t0, e->stream);
+        for (int r = 0; r < reps && ce == cudaSuccess; ++r) ce = cudaGraphLaunch(g, e->stream);
+        if (ce == cudaSuccess) ce = cudaEventRecord(t1, e->stream);
+        if (ce == cudaSuccess) ce = cudaEventSynchronize(t1);
+        float ms = 0.0f;
+        if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, t0, t1);
+        cudaGraphExecDestroy(g);
+        if (ce != cudaSuccess) {
+            rc = fail(HEOM_E_CUDA, "autotune timing failed: %s", cudaGetErrorString(ce));
+            break;
+        }
+        for (heom_handle* h : e->cls) h->launches += warm + reps;
+        const double us = 1e3 * ms / reps;
+        if (us < best) {
+            best = us;
+            pick = q;
+        }
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (rc) return rc;
+    for (heom_handle* h : e->cls)
+        if (int rc2 = check_kernel_error(h)) return rc2;
+    for (size_t c = 0; c < C; ++c) e->cls[c]->grid_override = cand[pick][c];
+    e->tuned = true;
+    e->tuned_us = best;
+    ens_drop_graph(e);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        g_tune_cache.emplace_back(sig, cand[pick]);
+    }
+    if (best_us) *best_us = best;
+    return 0;
+}
+
+int ens_run_steps(heom_ensemble* e, double dt, int64_t steps)
+{
+    if (steps <= 0) return 0;
+    if (!e->tuned)
+        if (int rc = ens_autotune(e, nullptr)) return rc;
+    for (heom_handle* h : e->cls) {
+        if (int rc = prepare_scheme(h)) return rc;
+        const void* fn = nullptr;
+        if (int rc = resolve_stage(h, &fn)) return rc;
+        if (h->stage_smem == 0) return fail(HEOM_E_CUDA, "stage kernel shape unresolved");
+    }
+    if (!e->opt.use_graphs) {
+        for (int64_t s = 0; s < steps; ++s)
+            if (int rc = ens_enqueue_step(e, dt)) return rc;
+        return 0;
+    }
+    if (e->step_graph && e->graph_dt != dt) ens_drop_graph(e);
+    if (!e->step_graph) {
+        std::vector<int64_t> saved;
+        for (heom_handle* h : e->cls) saved.push_back(h->launches);
+        cudaGraph_t graph = nullptr;
+        CUDA_TRY(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = ens_enqueue_step(e, dt);
+        cudaError_t ce = cudaStreamEndCapture(e->stream, &graph);
+        for (size_t c = 0; c < e->cls.size(); ++c) e->cls[c]->launches = saved[c];
+        if (rc) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        if (ce != cudaSuccess) return fail(HEOM_E_CUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+        ce = cudaGraphInstantiate(&e->step_graph, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) return fail(HEOM_E_CUDA, "graph instantiate failed: %s", cudaGetErrorString(ce));
+        e->graph_dt = dt;
+    }
+    for (int64_t s = 0; s < steps; ++s) {
+        CUDA_TRY(cudaGraphLaunch(e->step_graph, e->stream));
+        for (heom_handle* h : e->cls) h->launches += launches_per_step(h);
+    }
+    return 0;
+}
+
+int ens_check(heom_ensemble* e, int32_t inst, heom_handle** h, int32_t* idx)
+{
+    if (!e) return fail(HEOM_E_ARG, "NULL ensemble");
+    if (inst < 0 || inst >= (int32_t)e->cls_of.size()) return fail(HEOM_E_ARG, "instance %d out of range", inst);
+    *h = e->cls[e->cls_of[inst]];
+    *idx = e->idx_of[inst];
+    return 0;
+}
+
+} // namespace
+
+extern "C" {
+
+int heom_ensemble_footprint(const heom_instance_desc* descs, int32_t count, const heom_options* opt, size_t* bytes)
+{
+    if (!descs || count < 1 || !bytes) return fail(HEOM_E_ARG, "bad argument");
+    for (int32_t k = 0; k < count; ++k)
+        if (int rc = check_desc(&descs[k])) return fail(rc, "instance %d: %s", k, g_last_error.c_str());
+    heom_options o;
+    heom_default_options(&o);
+    if (opt) o = *opt;
+    std::vector<std::vector<int32_t>> groups;
+    group_classes(descs, count, groups);
+    size_t total = 0;
+    for (auto& g : groups) total += class_footprint(descs, g, o.rk4_scheme);
+    *bytes = total;
+    return 0;
+}
+
+int heom_ensemble_create(const heom_instance_desc* descs, int32_t count, const heom_options* opt, heom_ensemble** out)
+{
+    if (!out) return fail(HEOM_E_ARG, "out is NULL");
+    *out = nullptr;
+    size_t need = 0;
+    if (int rc = heom_ensemble_footprint(descs, count, opt, &need)) return rc;
+    std::unique_ptr<heom_ensemble> e(new heom_ensemble());
+    heom_default_options(&e->opt);
+    if (opt) e->opt = *opt;
+    e->device = e->opt.device;
+    CUDA_TRY(cudaSetDevice(e->device));
+    size_t free_b = 0, total_b = 0;
+    CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    if (need > free_b)
+        return fail(HEOM_E_NOMEM, "ensemble needs %.3f GB of device memory, %.3f GB are free", need / 1e9,
+                    free_b / 1e9);
+    CUDA_TRY(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
+    std::vector<std::vector<int32_t>> groups;
+    group_classes(descs, count, groups);
+    e->cls_of.assign(count, 0);
+    e->idx_of.assign(count, 0);
+    for (size_t c = 0; c < groups.size(); ++c) {
+        std::vector<heom_instance_desc> members;
+        for (size_t i = 0; i < groups[c].size(); ++i) {
+            members.push_back(descs[groups[c][i]]);
+            e->cls_of[groups[c][i]] = (int32_t)c;
+            e->idx_of[groups[c][i]] = (int32_t)i;
+        }
+        heom_handle* h = nullptr;
+        if (int rc = heom_create_batch(members.data(), (int32_t)members.size(), &e->opt, &h))
+            return fail(rc, "class %zu: %s", c, g_last_error.c_str());
+        e->cls.push_back(h);
+        cudaEvent_t ev = nullptr;
+        CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        e->join.push_back(ev);
+    }
+    e->top_off.assign(count, 0);
+    for (int32_t k = 0; k < count; ++k) {
+        e->top_off[k] = e->row_len;
+        e->row_len += (int64_t)2 * descs[k].states * descs[k].states;
+    }
+    *out = e.release();
+    return 0;
+}
+
+int heom_ensemble_destroy(heom_ensemble* e)
+{
+    if (!e) return 0;
+    cudaSetDevice(e->device);
+    delete e;
+    return 0;
+}
+
+int32_t heom_ensemble_instances(const heom_ensemble* e) { return e ? (int32_t)e->cls_of.size() : 0; }
+int32_t heom_ensemble_classes(const heom_ensemble* e) { return e ? (int32_t)e->cls.size() : 0; }
+
+int heom_ensemble_locate(const heom_ensemble* e, int32_t inst, int32_t* cls, int32_t* index)
+{
+    if (!e || inst < 0 || inst >= (int32_t)e->cls_of.size()) return fail(HEOM_E_ARG, "instance out of range");
+    if (cls) *cls = e->cls_of[inst];
+    if (index) *index = e->idx_of[inst];
+    return 0;
+}
+
+heom_handle* heom_ensemble_class(heom_ensemble* e, int32_t cls)
+{
+    return (e && cls >= 0 && cls < (int32_t)e->cls.size()) ? e->cls[cls] : nullptr;
+}
+
+int heom_ensemble_set_hamiltonian(heom_ensemble* e, int32_t inst, const double* ham)
+{
+    heom_handle* h = nullptr;
+    int32_t idx = 0;
+    if (int rc = ens_check(e, inst, &h, &idx)) return rc;
+    CUDA_TRY(cudaSetDevice(e->device));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    const int old_kind = h->hkind;
+    if (int rc = heom_set_instance_hamiltonian(h, idx, ham)) return rc;
+    ens_drop_graph(e);
+    if (h->hkind != old_kind) e->tuned = false; // another kernel variant: shapes are re-timed
+    return 0;
+}
+
+int heom_ensemble_set_top(heom_ensemble* e, int32_t inst, const double* top)
+{
+    heom_handle* h = nullptr;
+    int32_t idx = 0;
+    if (int rc = ens_check(e, inst, &h, &idx)) return rc;
+    CUDA_TRY(cudaSetDevice(e->device));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    return heom_set_instance_top(h, idx, top);
+}
+
+int heom_ensemble_get_top(heom_ensemble* e, int32_t inst, double* top)
+{
+    heom_handle* h = nullptr;
+    int32_t idx = 0;
+    if (int rc = ens_check(e, inst, &h, &idx)) return rc;
+    CUDA_TRY(cudaSetDevice(e->device));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    return heom_get_instance_top(h, idx, top);
+}
+
+int heom_ensemble_autotune(heom_ensemble* e, double* best_stage_us)
+{
+    if (!e) return fail(HEOM_E_ARG, "NULL ensemble");
+    CUDA_TRY(cudaSetDevice(e->device));
+    return ens_autotune(e, best_stage_us);
+}
+
+int heom_ensemble_rk4_steps(heom_ensemble* e, double dt, int64_t steps)
+{
+    if (!e || steps < 0 || !(dt > 0.0)) return fail(HEOM_E_ARG, "bad argument");
+    CUDA_TRY(cudaSetDevice(e->device));
+    if (int rc = ens_run_steps(e, dt, steps)) return rc;
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    for (heom_handle* h : e->cls)
+        if (int rc = check_kernel_error(h)) return rc;
+    return 0;
+}
+
+int heom_ensemble_propagate(heom_ensemble* e, double dt, int64_t steps, int64_t observe_every, double* host_tops)
+{
+    if (!e || !host_tops || steps < 0 || observe_every <= 0 || steps % observe_every != 0 || !(dt > 0.0))
+        return fail(HEOM_E_ARG, "bad argument (steps must be a multiple of observe_every)");
+    CUDA_TRY(cudaSetDevice(e->device));
+    const int64_t rows = steps / observe_every + 1;
+    for (heom_handle* h : e->cls) {
+        const int64_t nn = (int64_t)h->N * h->N * h->n_inst;
+        if ((int64_t)h->toplog.n < rows * nn)
+            if (int rc = h->toplog.alloc(rows * nn)) return rc;
+        CUDA_TRY(cudaStreamSynchronize(h->stream));
+    }
+    auto record = [&](int64_t row) -> int {
+        for (heom_handle* h : e->cls) {
+            heomk::heom_record_top<<<h->n_inst, 128, 0, e->stream>>>(h->toplog.p, h->y.data.p, h->d_pair.p,
+                                                                     h->d_top.p, h->N, h->P, row);
+            h->launches++;
+            CUDA_TRY(cudaGetLastError());
+        }
+        return 0;
+    };
+    if (int rc = record(0)) return rc;
+    for (int64_t r = 1; r < rows; ++r) {
+        if (int rc = ens_run_steps(e, dt, observe_every)) return rc;
+        if (int rc = record(r)) return rc;
+    }
+    // gather every class's log, then scatter into instance order
+    std::vector<std::vector<double>> logs(e->cls.size());
+    for (size_t c = 0; c < e->cls.size(); ++c) {
+        heom_handle* h = e->cls[c];
+        logs[c].resize((size_t)rows * h->n_inst * h->N * h->N * 2);
+        CUDA_TRY(cudaMemcpyAsync(logs[c].data(), h->toplog.p, logs[c].size() * 8, cudaMemcpyDeviceToHost, e->stream));
+    }
+    // failure detection: a non-finite state is reported instead of returned silently
+    for (heom_handle* h : e->cls) {
+        CUDA_TRY(cudaMemsetAsync(h->d_flag.p, 0, sizeof(int), e->stream));
+        heomk::heom_check_finite<<<h->sm_count * 4, 256, 0, e->stream>>>(
+            reinterpret_cast<const double*>(h->y.data.p), (int64_t)h->state_elems() * 2, h->d_flag.p);
+        h->launches++;
+        CUDA_TRY(cudaGetLastError());
+    }
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    for (int32_t k = 0; k < (int32_t)e->cls_of.size(); ++k) {
+        const heom_handle* h = e->cls[e->cls_of[k]];
+        const int64_t nn2 = (int64_t)h->N * h->N * 2;
+        for (int64_t r = 0; r < rows; ++r)
+            std::memcpy(host_tops + r * e->row_len + e->top_off[k],
+                        logs[e->cls_of[k]].data() + (r * h->n_inst + e->idx_of[k]) * nn2, nn2 * 8);
+    }
+    for (heom_handle* h : e->cls) {
+        if (int rc = check_kernel_error(h)) return rc;
+        int flag = 0;
+        CUDA_TRY(cudaMemcpy(&flag, h->d_flag.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (flag) return fail(HEOM_E_NONFINITE, "non-finite value in the hierarchy state after propagation");
+    }
+    return 0;
+}
+
+int64_t heom_ensemble_top_row_len(const heom_ensemble* e) { return e ? e->row_len : 0; }
+int64_t heom_ensemble_top_offset(const heom_ensemble* e, int32_t inst)
+{
+    return (e && inst >= 0 && inst < (int32_t)e->top_off.size()) ? e->top_off[inst] : -1;
+}
+
+int64_t heom_ensemble_kernel_launches(const heom_ensemble* e)
+{
+    int64_t n = 0;
+    if (e)
+        for (const heom_handle* h : e->cls) n += h->launches;
+    return n;
+}
+
+void* heom_ensemble_stream(heom_ensemble* e) { return e ? (void*)e->stream : nullptr; }
 
 } // extern "C"

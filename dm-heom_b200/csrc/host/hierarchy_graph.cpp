@@ -95,22 +95,41 @@ hierarchy_graph::hierarchy_graph(int64_t width, int64_t depth) : width_(width), 
     }
     if (uid != nodes_) throw std::logic_error("hierarchy_graph: node count mismatch");
 
+    // Neighbour ranks in O(1) each.  With prefix_k = t_0 + ... + t_{k-1} and
+    // w_k = W-1-k, the rank is sum_k A_k(0) where
+    //   A_k(d) = sum_{x < t_k} C(D - prefix_k - d - x + w_k, w_k)
+    //          = C(D - prefix_k - d + w_k + 1, w_k + 1) - C(D - prefix_k - d - t_k + w_k + 1, w_k + 1)
+    // (hockey stick).  Raising t_j shifts the prefixes after j by +1 (d = 1)
+    // and adds one term at j; lowering it shifts them by -1 and drops one.
     plus_.assign((size_t)nodes_ * W, invalid_uid);
     minus_.assign((size_t)nodes_ * W, invalid_uid);
+    auto C = [this](int64_t a, int64_t b) -> int64_t { return a < b || a < 0 ? 0 : binom_[a][b]; };
+    std::vector<int64_t> prefix(W + 1), a0(W), pre0(W + 1), sufp(W + 1), sufm(W + 1);
     for (int64_t u = 0; u < nodes_; ++u) {
-        std::copy(tuples_.begin() + u * W, tuples_.begin() + (u + 1) * W, t.begin());
-        const int64_t sum = std::accumulate(t.begin(), t.end(), int64_t(0));
+        const int32_t* tu = tuples_.data() + u * W;
+        prefix[0] = 0;
+        for (size_t k = 0; k < W; ++k) prefix[k + 1] = prefix[k] + tu[k];
+        const int64_t sum = prefix[W];
+        auto A = [&](size_t k, int64_t d) {
+            const int64_t w = (int64_t)W - 1 - (int64_t)k, R = depth - prefix[k] - d;
+            return C(R + w + 1, w + 1) - C(R - tu[k] + w + 1, w + 1);
+        };
+        pre0[0] = 0;
+        for (size_t k = 0; k < W; ++k) {
+            a0[k] = A(k, 0);
+            pre0[k + 1] = pre0[k] + a0[k];
+        }
+        sufp[W] = sufm[W] = 0;
+        for (size_t k = W; k-- > 0;) {
+            sufp[k] = sufp[k + 1] + (sum < depth ? A(k, 1) : 0); // :151-156 (plus only below the last layer)
+            sufm[k] = sufm[k + 1] + A(k, -1);
+        }
         for (size_t j = 0; j < W; ++j) {
-            if (sum < depth) { // :151-156
-                t[j] += 1;
-                plus_[u * W + j] = uid_of_rank[lex_rank(t.data())];
-                t[j] -= 1;
-            }
-            if (t[j] > 0) { // :158-163
-                t[j] -= 1;
-                minus_[u * W + j] = uid_of_rank[lex_rank(t.data())];
-                t[j] += 1;
-            }
+            const int64_t w = (int64_t)W - 1 - (int64_t)j, R = depth - prefix[j];
+            if (sum < depth) // :151-156
+                plus_[u * W + j] = uid_of_rank[pre0[j] + a0[j] + C(R - tu[j] + w, w) + sufp[j + 1]];
+            if (tu[j] > 0) // :158-163
+                minus_[u * W + j] = uid_of_rank[pre0[j] + a0[j] - C(R - tu[j] + 1 + w, w) + sufm[j + 1]];
         }
     }
 }

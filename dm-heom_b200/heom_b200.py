@@ -36,6 +36,14 @@ EXPORTS = [
     "heom_tables_build", "heom_tables_view", "heom_tables_free", "heom_create_from_system",
     "heom_config_load", "heom_config_free", "heom_config_system", "heom_config_rho_init",
     "heom_config_get", "heom_tables_mask", "heom_rk4_steps_noalloc",
+    "heom_create_batch", "heom_instances", "heom_instance_matrices", "heom_instance_offset",
+    "heom_set_instance_hamiltonian", "heom_set_instance_top", "heom_get_instance_top",
+    "heom_ensemble_footprint", "heom_ensemble_create", "heom_ensemble_destroy",
+    "heom_ensemble_instances", "heom_ensemble_classes", "heom_ensemble_locate",
+    "heom_ensemble_class", "heom_ensemble_set_hamiltonian", "heom_ensemble_set_top",
+    "heom_ensemble_get_top", "heom_ensemble_autotune", "heom_ensemble_rk4_steps",
+    "heom_ensemble_propagate", "heom_ensemble_top_row_len", "heom_ensemble_top_offset",
+    "heom_ensemble_kernel_launches", "heom_ensemble_stream",
 ]
 
 
@@ -117,6 +125,36 @@ def lib():
         L.heom_config_rho_init.argtypes = [vp, vp]
         L.heom_config_get.argtypes = [vp, C.c_char_p, C.c_char_p, C.c_size_t]
         L.heom_rk4_steps_noalloc.argtypes = [vp, vp, dbl, i64]
+        L.heom_create_batch.argtypes = [C.POINTER(InstanceDesc), i32, C.POINTER(Options), C.POINTER(vp)]
+        L.heom_instances.restype = i32
+        L.heom_instances.argtypes = [vp]
+        for name in ["heom_instance_matrices", "heom_instance_offset"]:
+            getattr(L, name).restype = i64
+            getattr(L, name).argtypes = [vp, i32]
+        for name in ["heom_set_instance_hamiltonian", "heom_set_instance_top", "heom_get_instance_top",
+                     "heom_ensemble_set_hamiltonian", "heom_ensemble_set_top", "heom_ensemble_get_top"]:
+            getattr(L, name).argtypes = [vp, i32, vp]
+        L.heom_ensemble_footprint.argtypes = [C.POINTER(InstanceDesc), i32, C.POINTER(Options),
+                                              C.POINTER(C.c_size_t)]
+        L.heom_ensemble_create.argtypes = [C.POINTER(InstanceDesc), i32, C.POINTER(Options), C.POINTER(vp)]
+        L.heom_ensemble_destroy.argtypes = [vp]
+        for name in ["heom_ensemble_instances", "heom_ensemble_classes"]:
+            getattr(L, name).restype = i32
+            getattr(L, name).argtypes = [vp]
+        L.heom_ensemble_locate.argtypes = [vp, i32, C.POINTER(i32), C.POINTER(i32)]
+        L.heom_ensemble_class.restype = vp
+        L.heom_ensemble_class.argtypes = [vp, i32]
+        L.heom_ensemble_autotune.argtypes = [vp, C.POINTER(dbl)]
+        L.heom_ensemble_rk4_steps.argtypes = [vp, dbl, i64]
+        L.heom_ensemble_propagate.argtypes = [vp, dbl, i64, i64, vp]
+        L.heom_ensemble_top_row_len.restype = i64
+        L.heom_ensemble_top_row_len.argtypes = [vp]
+        L.heom_ensemble_top_offset.restype = i64
+        L.heom_ensemble_top_offset.argtypes = [vp, i32]
+        L.heom_ensemble_kernel_launches.restype = i64
+        L.heom_ensemble_kernel_launches.argtypes = [vp]
+        L.heom_ensemble_stream.restype = vp
+        L.heom_ensemble_stream.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -159,51 +197,83 @@ class Buffer:
             pass
 
 
+TABLE_KEYS = ("states", "matsubaras", "baths", "baths_per_state", "ado_width", "ado_depth", "matrices",
+              "first_non_plus_id", "baths_coupling", "hamiltonian", "ado_tuples", "ado_plus", "ado_minus",
+              "pf_same_sum", "pf_same", "pf_circ", "cbk", "cbk_sqrt")
+
+
+def make_desc(tables: dict, keep: list) -> InstanceDesc:
+    """InstanceDesc over numpy copies of the tables (kept alive in `keep`)."""
+    def arr(a, dt):
+        a = np.ascontiguousarray(np.asarray(a, dtype=dt).reshape(-1))
+        keep.append(a)
+        return a.ctypes.data
+
+    t = tables
+    return InstanceDesc(t["states"], t["matsubaras"], t["baths"], t["baths_per_state"], t["ado_width"],
+                        t["ado_depth"], t["matrices"], t["first_non_plus_id"],
+                        arr(t["baths_coupling"], np.int32), arr(t["hamiltonian"], np.float64),
+                        arr(t["ado_tuples"], np.int32), arr(t["ado_plus"], np.int32),
+                        arr(t["ado_minus"], np.int32), arr(t["pf_same_sum"], np.float64),
+                        arr(t["pf_same"], np.float64), arr(t["pf_circ"], np.float64),
+                        arr(t["cbk"], np.float64), arr(t["cbk_sqrt"], np.float64))
+
+
+def make_options(device=0, order="lex", scheme="product", graphs=True) -> Options:
+    o = Options()
+    lib().heom_default_options(C.byref(o))
+    o.device = device
+    o.ado_order = ORDERS[order] if isinstance(order, str) else order
+    o.rk4_scheme = SCHEMES[scheme] if isinstance(scheme, str) else scheme
+    o.use_graphs = 1 if graphs else 0
+    return o
+
+
 class Heom:
-    """One hierarchy instance on one GPU (a heom_handle)."""
+    """Hierarchy instances on one GPU (a heom_handle): one instance, or a batch
+    of instances that share states and baths (Heom.batch).  For a batch every
+    state / top / Hamiltonian array holds the instances back to back."""
 
-    def __init__(self, *, states, matsubaras, baths, baths_per_state, ado_width, ado_depth,
-                 matrices, first_non_plus_id, baths_coupling, hamiltonian, ado_tuples, ado_plus,
-                 ado_minus, pf_same_sum, pf_same, pf_circ, cbk, cbk_sqrt, device=0,
-                 order="lex", scheme="product", graphs=True):
-        keep = {}
-
-        def arr(name, a, dt):
-            a = np.ascontiguousarray(np.asarray(a, dtype=dt).reshape(-1))
-            keep[name] = a
-            return a.ctypes.data
-
-        d = InstanceDesc(states, matsubaras, baths, baths_per_state, ado_width, ado_depth, matrices,
-                         first_non_plus_id,
-                         arr("c", baths_coupling, np.int32), arr("h", hamiltonian, np.float64),
-                         arr("t", ado_tuples, np.int32), arr("p", ado_plus, np.int32),
-                         arr("m", ado_minus, np.int32), arr("pss", pf_same_sum, np.float64),
-                         arr("pfs", pf_same, np.float64), arr("pfc", pf_circ, np.float64),
-                         arr("cbk", cbk, np.float64), arr("cbs", cbk_sqrt, np.float64))
-        o = Options()
-        lib().heom_default_options(C.byref(o))
-        o.device = device
-        o.ado_order = ORDERS[order] if isinstance(order, str) else order
-        o.rk4_scheme = SCHEMES[scheme] if isinstance(scheme, str) else scheme
-        o.use_graphs = 1 if graphs else 0
+    def __init__(self, *, device=0, order="lex", scheme="product", graphs=True, _batch=None, **tables):
+        keep = []
+        tabs = _batch if _batch is not None else [tables]
+        descs = (InstanceDesc * len(tabs))(*[make_desc(t, keep) for t in tabs])
+        o = make_options(device, order, scheme, graphs)
         self.h = C.c_void_p()
-        _check(lib().heom_create(C.byref(d), C.byref(o), C.byref(self.h)))
-        self.states = states
-        self.matrices = matrices
-        self.state_len = matrices * states * states * 2
+        _check(lib().heom_create_batch(descs, len(tabs), C.byref(o), C.byref(self.h)))
+        self.states = tabs[0]["states"]
+        self.instances = len(tabs)
+        self.instance_matrices = [int(t["matrices"]) for t in tabs]
+        self.matrices = sum(self.instance_matrices)
+        self.state_len = self.matrices * self.states * self.states * 2
+
+    @classmethod
+    def batch(cls, tables_list, **kw):
+        """One handle over several instances (dicts of build_tables)."""
+        return cls(_batch=list(tables_list), **kw)
+
+    def instance_offset(self, k):
+        """First ADO of instance k in the concatenated state."""
+        return lib().heom_instance_offset(self.h, k)
+
+    @staticmethod
+    def tables_of(prob) -> dict:
+        """Tables (reference layout) of a problem object with the attributes
+        system, graph, hamiltonian, pf_* and cbk* (the test oracle's Problem)."""
+        s = prob.system
+        g = prob.graph
+        return dict(states=s.states, matsubaras=s.matsubaras, baths=s.baths,
+                    baths_per_state=s.coupling.shape[1], ado_width=g.width, ado_depth=g.depth,
+                    matrices=g.nodes, first_non_plus_id=g.first_non_plus,
+                    baths_coupling=prob.coupling_flat, hamiltonian=prob.hamiltonian,
+                    ado_tuples=g.tuples, ado_plus=g.plus, ado_minus=g.minus,
+                    pf_same_sum=prob.pf_same_sum, pf_same=prob.pf_same, pf_circ=prob.pf_circ,
+                    cbk=prob.cbk, cbk_sqrt=prob.cbk_sqrt)
 
     @classmethod
     def from_problem(cls, prob, **kw):
         """Build from an oracle Problem (tables in reference layout)."""
-        s = prob.system
-        g = prob.graph
-        return cls(states=s.states, matsubaras=s.matsubaras, baths=s.baths,
-                   baths_per_state=s.coupling.shape[1], ado_width=g.width, ado_depth=g.depth,
-                   matrices=g.nodes, first_non_plus_id=g.first_non_plus,
-                   baths_coupling=prob.coupling_flat, hamiltonian=prob.hamiltonian,
-                   ado_tuples=g.tuples, ado_plus=g.plus, ado_minus=g.minus,
-                   pf_same_sum=prob.pf_same_sum, pf_same=prob.pf_same, pf_circ=prob.pf_circ,
-                   cbk=prob.cbk, cbk_sqrt=prob.cbk_sqrt, **kw)
+        return cls(**cls.tables_of(prob), **kw)
 
     def close(self):
         if self.h:
@@ -238,13 +308,29 @@ class Heom:
         _check(lib().heom_set_top(self.h, _ptr(top)))
 
     def get_top(self):
-        t = np.empty(self.states * self.states * 2)
+        t = np.empty(self.instances * self.states * self.states * 2)
         _check(lib().heom_get_top(self.h, _ptr(t)))
+        return t
+
+    def set_instance_top(self, k, top):
+        top = np.ascontiguousarray(top, dtype=np.float64)
+        assert top.size == self.states * self.states * 2
+        _check(lib().heom_set_instance_top(self.h, k, _ptr(top)))
+
+    def get_instance_top(self, k):
+        t = np.empty(self.states * self.states * 2)
+        _check(lib().heom_get_instance_top(self.h, k, _ptr(t)))
         return t
 
     def set_hamiltonian(self, ham):
         ham = np.ascontiguousarray(ham, dtype=np.float64)
+        assert ham.size == self.instances * self.states * self.states * 2
         _check(lib().heom_set_hamiltonian(self.h, _ptr(ham)))
+
+    def set_instance_hamiltonian(self, k, ham):
+        ham = np.ascontiguousarray(ham, dtype=np.float64)
+        assert ham.size == self.states * self.states * 2
+        _check(lib().heom_set_instance_hamiltonian(self.h, k, _ptr(ham)))
 
     def set_mask(self, mask):
         mask = np.ascontiguousarray(mask, dtype=np.uint8)
@@ -265,14 +351,19 @@ class Heom:
         _check(lib().heom_synchronize(self.h))
 
     def propagate(self, dt, steps, observe_every):
+        """Tops at every observation: [rows, states^2 * 2] for one instance,
+        [rows, instances, states^2 * 2] for a batch."""
         rows = steps // observe_every + 1
-        tops = np.empty(rows * self.states * self.states * 2)
+        nn2 = self.states * self.states * 2
+        tops = np.empty(rows * self.instances * nn2)
         _check(lib().heom_propagate(self.h, dt, steps, observe_every, _ptr(tops)))
-        return tops.reshape(rows, self.states * self.states * 2)
+        if self.instances == 1:
+            return tops.reshape(rows, nn2)
+        return tops.reshape(rows, self.instances, nn2)
 
     def populations_from_tops(self, tops):
         n = self.states
-        return tops[:, [(n + 1) * 2 * i for i in range(n)]]
+        return tops[..., [(n + 1) * 2 * i for i in range(n)]]
 
     def stream(self):
         return lib().heom_stream(self.h)
@@ -293,6 +384,100 @@ class Heom:
         c = np.ascontiguousarray(np.asarray(coeffs, np.float64))
         kp = (C.c_void_p * max(1, len(ks)))(*[k.h.value for k in ks])
         _check(lib().heom_weighted_add(self.h, len(ks), step, out.h, y.h, _ptr(c), kp))
+
+
+class Ensemble:
+    """Instances of any sizes on one GPU (a heom_ensemble): grouped into
+    classes of batch handles, one graph launch per RK4 step with the classes
+    as concurrent branches, stage grids picked by the autotuner."""
+
+    def __init__(self, tables_list, device=0, order="lex", scheme="product", graphs=True):
+        keep = []
+        tabs = list(tables_list)
+        descs = (InstanceDesc * len(tabs))(*[make_desc(t, keep) for t in tabs])
+        o = make_options(device, order, scheme, graphs)
+        self.h = C.c_void_p()
+        _check(lib().heom_ensemble_create(descs, len(tabs), C.byref(o), C.byref(self.h)))
+        self.instances = len(tabs)
+        self.states = [int(t["states"]) for t in tabs]
+        self.row_len = lib().heom_ensemble_top_row_len(self.h)
+        self.top_offsets = [lib().heom_ensemble_top_offset(self.h, k) for k in range(len(tabs))]
+
+    @staticmethod
+    def footprint(tables_list, scheme="product"):
+        keep = []
+        tabs = list(tables_list)
+        descs = (InstanceDesc * len(tabs))(*[make_desc(t, keep) for t in tabs])
+        o = make_options(0, "lex", scheme, True)
+        b = C.c_size_t()
+        _check(lib().heom_ensemble_footprint(descs, len(tabs), C.byref(o), C.byref(b)))
+        return b.value
+
+    def close(self):
+        if self.h:
+            lib().heom_ensemble_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def classes(self):
+        return lib().heom_ensemble_classes(self.h)
+
+    def locate(self, k):
+        c, i = C.c_int32(), C.c_int32()
+        _check(lib().heom_ensemble_locate(self.h, k, C.byref(c), C.byref(i)))
+        return c.value, i.value
+
+    def set_top(self, k, top):
+        top = np.ascontiguousarray(top, dtype=np.float64)
+        assert top.size == self.states[k] ** 2 * 2
+        _check(lib().heom_ensemble_set_top(self.h, k, _ptr(top)))
+
+    def get_top(self, k):
+        t = np.empty(self.states[k] ** 2 * 2)
+        _check(lib().heom_ensemble_get_top(self.h, k, _ptr(t)))
+        return t
+
+    def set_hamiltonian(self, k, ham):
+        ham = np.ascontiguousarray(ham, dtype=np.float64)
+        assert ham.size == self.states[k] ** 2 * 2
+        _check(lib().heom_ensemble_set_hamiltonian(self.h, k, _ptr(ham)))
+
+    def autotune(self):
+        us = C.c_double()
+        _check(lib().heom_ensemble_autotune(self.h, C.byref(us)))
+        return us.value
+
+    def rk4_steps(self, dt, steps):
+        _check(lib().heom_ensemble_rk4_steps(self.h, dt, steps))
+
+    def propagate(self, dt, steps, observe_every):
+        """Per-instance tops: a list of [rows, states_k^2 * 2] arrays."""
+        rows = steps // observe_every + 1
+        buf = np.empty(rows * self.row_len)
+        _check(lib().heom_ensemble_propagate(self.h, dt, steps, observe_every, _ptr(buf)))
+        buf = buf.reshape(rows, self.row_len)
+        return [buf[:, o:o + 2 * n * n].copy() for o, n in zip(self.top_offsets, self.states)]
+
+    def populations(self, tops, k):
+        n = self.states[k]
+        return tops[:, [(n + 1) * 2 * i for i in range(n)]]
+
+    def kernel_launches(self):
+        return lib().heom_ensemble_kernel_launches(self.h)
+
+    def stream(self):
+        return lib().heom_ensemble_stream(self.h)
 
 
 # --------------------------------------------------------------------------

@@ -201,6 +201,79 @@ int32_t heom_states(const heom_handle* h);
 int64_t heom_kernel_launches(const heom_handle* h);
 
 /* ------------------------------------------------------------------------
+ * Batches: several hierarchy instances in one handle.  No counterpart in the
+ * reference, which propagates one instance per process.
+ * ------------------------------------------------------------------------ */
+
+/* Instances that share states, matsubaras, baths, baths_per_state,
+ * baths_coupling and the bath tables (pf_same, pf_circ, cbk, cbk_sqrt) but may
+ * differ in depth, hierarchy tables, mask and Hamiltonian (the realisations
+ * of a static-disorder ensemble, say) are propagated together: every RK4
+ * stage is one kernel launch over the ADOs of all instances.  On such a
+ * handle every per-handle host array holds the instances back to back in
+ * instance order:
+ *   states (heom_set_state, heom_get_state, heom_buffer_*):  sum of matrices x states^2 complex
+ *   tops (heom_set_top, heom_get_top):                       count x states^2 complex
+ *   tops (heom_propagate):                                   rows x count x states^2 complex
+ *   Hamiltonians (heom_set_hamiltonian):                     count x states^2 complex
+ *   mask (heom_set_mask):                                    sum of matrices
+ * heom_matrices gives the total number of ADOs.  A handle made by
+ * heom_create is a batch of one.  Fails with HEOM_E_ARG when the instances
+ * do not share the above. */
+int heom_create_batch(const heom_instance_desc* descs, int32_t count, const heom_options* opt,
+                      heom_handle** out);
+int32_t heom_instances(const heom_handle* h);
+int64_t heom_instance_matrices(const heom_handle* h, int32_t inst);
+/* First ADO of the instance in the concatenated state (reference uid order); -1 if out of range. */
+int64_t heom_instance_offset(const heom_handle* h, int32_t inst);
+int heom_set_instance_hamiltonian(heom_handle* h, int32_t inst, const double* hamiltonian);
+int heom_set_instance_top(heom_handle* h, int32_t inst, const double* host_top);
+int heom_get_instance_top(heom_handle* h, int32_t inst, double* host_top);
+
+/* Ensembles: instances of any sizes (states, depth, Matsubara terms, baths).
+ * Instances that can share a batch handle are grouped into one class (in
+ * order of first appearance); each class is a batch handle.  One RK4 step of
+ * the ensemble is one CUDA graph in which the classes' stage launches run as
+ * concurrent branches; the grid of every class's stage kernel is chosen by
+ * heom_ensemble_autotune, which times candidate shapes on the device (run
+ * automatically before the first step unless already done).  Admission
+ * computes the device footprint first and fails with HEOM_E_NOMEM, before
+ * allocating anything, when it exceeds the device's free memory. */
+typedef struct heom_ensemble heom_ensemble;
+/* Device bytes an ensemble of these instances would hold (states, stage
+ * buffers and tables); host-only, no device needed. */
+int heom_ensemble_footprint(const heom_instance_desc* descs, int32_t count, const heom_options* opt,
+                            size_t* bytes);
+int heom_ensemble_create(const heom_instance_desc* descs, int32_t count, const heom_options* opt,
+                         heom_ensemble** out);
+int heom_ensemble_destroy(heom_ensemble* e);
+int32_t heom_ensemble_instances(const heom_ensemble* e);
+int32_t heom_ensemble_classes(const heom_ensemble* e);
+/* class of an instance and its index inside that class's batch handle */
+int heom_ensemble_locate(const heom_ensemble* e, int32_t inst, int32_t* cls, int32_t* index);
+/* borrowed batch handle of a class (valid until heom_ensemble_destroy) */
+heom_handle* heom_ensemble_class(heom_ensemble* e, int32_t cls);
+int heom_ensemble_set_hamiltonian(heom_ensemble* e, int32_t inst, const double* hamiltonian);
+int heom_ensemble_set_top(heom_ensemble* e, int32_t inst, const double* host_top);
+int heom_ensemble_get_top(heom_ensemble* e, int32_t inst, double* host_top);
+/* Time the candidate stage-kernel grids (on the stage buffers, not on the
+ * states) and keep the fastest; *best_stage_us (may be NULL) receives the
+ * time of one stage of all classes with the chosen grids. */
+int heom_ensemble_autotune(heom_ensemble* e, double* best_stage_us);
+int heom_ensemble_rk4_steps(heom_ensemble* e, double dt, int64_t steps);
+/* As heom_propagate for every instance: host_tops holds rows of
+ * heom_ensemble_top_row_len doubles; instance k's top (states_k^2 complex)
+ * starts at heom_ensemble_top_offset(e, k) within each row. */
+int heom_ensemble_propagate(heom_ensemble* e, double dt, int64_t steps, int64_t observe_every,
+                            double* host_tops);
+int64_t heom_ensemble_top_row_len(const heom_ensemble* e);
+int64_t heom_ensemble_top_offset(const heom_ensemble* e, int32_t inst);
+/* kernel launches of all classes, graph nodes counted one by one */
+int64_t heom_ensemble_kernel_launches(const heom_ensemble* e);
+/* the ensemble's CUDA stream (a cudaStream_t); steps are enqueued on it */
+void* heom_ensemble_stream(heom_ensemble* e);
+
+/* ------------------------------------------------------------------------
  * Host set-up: the reference's hierarchy_graph + instance construction
  * (dm-heom/src/heom/hierarchy_graph.cpp:30-181, instance.cpp:25-71,155-273)
  * and config parsing (config.cpp:20-191, population_dynamics_config.cpp).

@@ -27,16 +27,20 @@ int main()
         for (int W = 1; W <= 64; ++W)
             for (int depth = 1; depth <= 40; ++depth) {
                 const int LS = depth + 1, NW = (2 * W + 3) & ~3, TWB = (W + 15) & ~15;
-                const heomk::PairSmem L = heomk::pair_smem_layout(n, W, NW, TWB, LS);
-                const int kmin = 0, h = 3 * W * LS * 16, cplus = h + n * n * 16, hr = cplus + W * LS * 8;
-                const int end = hr + n * (n + 1) * 8;
-                if (kmin % 16 || h % 16 || cplus % 8 || hr % 8 || end > L.lut) { printf("bad lut n=%d W=%d LS=%d\n", n, W, LS); ++bad; }
-                if (L.lut % 16 || L.slot % 16 || L.team % 16 || L.tile_off % 16 || L.nbr_off % 16 ||
-                    L.tup_off % 16 || L.pss_off % 16) { printf("bad slot n=%d W=%d\n", n, W); ++bad; }
-                if (L.nbr_off - L.tile_off < n * (n + 1) * 16 || L.tup_off - L.nbr_off < NW * 4 ||
-                    L.pss_off - L.tup_off < TWB || L.slot - L.pss_off < 16) { printf("bad sizes n=%d W=%d\n", n, W); ++bad; }
-                if (NW % 4 || NW < 2 * W || TWB % 16 || TWB < W) { printf("bad pads W=%d\n", W); ++bad; }
-                ++checked;
+                for (int hk = 0; hk < 2; ++hk) {
+                    const heomk::PairSmem L = heomk::pair_smem_layout(n, W, NW, TWB, LS, hk);
+                    const int kmin = 0, cplus = 3 * W * LS * 16, end = cplus + W * LS * 8;
+                    if (kmin % 16 || cplus % 16 || end > L.lut) { printf("bad lut n=%d W=%d LS=%d\n", n, W, LS); ++bad; }
+                    if (L.lut % 16 || L.slot % 16 || L.team % 16 || L.tile_off % 16 || L.nbr_off % 16 ||
+                        L.tup_off % 16 || L.pss_off % 16 || L.h_off % 16) { printf("bad slot n=%d W=%d\n", n, W); ++bad; }
+                    const int hbytes = hk == heomk::H_REAL_SYM ? n * (n + 1) * 8 : n * n * 16;
+                    if (hbytes % 16) { printf("bad H bytes n=%d hk=%d\n", n, hk); ++bad; }
+                    if (L.nbr_off - L.tile_off < n * (n + 1) * 16 || L.tup_off - L.nbr_off < NW * 4 ||
+                        L.pss_off - L.tup_off < TWB || L.h_off - L.pss_off < 16 || L.slot - L.h_off < hbytes)
+                        { printf("bad sizes n=%d W=%d\n", n, W); ++bad; }
+                    if (NW % 4 || NW < 2 * W || TWB % 16 || TWB < W) { printf("bad pads W=%d\n", W); ++bad; }
+                    ++checked;
+                }
             }
     }
     // searched sector tables for N <= 8: coverage, and for N = 8 conflict-free

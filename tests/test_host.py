@@ -164,3 +164,28 @@ def test_create_without_gpu_fails_loudly():
     with pytest.raises(hb.HeomError) as e:
         hb.Heom(**_good_desc())
     assert "heom error -2" in str(e.value)
+
+
+def test_ensemble_footprint_groups_classes():
+    # host-only: the admission arithmetic needs no device
+    t3 = hb.build_tables(hb.System(ho.synthetic_hamiltonian(3, 2), [35] * 3, [50] * 3, [0] * 3, 1, 300.0, 2))
+    t3b = dict(t3, hamiltonian=hb.build_tables(hb.System(ho.synthetic_hamiltonian(3, 4), [35] * 3, [50] * 3,
+                                                         [0] * 3, 1, 300.0, 2))["hamiltonian"])
+    t5 = hb.build_tables(hb.System(ho.synthetic_hamiltonian(5, 2), [35] * 5, [50] * 5, [0] * 5, 2, 300.0, 3))
+    one3, one5 = hb.Ensemble.footprint([t3]), hb.Ensemble.footprint([t5])
+    # product scheme: state + 2 stage buffers of nodes x sectors x 32 B, plus tables
+    assert one5 >= t5["matrices"] * 15 * 32 * 3
+    both = hb.Ensemble.footprint([t3, t5])
+    assert both == one3 + one5
+    # two instances of one class share a handle: states add, and each ADO carries an instance id
+    pair = hb.Ensemble.footprint([t3, t3b])
+    assert pair > 2 * t3["matrices"] * 5 * 32 * 3 and pair <= 2 * one3 + 4 * 2 * t3["matrices"]
+    assert hb.Ensemble.footprint([t3], scheme="reference") > one3
+
+
+def test_batch_admission_rejects_mixed_classes():
+    t3 = hb.build_tables(hb.System(ho.synthetic_hamiltonian(3, 2), [35] * 3, [50] * 3, [0] * 3, 1, 300.0, 2))
+    t3l = hb.build_tables(hb.System(ho.synthetic_hamiltonian(3, 2), [40] * 3, [50] * 3, [0] * 3, 1, 300.0, 2))
+    with pytest.raises(hb.HeomError) as e:
+        hb.Heom.batch([t3, t3l])
+    assert "heom error -1" in str(e.value) and "bath tables differ" in str(e.value)
