@@ -199,14 +199,17 @@ __device__ __forceinline__ void prefetch_ado(unsigned char* slot, const PairPara
     if (lt == 0) cp_async16(slot + L.pss_off, p.pss + u);
 }
 
-template <int N, int HK, int SLT>
+// ADJ: the adjoint operator L^H (see heom_dmma_stage); the coefficient
+// tables are indexed by the tuple entry n: cplus(n) = chat sqrt(n+1) and
+// kappa(n) = khat sqrt(n), so L^H takes cplus(n-1) and conj(kappa(n+1)).
+template <int N, int HK, int SLT, bool ADJ>
 __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_pair_stage(const PairParams p)
 {
     constexpr int P = pairs_of(N);
     constexpr int TW = team_warps(N);
     constexpr int TT = 32 * TW;
     constexpr int TEAMS = kCtaWarps / TW;
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     const PairSmem L = pair_smem_layout(N, p.W, p.NW, p.TWB, p.LS, HK);
     const int W = p.W, LS = p.LS, SL = p.SL;
 
@@ -335,13 +338,18 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_pair_stage(const PairP
 #pragma unroll
             for (int sd = 0; sd < 2; ++sd) {
                 double2 xp[SLT][2], xm[SLT][2];
-                int ix[SLT];
+                int ix[SLT], ik[SLT];
 #pragma unroll
                 for (int q = 0; q < SLT; ++q) {
                     const int sl = sd == 0 ? sli[q] : slj[q];
-                    const int32_t vp = (sl >= 0 && !diag) ? nb[sl] : -1;
-                    const int32_t vm = sl >= 0 ? nb[W + sl] : -1;
+                    const int32_t vp = (sl >= 0 && (ADJ || !diag)) ? nb[sl] : -1;
+                    const int32_t vm = (sl >= 0 && (!ADJ || !diag)) ? nb[W + sl] : -1;
                     ix[q] = sl >= 0 ? (sl * LS + tu[sl]) : 0;
+                    ik[q] = ix[q];
+                    if (ADJ) { // table entries of L^H: cplus at n-1 (minus neighbour), kappa at n+1 (plus neighbour)
+                        ik[q] = vp >= 0 ? ix[q] + 1 : ix[q];
+                        ix[q] = vm >= 0 ? ix[q] - 1 : ix[q];
+                    }
                     xp[q][0] = xp[q][1] = xm[q][0] = xm[q][1] = make_double2(0.0, 0.0);
                     if (vp >= 0) {
                         const double2* src = p.in + (int64_t)vp * (2 * P) + 2 * lt;
@@ -358,23 +366,31 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_pair_stage(const PairP
                 for (int q = 0; q < SLT; ++q) {
                     const int sl = sd == 0 ? sli[q] : slj[q];
                     if (sl < 0) continue;
-                    const double c = diag ? 0.0 : s_cplus[ix[q]];
+                    // L: i-coefficient on the plus neighbour, kappa on the minus one;
+                    // L^H: -i cplus(n-1) on the minus neighbour, conj(kappa(n+1)) on the plus one
+                    const double c = diag ? 0.0 : (ADJ ? -s_cplus[ix[q]] : s_cplus[ix[q]]);
+                    const double2 t1 = ADJ ? xm[q][0] : xp[q][0], t2 = ADJ ? xm[q][1] : xp[q][1];
+                    const double2 k1 = ADJ ? xp[q][0] : xm[q][0], k2 = ADJ ? xp[q][1] : xm[q][1];
+                    auto kap = [&](const double2* tab) {
+                        const double2 v = tab[ik[q]];
+                        return ADJ ? make_double2(v.x, -v.y) : v;
+                    };
                     if (sd == 0) {
                         // site i: element 1 (i,j) i-side (+i c, kappa_i); element 2 (j,i) j-side (-i c, kappa_j)
-                        L1.x = fma(-c, xp[q][0].y, L1.x);
-                        L1.y = fma(c, xp[q][0].x, L1.y);
-                        L2.x = fma(c, xp[q][1].y, L2.x);
-                        L2.y = fma(-c, xp[q][1].x, L2.y);
-                        cmac(L1, kap_i1[ix[q]], xm[q][0]);
-                        if (!diag) cmac(L2, kap_i2[ix[q]], xm[q][1]);
+                        L1.x = fma(-c, t1.y, L1.x);
+                        L1.y = fma(c, t1.x, L1.y);
+                        L2.x = fma(c, t2.y, L2.x);
+                        L2.y = fma(-c, t2.x, L2.y);
+                        cmac(L1, kap(kap_i1), k1);
+                        if (!diag) cmac(L2, kap(kap_i2), k2);
                     } else {
                         // site j: element 1 j-side (-i c, kappa_j); element 2 i-side (+i c, kappa_i)
-                        L1.x = fma(c, xp[q][0].y, L1.x);
-                        L1.y = fma(-c, xp[q][0].x, L1.y);
-                        L2.x = fma(-c, xp[q][1].y, L2.x);
-                        L2.y = fma(c, xp[q][1].x, L2.y);
-                        if (!diag) cmac(L1, kap_j1[ix[q]], xm[q][0]);
-                        cmac(L2, kap_j2[ix[q]], xm[q][1]);
+                        L1.x = fma(c, t1.y, L1.x);
+                        L1.y = fma(-c, t1.x, L1.y);
+                        L2.x = fma(-c, t2.y, L2.x);
+                        L2.y = fma(c, t2.x, L2.y);
+                        if (!diag) cmac(L1, kap(kap_j1), k1);
+                        cmac(L2, kap(kap_j2), k2);
                     }
                 }
             }
@@ -544,8 +560,12 @@ __host__ inline size_t dmma_smem_bytes(int P, int W, int NW, int TWB, int LS)
 }
 
 // MI: the handle holds several instances (p.inst set); each ADO's instance
-// selects its H fragments, reloaded whenever the instance changes
-template <int N, int HK, int SLT, bool MI>
+// selects its H fragments, reloaded whenever the instance changes.
+// ADJ: apply the adjoint operator L^H instead of L.  The caller passes the
+// tables of -H^H (fragments), conj(pf_same_sum) and conj(gamma0); in the bath
+// terms the roles of the neighbours swap: the plus neighbour enters with
+// conj(khat) sqrt(n+1), the minus neighbour with -/+ i chat sqrt(n).
+template <int N, int HK, int SLT, bool MI, bool ADJ>
 __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_dmma_stage(const DmmaParams dp)
 {
     static_assert(N <= 8, "DMMA stage handles N <= 8");
@@ -713,8 +733,9 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_dmma_stage(const DmmaP
 #pragma unroll
                 for (int q = 0; q < SLT; ++q) {
                     const int sl = sd == 0 ? sli[q] : slj[q];
-                    const int32_t vp = (sl >= 0 && !diag) ? nb[sl] : -1;
-                    const int32_t vm = sl >= 0 ? nb[W + sl] : -1;
+                    // diagonal elements: the plus terms of L cancel (the minus terms of L^H)
+                    const int32_t vp = (sl >= 0 && (ADJ || !diag)) ? nb[sl] : -1;
+                    const int32_t vm = (sl >= 0 && (!ADJ || !diag)) ? nb[W + sl] : -1;
                     nn[q] = sl >= 0 ? tu[sl] : 0;
                     xp[q][0] = xp[q][1] = xm[q][0] = xm[q][1] = make_double2(0.0, 0.0);
                     if (vp >= 0) ld256(p.in + (int64_t)vp * (2 * P) + 2 * lane, xp[q][0], xp[q][1]);
@@ -725,25 +746,36 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_dmma_stage(const DmmaP
                     const int sl = sd == 0 ? sli[q] : slj[q];
                     if (sl < 0) continue;
                     const int ps = sd == 0 ? pi[q] : pj[q];
-                    const double sqn = s_sq[nn[q]];
-                    const double c = diag ? 0.0 : s_ch[ps] * s_sq[nn[q] + 1];
-                    // minus neighbours scale as sqrt(n); fold it into the neighbour value
-                    const double2 m1 = make_double2(xm[q][0].x * sqn, xm[q][0].y * sqn);
-                    const double2 m2 = make_double2(xm[q][1].x * sqn, xm[q][1].y * sqn);
+                    const double sq_lo = s_sq[nn[q]], sq_hi = s_sq[nn[q] + 1];
+                    // L:   i-coefficient term on the plus neighbour (chat sqrt(n+1)),
+                    //      complex term on the minus neighbour (khat sqrt(n))
+                    // L^H: i-coefficient term on the minus neighbour (-chat sqrt(n)),
+                    //      complex term on the plus neighbour (conj(khat) sqrt(n+1))
+                    const double c = diag ? 0.0 : (ADJ ? -s_ch[ps] * sq_lo : s_ch[ps] * sq_hi);
+                    const double sk = ADJ ? sq_hi : sq_lo;
+                    const double2 t1 = ADJ ? xm[q][0] : xp[q][0], t2 = ADJ ? xm[q][1] : xp[q][1];
+                    const double2 k1 = ADJ ? xp[q][0] : xm[q][0], k2 = ADJ ? xp[q][1] : xm[q][1];
+                    // the complex-coefficient neighbour scales as sqrt(n) (sqrt(n+1) for L^H); fold it in
+                    const double2 m1 = make_double2(k1.x * sk, k1.y * sk);
+                    const double2 m2 = make_double2(k2.x * sk, k2.y * sk);
+                    auto kap = [&](const double2* tab) {
+                        const double2 v = tab[ps];
+                        return ADJ ? make_double2(v.x, -v.y) : v;
+                    };
                     if (sd == 0) {
-                        L1.x = fma(-c, xp[q][0].y, L1.x);
-                        L1.y = fma(c, xp[q][0].x, L1.y);
-                        L2.x = fma(c, xp[q][1].y, L2.x);
-                        L2.y = fma(-c, xp[q][1].x, L2.y);
-                        cmac(L1, kap_i1[ps], m1);
-                        if (!diag) cmac(L2, kap_i2[ps], m2);
+                        L1.x = fma(-c, t1.y, L1.x);
+                        L1.y = fma(c, t1.x, L1.y);
+                        L2.x = fma(c, t2.y, L2.x);
+                        L2.y = fma(-c, t2.x, L2.y);
+                        cmac(L1, kap(kap_i1), m1);
+                        if (!diag) cmac(L2, kap(kap_i2), m2);
                     } else {
-                        L1.x = fma(c, xp[q][0].y, L1.x);
-                        L1.y = fma(-c, xp[q][0].x, L1.y);
-                        L2.x = fma(-c, xp[q][1].y, L2.x);
-                        L2.y = fma(c, xp[q][1].x, L2.y);
-                        if (!diag) cmac(L1, kap_j1[ps], m1);
-                        cmac(L2, kap_j2[ps], m2);
+                        L1.x = fma(c, t1.y, L1.x);
+                        L1.y = fma(-c, t1.x, L1.y);
+                        L2.x = fma(-c, t2.y, L2.x);
+                        L2.y = fma(c, t2.x, L2.y);
+                        if (!diag) cmac(L1, kap(kap_j1), m1);
+                        cmac(L2, kap(kap_j2), m2);
                     }
                 }
             }
@@ -874,6 +906,200 @@ __global__ void heom_write_top(double2* __restrict__ y, const double2* __restric
     for (int pr = threadIdx.x; pr < P; pr += blockDim.x) {
         y[(u * P + pr) * 2] = src[pe[2 * pr]];
         y[(u * P + pr) * 2 + 1] = src[pe[2 * pr + 1]];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint gradients.  For one RK4 stage factor F_k = I + beta_k h L of the
+// product form, dJ/dtheta gains Re(beta_k h <a, dL/dtheta w>), with a the
+// adjoint after the later factors and w the stage input (<x, y> = x^H y).
+//   H:      <a, dL/dH_ab w> = (i/hbar) Z(a,b),
+//           Z = sum_u (w_u^T conj(a_u) - conj(a_u) w_u^T)          (all a, b at once)
+//   lambda, gamma (shared by all baths): L is linear in its coefficient
+//           tables, so dL/dtheta is L with H = 0 and the tables replaced by
+//           their derivatives (dpss, dgamma0, dchat, dkhat).
+// One warp per ADO; lanes own sectors (pair layout).  Every block adds
+// weight * (its sum) to its own row of `partial` (deterministic; summed on
+// the host at the end).
+// ---------------------------------------------------------------------------
+struct GradParams {
+    const double2* __restrict__ a;     // adjoint (pair layout, internal order)
+    const double2* __restrict__ w;     // forward stage input
+    const int32_t* __restrict__ nbr;   // [nodes][NW] plus[W], minus[W]
+    const uint8_t* __restrict__ tup;   // [nodes][TWB]
+    const int16_t* __restrict__ pe;    // [2P] element indices of the sector halves
+    const int16_t* __restrict__ slots; // [N][SL] slot ids of each state, -1 padded
+    const double* __restrict__ dpss;   // [nodes] d pf_same_sum / d gamma (real)
+    const double2* __restrict__ dg0;   // [2][N*N] d gamma0 / d(lambda, gamma)
+    const double* __restrict__ dchat;  // [2][W] d chat
+    const double2* __restrict__ dkhat; // [2][3][W] d khat (side i, side j, diagonal)
+    const double* __restrict__ sq;     // [LS+1] sqrt(n)
+    double2 weight;                    // beta_k h
+    double2* partial;                  // [gridDim.x][N*N + 2]
+    int64_t nodes;
+    int N, P, W, NW, TWB, SL;
+};
+
+__host__ __device__ inline int grad_warp_bytes(int n) { return 2 * n * (n + 1) * 16; }
+__host__ inline size_t grad_smem_bytes(int n)
+{
+    return (size_t)kCtaWarps * grad_warp_bytes(n) + (size_t)kCtaWarps * (n * n + 2) * 16;
+}
+
+__global__ void __launch_bounds__(kCtaWarps * 32) heom_adjoint_grad(const GradParams g)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int N = g.N, P = g.P, W = g.W, SL = g.SL, NN = N * N;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double2* At = reinterpret_cast<double2*>(smem + warp * grad_warp_bytes(N)); // [N][N+1]
+    double2* Wt = At + N * (N + 1);
+    double2* red = reinterpret_cast<double2*>(smem + kCtaWarps * grad_warp_bytes(N)); // [warps][NN+2]
+    double2 zac[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) zac[r] = make_double2(0.0, 0.0);
+    double2 dl = make_double2(0.0, 0.0), dgm = dl;
+
+    const int64_t stride = (int64_t)gridDim.x * kCtaWarps;
+    for (int64_t u = (int64_t)blockIdx.x * kCtaWarps + warp; u < g.nodes; u += stride) {
+        const int32_t* nb = g.nbr + u * g.NW;
+        const uint8_t* tu = g.tup + u * g.TWB;
+        const double dps = g.dpss[u];
+        for (int p = lane; p < P; p += 32) {
+            const int e1 = g.pe[2 * p], e2 = g.pe[2 * p + 1];
+            const int i1 = e1 / N, j1 = e1 - i1 * N, i2 = e2 / N, j2 = e2 - i2 * N;
+            const double2 a1 = g.a[(u * P + p) * 2], a2 = g.a[(u * P + p) * 2 + 1];
+            const double2 w1 = g.w[(u * P + p) * 2], w2 = g.w[(u * P + p) * 2 + 1];
+            At[i1 * (N + 1) + j1] = a1;
+            At[i2 * (N + 1) + j2] = a2;
+            Wt[i1 * (N + 1) + j1] = w1;
+            Wt[i2 * (N + 1) + j2] = w2;
+            const bool diag = i1 == j1;
+            const bool twin = e2 == e1; // padding half of an odd diagonal pair
+            // derivative of the operator applied to w, for theta = lambda (0), gamma (1)
+            double2 D1[2], D2[2];
+            for (int th = 0; th < 2; ++th) {
+                const double2 s1 = g.dg0[th * NN + e1], s2 = g.dg0[th * NN + e2];
+                const double sp = th == 1 ? dps : 0.0;
+                D1[th] = make_double2((sp + s1.x) * w1.x - s1.y * w1.y, (sp + s1.x) * w1.y + s1.y * w1.x);
+                D2[th] = make_double2((sp + s2.x) * w2.x - s2.y * w2.y, (sp + s2.x) * w2.y + s2.y * w2.x);
+            }
+            // bath terms: side 0 = slots of site i1, side 1 = slots of site j1
+            // (diagonal pairs: element 1 takes the slots of i1, element 2 those of i2)
+            for (int sd = 0; sd < 2; ++sd) {
+                const int site = sd == 0 ? i1 : (diag ? i2 : j1);
+                for (int q = 0; q < SL; ++q) {
+                    const int sl = g.slots[site * SL + q];
+                    if (sl < 0) continue;
+                    const int n = tu[sl];
+                    const int32_t vp = diag ? -1 : nb[sl];
+                    const int32_t vm = nb[W + sl];
+                    double2 p1 = make_double2(0.0, 0.0), p2 = p1, m1 = p1, m2 = p1;
+                    if (vp >= 0) { p1 = g.w[((int64_t)vp * P + p) * 2]; p2 = g.w[((int64_t)vp * P + p) * 2 + 1]; }
+                    if (vm >= 0) { m1 = g.w[((int64_t)vm * P + p) * 2]; m2 = g.w[((int64_t)vm * P + p) * 2 + 1]; }
+                    const double shi = g.sq[n + 1], slo = g.sq[n];
+                    for (int th = 0; th < 2; ++th) {
+                        const double c = g.dchat[th * W + sl] * shi;
+                        const double2* kh = g.dkhat + th * 3 * W;
+                        if (diag) {
+                            // element (site, site): kappa_i + kappa_j only
+                            const double2 k = kh[2 * W + sl];
+                            double2& D = sd == 0 ? D1[th] : D2[th];
+                            cmac(D, make_double2(k.x * slo, k.y * slo), sd == 0 ? m1 : m2);
+                        } else if (sd == 0) {
+                            // site i: element 1 (i,j) i-side, element 2 (j,i) j-side
+                            D1[th].x -= c * p1.y; D1[th].y += c * p1.x;
+                            D2[th].x += c * p2.y; D2[th].y -= c * p2.x;
+                            const double2 ki = kh[sl], kj = kh[W + sl];
+                            cmac(D1[th], make_double2(ki.x * slo, ki.y * slo), m1);
+                            cmac(D2[th], make_double2(kj.x * slo, kj.y * slo), m2);
+                        } else {
+                            D1[th].x += c * p1.y; D1[th].y -= c * p1.x;
+                            D2[th].x -= c * p2.y; D2[th].y += c * p2.x;
+                            const double2 ki = kh[sl], kj = kh[W + sl];
+                            cmac(D1[th], make_double2(kj.x * slo, kj.y * slo), m1);
+                            cmac(D2[th], make_double2(ki.x * slo, ki.y * slo), m2);
+                        }
+                    }
+                }
+            }
+            // <a, D>: conj(a) * D over the sector's elements (a padding half counts once)
+            double2* acc[2] = {&dl, &dgm};
+            for (int th = 0; th < 2; ++th) {
+                acc[th]->x += a1.x * D1[th].x + a1.y * D1[th].y;
+                acc[th]->y += a1.x * D1[th].y - a1.y * D1[th].x;
+                if (!twin) {
+                    acc[th]->x += a2.x * D2[th].x + a2.y * D2[th].y;
+                    acc[th]->y += a2.x * D2[th].y - a2.y * D2[th].x;
+                }
+            }
+        }
+        __syncwarp();
+        // Z(k,l) = sum_i w(i,k) conj(a(i,l)) - sum_j conj(a(k,j)) w(l,j)
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            const int q = lane + 32 * r;
+            if (q >= NN) break;
+            const int k = q / N, l = q - k * N;
+            double zr = 0.0, zi = 0.0;
+            for (int i = 0; i < N; ++i) {
+                const double2 wv = Wt[i * (N + 1) + k], av = At[i * (N + 1) + l];
+                zr += wv.x * av.x + wv.y * av.y;
+                zi += wv.y * av.x - wv.x * av.y;
+                const double2 ak = At[k * (N + 1) + i], wl = Wt[l * (N + 1) + i];
+                zr -= ak.x * wl.x + ak.y * wl.y;
+                zi -= ak.x * wl.y - ak.y * wl.x;
+            }
+            zac[r].x += zr;
+            zac[r].y += zi;
+        }
+        __syncwarp();
+    }
+    // block sum in a fixed order, then weight * sum into this block's row
+    double2* mine = red + warp * (NN + 2);
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        const int q = lane + 32 * r;
+        if (q < NN) mine[q] = zac[r];
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        dl.x += __shfl_down_sync(0xffffffffu, dl.x, off);
+        dl.y += __shfl_down_sync(0xffffffffu, dl.y, off);
+        dgm.x += __shfl_down_sync(0xffffffffu, dgm.x, off);
+        dgm.y += __shfl_down_sync(0xffffffffu, dgm.y, off);
+    }
+    if (lane == 0) {
+        mine[NN] = dl;
+        mine[NN + 1] = dgm;
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < NN + 2; q += blockDim.x) {
+        double2 s = make_double2(0.0, 0.0);
+        for (int v = 0; v < kCtaWarps; ++v) {
+            s.x += red[v * (NN + 2) + q].x;
+            s.y += red[v * (NN + 2) + q].y;
+        }
+        double2& out = g.partial[(int64_t)blockIdx.x * (NN + 2) + q];
+        out.x += g.weight.x * s.x - g.weight.y * s.y;
+        out.y += g.weight.x * s.y + g.weight.y * s.x;
+    }
+}
+
+// y[top] += weight * O (O row-major n x n complex), pair layout; one block
+__global__ void heom_add_top(double2* __restrict__ y, const double2* __restrict__ obs,
+                             const int16_t* __restrict__ pe, int64_t top, int P, double weight)
+{
+    for (int pr = threadIdx.x; pr < P; pr += blockDim.x) {
+        const int e1 = pe[2 * pr], e2 = pe[2 * pr + 1];
+        double2& h1 = y[(top * P + pr) * 2];
+        double2& h2 = y[(top * P + pr) * 2 + 1];
+        h1.x += weight * obs[e1].x;
+        h1.y += weight * obs[e1].y;
+        if (e2 != e1) {
+            h2.x += weight * obs[e2].x;
+            h2.y += weight * obs[e2].y;
+        } else {
+            h2 = h1; // padding half mirrors its element
+        }
     }
 }
 

@@ -19,6 +19,7 @@
 
 #include "heom_b200.h"
 #include "heom_kernels.cuh"
+#include "host/heom_host.hpp"
 
 namespace {
 #include "pair_tables.inc"
@@ -93,28 +94,32 @@ struct DevBuf {
 typedef void (*stage_fn_t)(const PairParams);
 typedef void (*dmma_fn_t)(const heomk::DmmaParams);
 
-template <int N, int HK>
+template <int N, int HK, bool ADJ>
 stage_fn_t pick_slt(int slt)
 {
     switch (slt) {
-    case 2: return heomk::heom_pair_stage<N, HK, 2>;
-    case 4: return heomk::heom_pair_stage<N, HK, 4>;
-    default: return heomk::heom_pair_stage<N, HK, 8>;
+    case 2: return heomk::heom_pair_stage<N, HK, 2, ADJ>;
+    case 4: return heomk::heom_pair_stage<N, HK, 4, ADJ>;
+    default: return heomk::heom_pair_stage<N, HK, 8, ADJ>;
     }
 }
 
 template <int N>
-stage_fn_t pick_n(int hk, int slt)
+stage_fn_t pick_n(int hk, int slt, bool adj)
 {
-    return hk == heomk::H_REAL_SYM ? pick_slt<N, heomk::H_REAL_SYM>(slt) : pick_slt<N, heomk::H_GENERIC>(slt);
+    if (adj)
+        return hk == heomk::H_REAL_SYM ? pick_slt<N, heomk::H_REAL_SYM, true>(slt)
+                                       : pick_slt<N, heomk::H_GENERIC, true>(slt);
+    return hk == heomk::H_REAL_SYM ? pick_slt<N, heomk::H_REAL_SYM, false>(slt)
+                                   : pick_slt<N, heomk::H_GENERIC, false>(slt);
 }
 
 // SIMT pair kernel: N = 9..16
-stage_fn_t pick_stage(int n, int hk, int slt)
+stage_fn_t pick_stage(int n, int hk, int slt, bool adj)
 {
     switch (n) {
 #define HEOM_CASE(K) \
-    case K: return pick_n<K>(hk, slt);
+    case K: return pick_n<K>(hk, slt, adj);
         HEOM_CASE(9) HEOM_CASE(10) HEOM_CASE(11) HEOM_CASE(12)
         HEOM_CASE(13) HEOM_CASE(14) HEOM_CASE(15) HEOM_CASE(16)
 #undef HEOM_CASE
@@ -122,41 +127,52 @@ stage_fn_t pick_stage(int n, int hk, int slt)
     }
 }
 
-template <int N, int HK, bool MI>
+template <int N, int HK, bool MI, bool ADJ>
 dmma_fn_t pick_dslt(int slt)
 {
     switch (slt) {
-    case 2: return heomk::heom_dmma_stage<N, HK, 2, MI>;
-    case 4: return heomk::heom_dmma_stage<N, HK, 4, MI>;
-    default: return heomk::heom_dmma_stage<N, HK, 8, MI>;
+    case 2: return heomk::heom_dmma_stage<N, HK, 2, MI, ADJ>;
+    case 4: return heomk::heom_dmma_stage<N, HK, 4, MI, ADJ>;
+    default: return heomk::heom_dmma_stage<N, HK, 8, MI, ADJ>;
     }
 }
 
-template <int N, bool MI>
-dmma_fn_t pick_dhk(int hk, int slt)
+// variants: one instance, several instances (batch), adjoint of one instance
+template <int N, int HK>
+dmma_fn_t pick_dmode(int slt, bool multi, bool adj)
 {
-    return hk == heomk::H_REAL_SYM ? pick_dslt<N, heomk::H_REAL_SYM, MI>(slt)
-                                   : pick_dslt<N, heomk::H_GENERIC, MI>(slt);
+    if (adj) return pick_dslt<N, HK, false, true>(slt);
+    return multi ? pick_dslt<N, HK, true, false>(slt) : pick_dslt<N, HK, false, false>(slt);
 }
 
 template <int N>
-dmma_fn_t pick_dn(int hk, int slt, bool multi)
+dmma_fn_t pick_dn(int hk, int slt, bool multi, bool adj)
 {
-    return multi ? pick_dhk<N, true>(hk, slt) : pick_dhk<N, false>(hk, slt);
+    return hk == heomk::H_REAL_SYM ? pick_dmode<N, heomk::H_REAL_SYM>(slt, multi, adj)
+                                   : pick_dmode<N, heomk::H_GENERIC>(slt, multi, adj);
 }
 
 // tensor-pipe kernel: N = 1..8
-dmma_fn_t pick_dmma(int n, int hk, int slt, bool multi)
+dmma_fn_t pick_dmma(int n, int hk, int slt, bool multi, bool adj)
 {
     switch (n) {
 #define HEOM_CASE(K) \
-    case K: return pick_dn<K>(hk, slt, multi);
+    case K: return pick_dn<K>(hk, slt, multi, adj);
         HEOM_CASE(1) HEOM_CASE(2) HEOM_CASE(3) HEOM_CASE(4) HEOM_CASE(5) HEOM_CASE(6)
         HEOM_CASE(7) HEOM_CASE(8)
 #undef HEOM_CASE
     default: return nullptr;
     }
 }
+
+// tables of the adjoint operator L^H that replace the handle's own
+struct AdjTabs {
+    const double2* pss;    // conj(pf_same_sum)
+    const double2* gamma0; // conj(gamma0)
+    const double* hfrag;   // fragments of -H^H
+    const double* hr;      // -H (real symmetric H)
+    const double2* hs;     // -H^H
+};
 
 // stage write modes (runtime parameters of the one stage kernel)
 enum Epi : int {
@@ -246,7 +262,7 @@ struct heom_handle {
 
     // launch accounting and shape
     int64_t launches = 0;
-    int per_sm[2] = {0, 0};  // resident stage CTAs per SM, per H kind
+    int per_sm[2][2] = {{0, 0}, {0, 0}}; // resident stage CTAs per SM, per [adjoint][H kind]
     int grid_override = 0;   // stage grid chosen by an autotuner (0: one full wave)
     size_t stage_smem = 0;
 
@@ -304,55 +320,77 @@ int build_neighbours(heom_handle* h)
     return 0;
 }
 
-int upload_hamiltonian(heom_handle* h)
+// device-side forms of one instance's H (interleaved re/im, J): H / hbar
+// row-major (hs), its real part in padded rows (hr) and the MMA operand
+// fragments (frag, N <= 8: lane l = 4r + t, k-slice s: column c = 4s+t;
+// hb = H(c, r), ha = -H(r, c))
+void h_tables(const double* hk, int N, double2* hs, double* hr, double* frag)
 {
-    const int N = h->N, K = h->n_inst;
-    std::vector<double2> hs((size_t)K * N * N), g0(N * N);
-    std::vector<double> hr((size_t)K * N * (N + 1), 0.0);
-    std::vector<double> frag(N <= 8 ? (size_t)K * 256 : 0, 0.0);
-    bool real_sym = true;
-    for (int k = 0; k < K; ++k) {
-        const double* hk = h->ham.data() + (size_t)k * 2 * N * N;
-        for (int q = 0; q < N * N; ++q) {
-            hs[(size_t)k * N * N + q] = make_double2(hk[2 * q] / kHbar, hk[2 * q + 1] / kHbar);
-            if (hk[2 * q + 1] != 0.0) real_sym = false;
-            hr[(size_t)k * N * (N + 1) + (q / N) * (N + 1) + q % N] = hk[2 * q] / kHbar;
-        }
-        for (int i = 0; i < N && real_sym; ++i)
-            for (int j = 0; j < i; ++j)
-                if (hk[2 * (i * N + j)] != hk[2 * (j * N + i)]) real_sym = false;
-        // MMA operand fragments, lane l = 4r + t, k-slice s: column 4s+t
-        for (int l = 0; l < 32 && N <= 8; ++l) {
-            const int r = l >> 2, t = l & 3;
-            for (int sl = 0; sl < 2; ++sl) {
-                const int c = 4 * sl + t;
-                if (r >= N || c >= N) continue;
-                const double2 hcr = hs[(size_t)k * N * N + c * N + r]; // H(c, r)
-                const double2 hrc = hs[(size_t)k * N * N + r * N + c]; // H(r, c)
-                double* f = frag.data() + (size_t)k * 256 + l;
-                f[32 * (0 + sl)] = hcr.x;
-                f[32 * (2 + sl)] = hcr.y;
-                f[32 * (4 + sl)] = -hrc.x;
-                f[32 * (6 + sl)] = -hrc.y;
-            }
+    for (int q = 0; q < N * N; ++q) {
+        hs[q] = make_double2(hk[2 * q] / kHbar, hk[2 * q + 1] / kHbar);
+        hr[(q / N) * (N + 1) + q % N] = hk[2 * q] / kHbar;
+    }
+    for (int l = 0; l < 32 && N <= 8 && frag; ++l) {
+        const int r = l >> 2, t = l & 3;
+        for (int sl = 0; sl < 2; ++sl) {
+            const int c = 4 * sl + t;
+            if (r >= N || c >= N) continue;
+            const double2 hcr = hs[c * N + r], hrc = hs[r * N + c];
+            frag[32 * (0 + sl) + l] = hcr.x;
+            frag[32 * (2 + sl) + l] = hcr.y;
+            frag[32 * (4 + sl) + l] = -hrc.x;
+            frag[32 * (6 + sl) + l] = -hrc.y;
         }
     }
-    // real symmetric H (every instance) takes the cheaper kernel variants
-    h->hkind = real_sym ? heomk::H_REAL_SYM : heomk::H_GENERIC;
-    // same term (heom_ode.cl:138-168): for i != j subtract pf_same of every
-    // bath coupled to site i and to site j
+}
+
+bool real_symmetric(const double* hk, int N)
+{
+    for (int q = 0; q < N * N; ++q)
+        if (hk[2 * q + 1] != 0.0) return false;
+    for (int i = 0; i < N; ++i)
+        for (int j = 0; j < i; ++j)
+            if (hk[2 * (i * N + j)] != hk[2 * (j * N + i)]) return false;
+    return true;
+}
+
+// same term (heom_ode.cl:138-168): for i != j subtract pf_same of every bath
+// coupled to site i and to site j (linear in pf_same)
+std::vector<double2> gamma0_table(const heom_handle* h, const std::vector<double>& pf_same)
+{
+    const int N = h->N;
+    std::vector<double2> g0(N * N);
     for (int i = 0; i < N; ++i)
         for (int j = 0; j < N; ++j) {
             double gr = 0.0, gi = 0.0;
             if (i != j)
                 for (int b = 0; b < h->BPS; ++b) {
                     const int bi = h->coupling[i * h->BPS + b];
-                    if (bi >= 0) { gr -= h->pf_same[2 * bi]; gi -= h->pf_same[2 * bi + 1]; }
+                    if (bi >= 0) { gr -= pf_same[2 * bi]; gi -= pf_same[2 * bi + 1]; }
                     const int bj = h->coupling[j * h->BPS + b];
-                    if (bj >= 0) { gr -= h->pf_same[2 * bj]; gi -= h->pf_same[2 * bj + 1]; }
+                    if (bj >= 0) { gr -= pf_same[2 * bj]; gi -= pf_same[2 * bj + 1]; }
                 }
             g0[i * N + j] = make_double2(gr, gi);
         }
+    return g0;
+}
+
+int upload_hamiltonian(heom_handle* h)
+{
+    const int N = h->N, K = h->n_inst;
+    std::vector<double2> hs((size_t)K * N * N);
+    std::vector<double> hr((size_t)K * N * (N + 1), 0.0);
+    std::vector<double> frag(N <= 8 ? (size_t)K * 256 : 0, 0.0);
+    bool real_sym = true;
+    for (int k = 0; k < K; ++k) {
+        const double* hk = h->ham.data() + (size_t)k * 2 * N * N;
+        h_tables(hk, N, hs.data() + (size_t)k * N * N, hr.data() + (size_t)k * N * (N + 1),
+                 N <= 8 ? frag.data() + (size_t)k * 256 : nullptr);
+        real_sym = real_sym && real_symmetric(hk, N);
+    }
+    // real symmetric H (every instance) takes the cheaper kernel variants
+    h->hkind = real_sym ? heomk::H_REAL_SYM : heomk::H_GENERIC;
+    const std::vector<double2> g0 = gamma0_table(h, h->pf_same);
     if (!h->d_hs.p) {
         if (int rc = h->d_hs.alloc(hs.size())) return rc;
         if (int rc = h->d_hr.alloc(hr.size())) return rc;
@@ -490,22 +528,23 @@ int cta_threads(int n) { return (heomk::kCtaWarps / heomk::team_warps(n)) * heom
 int cta_teams(int n) { return heomk::kCtaWarps / heomk::team_warps(n); }
 
 // resolve the launch shape of the stage kernel (outside of any stream capture)
-int resolve_stage(heom_handle* h, const void** fn_out, int* blocks_out = nullptr)
+int resolve_stage(heom_handle* h, const void** fn_out, int* blocks_out = nullptr, bool adj = false)
 {
     const void* fn = nullptr;
     size_t smem = 0;
     int threads = 0;
+    if (adj && h->n_inst > 1) return fail(HEOM_E_UNSUPPORTED, "the adjoint runs on single-instance handles");
     if (h->N <= 8) {
-        fn = (const void*)pick_dmma(h->N, h->hkind, h->SLT, h->n_inst > 1);
+        fn = (const void*)pick_dmma(h->N, h->hkind, h->SLT, h->n_inst > 1, adj);
         smem = heomk::dmma_smem_bytes(h->P, h->W, h->NW, h->TWB, h->LS);
         threads = heomk::kCtaWarps * 32;
     } else {
-        fn = (const void*)pick_stage(h->N, h->hkind, h->SLT);
+        fn = (const void*)pick_stage(h->N, h->hkind, h->SLT, adj);
         smem = heomk::pair_smem_bytes(h->N, h->W, h->NW, h->TWB, h->LS, h->hkind);
         threads = cta_threads(h->N);
     }
     if (!fn) return fail(HEOM_E_UNSUPPORTED, "states = %d not supported", h->N);
-    int& per_sm = h->per_sm[h->hkind];
+    int& per_sm = h->per_sm[adj ? 1 : 0][h->hkind];
     if (per_sm == 0) {
         if (smem > 227 * 1024) return fail(HEOM_E_UNSUPPORTED, "stage kernel needs %zu B of shared memory", smem);
         if (int rc = allow_dynamic_smem(fn, smem)) return rc;
@@ -522,12 +561,19 @@ int resolve_stage(heom_handle* h, const void** fn_out, int* blocks_out = nullptr
 }
 
 int launch_stage(heom_handle* h, int epi, const double2* in, const double2* y, double2* out,
-                 double2* acc, double2 beta, int acc_init)
+                 double2* acc, double2 beta, int acc_init, const AdjTabs* adj = nullptr)
 {
     const void* fn = nullptr;
     int blocks = 0;
-    if (int rc = resolve_stage(h, &fn, &blocks)) return rc;
+    if (int rc = resolve_stage(h, &fn, &blocks, adj != nullptr)) return rc;
     PairParams p = base_params(h);
+    if (adj) {
+        p.pss = adj->pss;
+        p.gamma0 = adj->gamma0;
+        p.hfrag = adj->hfrag;
+        p.hr = adj->hr;
+        p.hs = adj->hs;
+    }
     p.in = in;
     p.out = out;
     switch (epi) {
@@ -1517,7 +1563,7 @@ int ens_autotune(heom_ensemble* e, double* best_us)
         const void* fn = nullptr;
         int blocks = 0;
         if (int rc = resolve_stage(h, &fn, &blocks)) return rc;
-        full[c] = h->per_sm[h->hkind] * h->sm_count;
+        full[c] = h->per_sm[0][h->hkind] * h->sm_count;
         groups[c] = blocks;
         work[c] = (double)h->nodes * h->P;
         total += work[c];
@@ -1866,5 +1912,332 @@ int64_t heom_ensemble_kernel_launches(const heom_ensemble* e)
 }
 
 void* heom_ensemble_stream(heom_ensemble* e) { return e ? (void*)e->stream : nullptr; }
+
+} // extern "C"
+
+// ---------------------------------------------------------------------------
+// Adjoint gradients of J = sum_n w_n Re(sum_ij conj(O_ij) rho_n(i,j)) over an
+// RK4 propagation (the product form: y_{n+1} = F_3 F_2 F_1 F_0 y_n with
+// F_k = I + beta_k dt L).  The adjoint g_n = dJ/dy_n obeys
+// g_n = w_n O_top + F_0^H F_1^H F_2^H F_3^H g_{n+1}, F_k^H = I + conj(beta_k) dt L^H,
+// and every factor adds Re(beta_k dt <a_k, dL/dtheta w_k>) to dJ/dtheta (a_k
+// the adjoint after F_k^H's successors, w_k the forward stage input).
+// Checkpoints every S = ceil(sqrt(steps)) steps; each segment's stage inputs
+// are recomputed (same kernels, bit-identical) before its backward sweep.
+// ---------------------------------------------------------------------------
+
+struct heom_adjoint {
+    heom_handle* h = nullptr;
+    AdjTabs tabs{};
+    DevBuf<double2> pss_adj, g0_adj, hs_adj;
+    DevBuf<double> hfrag_adj, hr_adj;
+    DevBuf<double> dpss;     // [nodes] d pf_same_sum / d gamma (internal order)
+    DevBuf<double2> dg0;     // [2][N*N]
+    DevBuf<double> dchat;    // [2][W]
+    DevBuf<double2> dkhat;   // [2][3][W]
+    DevBuf<double2> obs;     // [N*N]
+    DevBuf<double2> partial; // [grid][N*N + 2]
+    int grid = 0;
+    size_t grad_smem = 0;
+    DevBuf<double2> cps, seg, scratch, ga, gb, toplog;
+    int64_t cap_cps = 0, cap_seg = 0, cap_rows = 0;
+    ~heom_adjoint()
+    {
+        if (h) heom_destroy(h);
+    }
+};
+
+namespace {
+
+int adj_tables(heom_adjoint* A, const heomhost::system_params& sp)
+{
+    heom_handle* h = A->h;
+    const int N = h->N, W = h->W, M = h->M, B = h->B;
+    // L^H: conj(pf_same_sum), conj(gamma0), -H^H
+    std::vector<double2> pss(h->nodes);
+    for (int64_t r = 0; r < h->nodes; ++r)
+        pss[h->int_of_ref[r]] = make_double2(h->pss[2 * r], -h->pss[2 * r + 1]);
+    std::vector<double2> g0 = gamma0_table(h, h->pf_same);
+    for (auto& v : g0) v.y = -v.y;
+    std::vector<double> hadj(2 * N * N);
+    for (int i = 0; i < N; ++i)
+        for (int j = 0; j < N; ++j) {
+            hadj[2 * (i * N + j)] = -h->ham[2 * (j * N + i)];
+            hadj[2 * (i * N + j) + 1] = h->ham[2 * (j * N + i) + 1];
+        }
+    std::vector<double2> hs(N * N);
+    std::vector<double> hr(N * (N + 1), 0.0), frag(256, 0.0);
+    h_tables(hadj.data(), N, hs.data(), hr.data(), N <= 8 ? frag.data() : nullptr);
+    if (int rc = A->pss_adj.alloc(pss.size())) return rc;
+    if (int rc = A->g0_adj.alloc(g0.size())) return rc;
+    if (int rc = A->hs_adj.alloc(hs.size())) return rc;
+    if (int rc = A->hr_adj.alloc(hr.size())) return rc;
+    if (int rc = A->hfrag_adj.alloc(frag.size())) return rc;
+    CUDA_TRY(cudaMemcpy(A->pss_adj.p, pss.data(), pss.size() * 16, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(A->g0_adj.p, g0.data(), g0.size() * 16, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(A->hs_adj.p, hs.data(), hs.size() * 16, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(A->hr_adj.p, hr.data(), hr.size() * 8, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(A->hfrag_adj.p, frag.data(), frag.size() * 8, cudaMemcpyHostToDevice));
+    A->tabs = AdjTabs{A->pss_adj.p, A->g0_adj.p, A->hfrag_adj.p, A->hr_adj.p, A->hs_adj.p};
+
+    // derivative tables for theta = lambda (0), gamma (1)
+    heomhost::bath_derivs bd = heomhost::bath_derivatives(sp);
+    std::vector<double> dchat(2 * W, 0.0), dpss(h->nodes, 0.0);
+    std::vector<double2> dkhat(2 * 3 * W, make_double2(0.0, 0.0)), dg0(2 * N * N);
+    for (int th = 0; th < 2; ++th) {
+        for (int sl = 0; sl < W; ++sl) {
+            const int b = sl / M, m = sl - b * M;
+            const double cr = h->cbk[2 * sl], ci = h->cbk[2 * sl + 1];
+            const double dcr = bd.cbk[th][2 * sl], dci = bd.cbk[th][2 * sl + 1];
+            const double qr = m == 0 ? h->pf_circ[2 * b] : 0.0, qi = m == 0 ? h->pf_circ[2 * b + 1] : 0.0;
+            const double dqr = m == 0 ? bd.pf_circ[th][2 * b] : 0.0, dqi = m == 0 ? bd.pf_circ[th][2 * b + 1] : 0.0;
+            const double a = std::hypot(cr, ci), da = (cr * dcr + ci * dci) / a;
+            const double chat = std::sqrt(a / kHbar);
+            dchat[th * W + sl] = da / (2.0 * kHbar * chat);
+            const double sc = std::sqrt(kHbar / a), dsc = -0.5 * sc * da / a;
+            dkhat[th * 3 * W + sl] = make_double2(dsc * (-ci / kHbar + qr) + sc * (-dci / kHbar + dqr),
+                                                  dsc * (cr / kHbar + qi) + sc * (dcr / kHbar + dqi));
+            dkhat[th * 3 * W + W + sl] = make_double2(dsc * (ci / kHbar + qr) + sc * (dci / kHbar + dqr),
+                                                      dsc * (-cr / kHbar + qi) + sc * (-dcr / kHbar + dqi));
+            dkhat[th * 3 * W + 2 * W + sl] = make_double2(2.0 * (dsc * qr + sc * dqr), 2.0 * (dsc * qi + sc * dqi));
+        }
+        const std::vector<double2> g = gamma0_table(h, bd.pf_same[th]);
+        std::copy(g.begin(), g.end(), dg0.begin() + th * N * N);
+    }
+    (void)B;
+    for (int64_t r = 0; r < h->nodes; ++r) {
+        double v = 0.0;
+        for (int b = 0; b < h->B; ++b) v -= h->tuples[r * W + b * M];
+        dpss[h->int_of_ref[r]] = v;
+    }
+    if (int rc = A->dchat.alloc(dchat.size())) return rc;
+    if (int rc = A->dkhat.alloc(dkhat.size())) return rc;
+    if (int rc = A->dg0.alloc(dg0.size())) return rc;
+    if (int rc = A->dpss.alloc(dpss.size())) return rc;
+    CUDA_TRY(cudaMemcpy(A->dchat.p, dchat.data(), dchat.size() * 8, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(A->dkhat.p, dkhat.data(), dkhat.size() * 16, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(A->dg0.p, dg0.data(), dg0.size() * 16, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(A->dpss.p, dpss.data(), dpss.size() * 8, cudaMemcpyHostToDevice));
+    return 0;
+}
+
+int adj_grad(heom_adjoint* A, const double2* a, const double2* w, double2 weight)
+{
+    heom_handle* h = A->h;
+    heomk::GradParams g{};
+    g.a = a;
+    g.w = w;
+    g.nbr = h->d_nbr.p;
+    g.tup = h->d_tup.p;
+    g.pe = h->d_pair.p;
+    g.slots = h->d_slots.p;
+    g.dpss = A->dpss.p;
+    g.dg0 = A->dg0.p;
+    g.dchat = A->dchat.p;
+    g.dkhat = A->dkhat.p;
+    g.sq = h->d_sq.p;
+    g.weight = weight;
+    g.partial = A->partial.p;
+    g.nodes = h->nodes;
+    g.N = h->N;
+    g.P = h->P;
+    g.W = h->W;
+    g.NW = h->NW;
+    g.TWB = h->TWB;
+    g.SL = h->SL;
+    heomk::heom_adjoint_grad<<<A->grid, heomk::kCtaWarps * 32, A->grad_smem, h->stream>>>(g);
+    h->launches++;
+    CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+int adj_add_top(heom_adjoint* A, double2* y, double weight)
+{
+    heom_handle* h = A->h;
+    if (weight == 0.0) return 0;
+    heomk::heom_add_top<<<1, 128, 0, h->stream>>>(y, A->obs.p, h->d_pair.p, h->top_int[0], h->P, weight);
+    h->launches++;
+    CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+} // namespace
+
+extern "C" {
+
+int heom_adjoint_create(const heom_system_desc* sys, const heom_options* opt, heom_adjoint** out)
+{
+    if (!sys || !out) return fail(HEOM_E_ARG, "NULL argument");
+    *out = nullptr;
+    std::unique_ptr<heom_adjoint> A(new heom_adjoint());
+    heomhost::system_params sp;
+    heomhost::instance inst;
+    try {
+        sp = heomhost::system_from_desc(*sys);
+        inst = heomhost::make_instance(sp);
+    } catch (const heomhost::config_error& e) {
+        return fail(HEOM_E_CONFIG, "%s", e.what());
+    } catch (const std::exception& e) {
+        return fail(HEOM_E_ARG, "%s", e.what());
+    }
+    heom_options o;
+    heom_default_options(&o);
+    if (opt) o = *opt;
+    o.rk4_scheme = HEOM_RK4_PRODUCT; // the backward sweep differentiates the product form
+    const heom_instance_desc d = inst.desc();
+    if (int rc = heom_create(&d, &o, &A->h)) return rc;
+    heom_handle* h = A->h;
+    CUDA_TRY(cudaSetDevice(h->device));
+    if (int rc = adj_tables(A.get(), sp)) return rc;
+    if (int rc = A->obs.alloc((size_t)h->N * h->N)) return rc;
+    A->grid = (int)std::max<int64_t>(1, std::min<int64_t>((h->nodes + heomk::kCtaWarps - 1) / heomk::kCtaWarps,
+                                                        (int64_t)h->sm_count * 2));
+    if (int rc = A->partial.alloc((size_t)A->grid * (h->N * h->N + 2))) return rc;
+    A->grad_smem = heomk::grad_smem_bytes(h->N);
+    if (int rc = allow_dynamic_smem((const void*)heomk::heom_adjoint_grad, A->grad_smem)) return rc;
+    *out = A.release();
+    return 0;
+}
+
+int heom_adjoint_destroy(heom_adjoint* A)
+{
+    if (!A) return 0;
+    cudaSetDevice(A->h ? A->h->device : 0);
+    delete A;
+    return 0;
+}
+
+heom_handle* heom_adjoint_handle(heom_adjoint* A) { return A ? A->h : nullptr; }
+
+int heom_adjoint_gradient(heom_adjoint* A, const double* rho0, const double* observable, const double* weights,
+                          double dt, int64_t steps, double* loss, double* grad_h, double* grad_lambda,
+                          double* grad_gamma, double* grad_rho0)
+{
+    if (!A || !rho0 || !observable || !weights || steps < 1 || !(dt > 0.0))
+        return fail(HEOM_E_ARG, "bad argument");
+    heom_handle* h = A->h;
+    CUDA_TRY(cudaSetDevice(h->device));
+    const int N = h->N, NN = N * N;
+    const size_t st = h->state_elems();
+    const int64_t S = std::max<int64_t>(1, (int64_t)std::ceil(std::sqrt((double)steps)));
+    const int64_t ncp = (steps + S - 1) / S;
+    // device memory: checkpoints, stage inputs of one segment, adjoint ping-pong, one scratch state
+    {
+        size_t free_b = 0, total_b = 0;
+        CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+        const int64_t need_states = (ncp > A->cap_cps ? ncp : 0) + (4 * S > A->cap_seg ? 4 * S : 0) + 3;
+        if ((double)need_states * st * 16 > (double)free_b)
+            return fail(HEOM_E_NOMEM, "adjoint needs %.3f GB of device memory (%lld checkpoints, segments of %lld steps)",
+                        need_states * st * 16 / 1e9, (long long)ncp, (long long)S);
+    }
+    if (ncp > A->cap_cps) {
+        if (int rc = A->cps.alloc(ncp * st)) return rc;
+        A->cap_cps = ncp;
+    }
+    if (4 * S > A->cap_seg) {
+        if (int rc = A->seg.alloc(4 * S * st)) return rc;
+        A->cap_seg = 4 * S;
+    }
+    if (!A->ga.p) {
+        if (int rc = A->ga.alloc(st)) return rc;
+        if (int rc = A->gb.alloc(st)) return rc;
+        if (int rc = A->scratch.alloc(st)) return rc;
+    }
+    if (steps + 1 > A->cap_rows) {
+        if (int rc = A->toplog.alloc((steps + 1) * NN)) return rc;
+        A->cap_rows = steps + 1;
+    }
+    if (int rc = prepare_scheme(h)) return rc;
+    CUDA_TRY(cudaMemcpy(A->obs.p, observable, NN * 16, cudaMemcpyHostToDevice));
+
+    // ---- forward: checkpoints and the observed tops ----
+    CUDA_TRY(cudaMemsetAsync(h->y.data.p, 0, st * 16, h->stream));
+    CUDA_TRY(cudaMemcpyAsync(h->topbuf.p, rho0, NN * 16, cudaMemcpyHostToDevice, h->stream));
+    heomk::heom_write_top<<<1, 128, 0, h->stream>>>(h->y.data.p, h->topbuf.p, h->d_pair.p, h->d_top.p, N, h->P);
+    h->launches++;
+    auto record = [&](int64_t row) -> int {
+        heomk::heom_record_top<<<1, 128, 0, h->stream>>>(A->toplog.p, h->y.data.p, h->d_pair.p, h->d_top.p, N, h->P,
+                                                         row);
+        h->launches++;
+        CUDA_TRY(cudaGetLastError());
+        return 0;
+    };
+    if (int rc = record(0)) return rc;
+    for (int64_t n = 0; n < steps; ++n) {
+        if (n % S == 0)
+            CUDA_TRY(cudaMemcpyAsync(A->cps.p + (n / S) * st, h->y.data.p, st * 16, cudaMemcpyDeviceToDevice,
+                                     h->stream));
+        if (int rc = run_steps(h, dt, 1)) return rc;
+        if (int rc = record(n + 1)) return rc;
+    }
+    std::vector<double> tops((steps + 1) * NN * 2);
+    CUDA_TRY(cudaMemcpyAsync(tops.data(), A->toplog.p, tops.size() * 8, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (int rc = check_kernel_error(h)) return rc;
+    long double J = 0.0L;
+    for (int64_t n = 0; n <= steps; ++n) {
+        long double v = 0.0L;
+        for (int q = 0; q < NN; ++q)
+            v += (long double)observable[2 * q] * tops[(n * NN + q) * 2] +
+                 (long double)observable[2 * q + 1] * tops[(n * NN + q) * 2 + 1];
+        J += (long double)weights[n] * v;
+    }
+    if (loss) *loss = (double)J;
+
+    // ---- backward ----
+    CUDA_TRY(cudaMemsetAsync(A->partial.p, 0, (size_t)A->grid * (NN + 2) * 16, h->stream));
+    double2* gcur = A->ga.p;
+    double2* gnxt = A->gb.p;
+    CUDA_TRY(cudaMemsetAsync(gcur, 0, st * 16, h->stream));
+    if (int rc = adj_add_top(A, gcur, weights[steps])) return rc;
+    for (int64_t sgm = ncp - 1; sgm >= 0; --sgm) {
+        const int64_t start = sgm * S, len = std::min(S, steps - start);
+        // stage inputs w_k of every step of the segment
+        CUDA_TRY(cudaMemcpyAsync(A->seg.p, A->cps.p + sgm * st, st * 16, cudaMemcpyDeviceToDevice, h->stream));
+        for (int64_t j = 0; j < len; ++j)
+            for (int k = 0; k < 4; ++k) {
+                const double2* in = A->seg.p + (4 * j + k) * st;
+                double2* o = k < 3 ? A->seg.p + (4 * j + k + 1) * st
+                                   : (j + 1 < len ? A->seg.p + 4 * (j + 1) * st : A->scratch.p);
+                const double2 beta = make_double2(dt * kProdBeta[k][0], dt * kProdBeta[k][1]);
+                if (int rc = launch_stage(h, EPI_AXPY_SELF, in, nullptr, o, nullptr, beta, 0)) return rc;
+            }
+        for (int64_t j = len - 1; j >= 0; --j) {
+            for (int k = 3; k >= 0; --k) {
+                const double2 beta = make_double2(dt * kProdBeta[k][0], dt * kProdBeta[k][1]);
+                if (int rc = adj_grad(A, gcur, A->seg.p + (4 * j + k) * st, beta)) return rc;
+                const double2 cbeta = make_double2(beta.x, -beta.y);
+                if (int rc = launch_stage(h, EPI_AXPY_SELF, gcur, nullptr, gnxt, nullptr, cbeta, 0, &A->tabs))
+                    return rc;
+                std::swap(gcur, gnxt);
+            }
+            if (int rc = adj_add_top(A, gcur, weights[start + j])) return rc;
+        }
+    }
+    std::vector<double> part((size_t)A->grid * (NN + 2) * 2);
+    CUDA_TRY(cudaMemcpyAsync(part.data(), A->partial.p, part.size() * 8, cudaMemcpyDeviceToHost, h->stream));
+    std::vector<double> g0top(NN * 2);
+    heomk::heom_record_top<<<1, 128, 0, h->stream>>>(h->topbuf.p, gcur, h->d_pair.p, h->d_top.p, N, h->P, 0);
+    h->launches++;
+    CUDA_TRY(cudaMemcpyAsync(g0top.data(), h->topbuf.p, NN * 16, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (int rc = check_kernel_error(h)) return rc;
+    std::vector<long double> sum((NN + 2) * 2, 0.0L);
+    for (int b = 0; b < A->grid; ++b)
+        for (size_t q = 0; q < sum.size(); ++q) sum[q] += part[(size_t)b * (NN + 2) * 2 + q];
+    // config units: H and lambda per cm^-1, gamma = 1/invnu per fs^-1
+    const long double c = heomhost::invcm_to_joule;
+    if (grad_h)
+        for (int q = 0; q < NN; ++q) {
+            grad_h[2 * q] = (double)(-sum[2 * q + 1] / kHbar * c); // Re(i Z / hbar)
+            grad_h[2 * q + 1] = (double)(-sum[2 * q] / kHbar * c); // Re(i i Z / hbar)
+        }
+    if (grad_lambda) *grad_lambda = (double)(sum[2 * NN] * c);
+    if (grad_gamma) *grad_gamma = (double)(sum[2 * NN + 2] * 1e15L);
+    if (grad_rho0) std::copy(g0top.begin(), g0top.end(), grad_rho0);
+    return 0;
+}
+
+int64_t heom_adjoint_kernel_launches(const heom_adjoint* A) { return A && A->h ? A->h->launches : 0; }
 
 } // extern "C"

@@ -94,6 +94,13 @@ struct instance {
 
 // instance.cpp:25-71 + precompute_baths_input (:155-273)
 instance make_instance(const system_params& sys);
+
+// derivatives of the bath tables for the adjoint: index 0 = lambda of every
+// bath together (per J), 1 = gamma = 1/invnu of every bath together (per 1/s)
+struct bath_derivs {
+    std::vector<double> pf_same[2], pf_circ[2], cbk[2]; // layouts of instance::pf_same, pf_circ, cbk
+};
+bath_derivs bath_derivatives(const system_params& sys);
 system_params system_from_desc(const heom_system_desc& d); // config units -> SI (config.cpp:182-191)
 void validate_system(const system_params& s);              // config.cpp:117-174 subset
 

@@ -64,6 +64,21 @@ int heom_create_from_system(const heom_system_desc* sys, const heom_options* opt
     return rc;
 }
 
+int heom_bath_derivatives(const heom_system_desc* sys, int32_t theta, double* d_pf_same, double* d_pf_circ,
+                          double* d_cbk)
+{
+    if (!sys || theta < 0 || theta > 1) return set_error(HEOM_E_ARG, "bad argument");
+    return guarded([&] {
+        const system_params sp = system_from_desc(*sys);
+        validate_system(sp);
+        const bath_derivs d = bath_derivatives(sp);
+        if (d_pf_same) std::memcpy(d_pf_same, d.pf_same[theta].data(), d.pf_same[theta].size() * 8);
+        if (d_pf_circ) std::memcpy(d_pf_circ, d.pf_circ[theta].data(), d.pf_circ[theta].size() * 8);
+        if (d_cbk) std::memcpy(d_cbk, d.cbk[theta].data(), d.cbk[theta].size() * 8);
+        return 0;
+    });
+}
+
 int heom_tables_mask(const heom_tables* t, const char* strategy, int64_t first_layer, uint8_t* mask)
 {
     if (!t || !strategy || !mask) return set_error(HEOM_E_ARG, "NULL argument");

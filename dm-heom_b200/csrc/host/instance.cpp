@@ -178,4 +178,74 @@ instance make_instance(const system_params& sys)
     return in;
 }
 
+// Derivatives of pf_same, pf_circ and cbk (the formulas of make_instance
+// above, instance.cpp:155-221 of the reference) with respect to theta = 0:
+// lambda of every bath moved together (per J), theta = 1: gamma = 1/invnu of
+// every bath moved together (per 1/s).  With nu = gamma + i Omega and
+// a = 1 / (beta hbar):
+//   pf_circ = nu lambda / hbar
+//   cb_0    = 2 lambda a (1 - S),  S = sum_j 2 eta_j nu^2 / (X_j - nu^2),  X_j = xi_j^2 a^2
+//   cb_k    = 4 lambda nu a^2 eta_k xi_k / (X_k - nu^2)                     (k >= 1)
+//   pf_same = 2 lambda a / (hbar nu) - cb_0 / (hbar nu) - sum_k cb_k / (hbar xi_k a)
+// pf_same_sum = -sum n_{b,k} nu_{b,k} changes with gamma only (by -n_{b,0}).
+bath_derivs bath_derivatives(const system_params& sys)
+{
+    const int M = sys.matsubaras, B = sys.baths;
+    const int row = (M - 1) * max_pade;
+    const double hbar = h_bar;
+    const double beta = 1.0 / (k_b * sys.temperature);
+    const double a = 1.0 / (beta * hbar);
+    bath_derivs d;
+    for (int th = 0; th < 2; ++th) {
+        d.pf_same[th].assign(2 * B, 0.0);
+        d.pf_circ[th].assign(2 * B, 0.0);
+        d.cbk[th].assign(2 * B * M, 0.0);
+    }
+    auto put = [](std::vector<double>& v, int q, complex_t z) {
+        v[2 * q] = z.real();
+        v[2 * q + 1] = z.imag();
+    };
+    for (int b = 0; b < B; ++b) {
+        const double lam = sys.lambda[b];
+        const complex_t nu{1.0 / sys.invnu[b], sys.omega[b]};
+        put(d.pf_circ[0], b, nu / hbar);
+        put(d.pf_circ[1], b, complex_t(lam / hbar));
+        complex_t dsame[2] = {2.0 * a / (hbar * nu), -2.0 * lam * a / (hbar * nu * nu)};
+        for (int k = 0; k < M; ++k) {
+            complex_t dcb[2];
+            if (k == 0) {
+                complex_t S = 0.0, dS = 0.0;
+                for (int j = 0; j < M; ++j) {
+                    const double eta = (double)heom_eta_pade[row + j];
+                    const double xi = (double)heom_xi_pade[row + j];
+                    const double X = xi * xi * a * a;
+                    const complex_t den = X - nu * nu;
+                    S += 2.0 * eta * nu * nu / den;
+                    dS += 4.0 * eta * nu * X / (den * den);
+                }
+                const complex_t cb = 2.0 * lam * a * (1.0 - S);
+                dcb[0] = 2.0 * a * (1.0 - S);
+                dcb[1] = -2.0 * lam * a * dS;
+                dsame[0] -= dcb[0] / (hbar * nu);
+                dsame[1] -= dcb[1] / (hbar * nu) - cb / (hbar * nu * nu);
+            } else {
+                const double eta = (double)heom_eta_pade[row + k];
+                const double xi = (double)heom_xi_pade[row + k];
+                const double X = xi * xi * a * a;
+                const complex_t den = X - nu * nu;
+                dcb[0] = 4.0 * nu * a * a * eta * xi / den;
+                dcb[1] = 4.0 * lam * a * a * eta * xi * (X + nu * nu) / (den * den);
+                const double nuk = xi * a;
+                dsame[0] -= dcb[0] / (hbar * nuk);
+                dsame[1] -= dcb[1] / (hbar * nuk);
+            }
+            put(d.cbk[0], b * M + k, dcb[0]);
+            put(d.cbk[1], b * M + k, dcb[1]);
+        }
+        put(d.pf_same[0], b, dsame[0]);
+        put(d.pf_same[1], b, dsame[1]);
+    }
+    return d;
+}
+
 } // namespace heomhost

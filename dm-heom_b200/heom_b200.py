@@ -44,6 +44,8 @@ EXPORTS = [
     "heom_ensemble_get_top", "heom_ensemble_autotune", "heom_ensemble_rk4_steps",
     "heom_ensemble_propagate", "heom_ensemble_top_row_len", "heom_ensemble_top_offset",
     "heom_ensemble_kernel_launches", "heom_ensemble_stream",
+    "heom_adjoint_create", "heom_adjoint_destroy", "heom_adjoint_handle", "heom_adjoint_gradient",
+    "heom_adjoint_kernel_launches", "heom_bath_derivatives",
 ]
 
 
@@ -155,6 +157,14 @@ def lib():
         L.heom_ensemble_kernel_launches.argtypes = [vp]
         L.heom_ensemble_stream.restype = vp
         L.heom_ensemble_stream.argtypes = [vp]
+        L.heom_adjoint_create.argtypes = [C.POINTER(SystemDesc), C.POINTER(Options), C.POINTER(vp)]
+        L.heom_adjoint_destroy.argtypes = [vp]
+        L.heom_adjoint_handle.restype = vp
+        L.heom_adjoint_handle.argtypes = [vp]
+        L.heom_adjoint_gradient.argtypes = [vp, vp, vp, vp, dbl, i64, vp, vp, vp, vp, vp]
+        L.heom_adjoint_kernel_launches.restype = i64
+        L.heom_adjoint_kernel_launches.argtypes = [vp]
+        L.heom_bath_derivatives.argtypes = [C.POINTER(SystemDesc), i32, vp, vp, vp]
         _lib = L
     return _lib
 
@@ -541,6 +551,73 @@ def build_tables(system: System) -> dict:
         return out
     finally:
         lib().heom_tables_free(t)
+
+
+def bath_derivatives(system: System, theta: int):
+    """d(pf_same, pf_circ, cbk)/d theta, theta 0 = lambda of every bath (per J),
+    1 = gamma = 1/invnu of every bath (per 1/s); SI tables as build_tables."""
+    d = system.desc()
+    b, m = system.baths, system.matsubaras
+    ps, pc, cb = np.zeros(2 * b), np.zeros(2 * b), np.zeros(2 * b * m)
+    _check(lib().heom_bath_derivatives(C.byref(d), theta, _ptr(ps), _ptr(pc), _ptr(cb)))
+    return ps, pc, cb
+
+
+class Adjoint:
+    """Adjoint gradients of a time-integrated observable (heom_adjoint_*):
+    J = sum_n weights[n] Re(sum_ij conj(O_ij) rho_n(i,j))."""
+
+    def __init__(self, system: System, device=0, graphs=True):
+        self.system = system
+        d = system.desc()
+        o = make_options(device, "lex", "product", graphs)
+        self.h = C.c_void_p()
+        _check(lib().heom_adjoint_create(C.byref(d), C.byref(o), C.byref(self.h)))
+        self.states = system.sites
+
+    def gradient(self, rho0, observable, weights, dt, steps):
+        n = self.states
+        rho0 = np.ascontiguousarray(np.asarray(rho0, np.complex128).reshape(n, n)).view(np.float64).reshape(-1)
+        obs = np.ascontiguousarray(np.asarray(observable, np.complex128).reshape(n, n)).view(np.float64).reshape(-1)
+        w = np.ascontiguousarray(np.asarray(weights, np.float64))
+        assert w.size == steps + 1
+        loss = C.c_double()
+        gl, gg = C.c_double(), C.c_double()
+        gh = np.zeros(2 * n * n)
+        gr = np.zeros(2 * n * n)
+        _check(lib().heom_adjoint_gradient(self.h, _ptr(rho0), _ptr(obs), _ptr(w), dt, steps, C.byref(loss),
+                                           _ptr(gh), C.byref(gl), C.byref(gg), _ptr(gr)))
+        return {"loss": loss.value,
+                "h": gh.view(np.complex128).reshape(n, n),      # dJ/dRe H + i dJ/dIm H, per cm^-1
+                "lambda": gl.value, "gamma": gg.value,
+                "rho0": gr.view(np.complex128).reshape(n, n)}
+
+    def kernel_launches(self):
+        return lib().heom_adjoint_kernel_launches(self.h)
+
+    def close(self):
+        if self.h:
+            lib().heom_adjoint_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def trapezoid_weights(steps, dt_fs):
+    """Weights of the trapezoid rule over t_n = n dt (fs), n = 0..steps."""
+    w = np.full(steps + 1, float(dt_fs))
+    w[0] = w[-1] = 0.5 * dt_fs
+    return w
 
 
 def tables_mask(system: System, strategy="none", first_layer=-1):

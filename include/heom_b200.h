@@ -321,6 +321,41 @@ int heom_config_get(const heom_config* c, const char* key, char* buf, size_t len
  * mask[matrices]. */
 int heom_tables_mask(const heom_tables* t, const char* strategy, int64_t first_layer, uint8_t* mask);
 
+/* ------------------------------------------------------------------------
+ * Adjoint gradients.  No counterpart in the reference.
+ * ------------------------------------------------------------------------ */
+
+/* Loss of a propagation from rho0 (the top ADO; all others zero) by RK4
+ * steps of size dt (the product-form scheme):
+ *     J = sum_{n=0}^{steps} weights[n] * Re(sum_ij conj(O_ij) rho_n(i,j))
+ * with rho_n the top after n steps and O = observable (states^2 complex,
+ * interleaved).  heom_adjoint_gradient returns J and its gradients from one
+ * forward and one backward sweep (the transposed derivative L^H run backward
+ * through the stages, checkpoints every ceil(sqrt(steps)) steps, each
+ * segment recomputed from its checkpoint):
+ *   grad_h      [states*states*2]: dJ/dRe H_ij, dJ/dIm H_ij (per cm^-1), every
+ *               entry independent (a symmetric coupling perturbation is the
+ *               sum of the (i,j) and (j,i) entries)
+ *   grad_lambda dJ/dlambda with lambda of every bath moved together (per cm^-1)
+ *   grad_gamma  dJ/dgamma with gamma = 1/invnu of every bath moved together (per fs^-1)
+ *   grad_rho0   [states*states*2]: dJ/dRe rho0_ij, dJ/dIm rho0_ij
+ * Any output pointer may be NULL.  Masks are not supported. */
+typedef struct heom_adjoint heom_adjoint;
+int heom_adjoint_create(const heom_system_desc* sys, const heom_options* opt, heom_adjoint** out);
+int heom_adjoint_destroy(heom_adjoint* a);
+/* the forward handle (borrowed): tables, stream, launch count */
+heom_handle* heom_adjoint_handle(heom_adjoint* a);
+int heom_adjoint_gradient(heom_adjoint* a, const double* rho0, const double* observable, const double* weights,
+                          double dt, int64_t steps, double* loss, double* grad_h, double* grad_lambda,
+                          double* grad_gamma, double* grad_rho0);
+int64_t heom_adjoint_kernel_launches(const heom_adjoint* a);
+/* Derivatives of the bath tables (pf_same [baths*2], pf_circ [baths*2],
+ * cbk [baths*matsubaras*2], SI units) with respect to theta = 0: lambda of
+ * every bath together (per J), theta = 1: gamma = 1/invnu of every bath
+ * together (per 1/s).  Host only. */
+int heom_bath_derivatives(const heom_system_desc* sys, int32_t theta, double* d_pf_same, double* d_pf_circ,
+                          double* d_cbk);
+
 #ifdef __cplusplus
 }
 #endif

@@ -189,3 +189,29 @@ def test_batch_admission_rejects_mixed_classes():
     with pytest.raises(hb.HeomError) as e:
         hb.Heom.batch([t3, t3l])
     assert "heom error -1" in str(e.value) and "bath tables differ" in str(e.value)
+
+
+@pytest.mark.parametrize("m,omega", [(1, 0.0), (2, 0.0), (3, 30.0)])
+def test_bath_derivatives_match_central_differences(m, omega):
+    # host only: the analytic d(pf_same, pf_circ, cbk)/d(lambda, gamma) against
+    # central differences of the tables themselves
+    n = 3
+    h = ho.synthetic_hamiltonian(n, 4)
+    lam, inv = 35.0, 50.0
+
+    def tabs(lam_v, inv_v):
+        t = hb.build_tables(hb.System(h, [lam_v] * n, [inv_v] * n, [omega] * n, m, 300.0, 1))
+        return np.concatenate([t["pf_same"], t["pf_circ"], t["cbk"]])
+
+    sysd = hb.System(h, [lam] * n, [inv] * n, [omega] * n, m, 300.0, 1)
+    for theta in (0, 1):
+        ana = np.concatenate(hb.bath_derivatives(sysd, theta))
+        if theta == 0:  # per J; lambda in the config is cm^-1
+            d = 1e-4 * lam
+            fd = (tabs(lam + d, inv) - tabs(lam - d, inv)) / (2 * d * 1.986456217327470903861498336971e-23)
+        else:  # per 1/s; gamma = 1 / invnu
+            g = 1.0 / (inv * 1e-15)
+            d = 1e-5 * g
+            fd = (tabs(lam, 1e15 / (g + d)) - tabs(lam, 1e15 / (g - d))) / (2 * d)
+        scale = np.max(np.abs(ana))
+        assert np.max(np.abs(ana - fd)) <= 1e-7 * scale, (theta, np.max(np.abs(ana - fd)) / scale)
