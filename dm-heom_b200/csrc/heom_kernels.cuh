@@ -895,6 +895,21 @@ __global__ void heom_record_top(double2* __restrict__ log, const double2* __rest
     }
 }
 
+// heom_record_top into row *base + j (a device offset, for captured graphs)
+__global__ void heom_record_top_at(double2* __restrict__ log, const double2* __restrict__ y,
+                                   const int16_t* __restrict__ pe, const int64_t* __restrict__ tops, int n, int P,
+                                   const int64_t* __restrict__ base, int64_t j)
+{
+    const int k = blockIdx.x;
+    const int64_t u = tops[k];
+    double2* dst = log + ((*base + j) * gridDim.x + k) * n * n;
+    for (int pr = threadIdx.x; pr < P; pr += blockDim.x) {
+        const int e1 = pe[2 * pr], e2 = pe[2 * pr + 1];
+        dst[e1] = y[(u * P + pr) * 2];
+        if (e2 != e1) dst[e2] = y[(u * P + pr) * 2 + 1];
+    }
+}
+
 // Write row-major top matrices top[k] ([n_inst][n*n]) into the pair layout
 // of each instance's top ADO (block k).
 __global__ void heom_write_top(double2* __restrict__ y, const double2* __restrict__ top,
@@ -918,9 +933,10 @@ __global__ void heom_write_top(double2* __restrict__ y, const double2* __restric
 //   lambda, gamma (shared by all baths): L is linear in its coefficient
 //           tables, so dL/dtheta is L with H = 0 and the tables replaced by
 //           their derivatives (dpss, dgamma0, dchat, dkhat).
-// One warp per ADO; lanes own sectors (pair layout).  Every block adds
-// weight * (its sum) to its own row of `partial` (deterministic; summed on
-// the host at the end).
+// One warp per ADO; lanes own sectors (pair layout).  The blocks are split
+// among the instances of the handle (each block sweeps one instance's ADOs),
+// and every block adds weight * (its sum) to its own row of `partial`
+// (deterministic; summed per instance on the host at the end).
 // ---------------------------------------------------------------------------
 struct GradParams {
     const double2* __restrict__ a;     // adjoint (pair layout, internal order)
@@ -936,7 +952,8 @@ struct GradParams {
     const double* __restrict__ sq;     // [LS+1] sqrt(n)
     double2 weight;                    // beta_k h
     double2* partial;                  // [gridDim.x][N*N + 2]
-    int64_t nodes;
+    const int64_t* inst_base;          // [instances + 1] first ADO of every instance
+    int blocks_per_inst;               // blocks [k*bpi, (k+1)*bpi) sweep instance k only
     int N, P, W, NW, TWB, SL;
 };
 
@@ -959,8 +976,9 @@ __global__ void __launch_bounds__(kCtaWarps * 32) heom_adjoint_grad(const GradPa
     for (int r = 0; r < 8; ++r) zac[r] = make_double2(0.0, 0.0);
     double2 dl = make_double2(0.0, 0.0), dgm = dl;
 
-    const int64_t stride = (int64_t)gridDim.x * kCtaWarps;
-    for (int64_t u = (int64_t)blockIdx.x * kCtaWarps + warp; u < g.nodes; u += stride) {
+    const int inst = blockIdx.x / g.blocks_per_inst, jb = blockIdx.x - inst * g.blocks_per_inst;
+    const int64_t stride = (int64_t)g.blocks_per_inst * kCtaWarps, end = g.inst_base[inst + 1];
+    for (int64_t u = g.inst_base[inst] + (int64_t)jb * kCtaWarps + warp; u < end; u += stride) {
         const int32_t* nb = g.nbr + u * g.NW;
         const uint8_t* tu = g.tup + u * g.TWB;
         const double dps = g.dpss[u];
@@ -1084,10 +1102,17 @@ __global__ void __launch_bounds__(kCtaWarps * 32) heom_adjoint_grad(const GradPa
     }
 }
 
-// y[top] += weight * O (O row-major n x n complex), pair layout; one block
-__global__ void heom_add_top(double2* __restrict__ y, const double2* __restrict__ obs,
-                             const int16_t* __restrict__ pe, int64_t top, int P, double weight)
+// y[top of instance k] += w * O_k (O_k row-major n x n complex, obs =
+// [instances][n*n]), pair layout; block k.  w = weights[*base + j] (a device
+// offset, so one captured graph serves every segment).
+__global__ void heom_add_top(double2* __restrict__ y, const double2* __restrict__ obs_all,
+                             const int16_t* __restrict__ pe, const int64_t* __restrict__ tops, int n, int P,
+                             const double* __restrict__ weights, const int64_t* __restrict__ base, int64_t j)
 {
+    const double weight = weights[*base + j];
+    if (weight == 0.0) return;
+    const int64_t top = tops[blockIdx.x];
+    const double2* obs = obs_all + (int64_t)blockIdx.x * n * n;
     for (int pr = threadIdx.x; pr < P; pr += blockDim.x) {
         const int e1 = pe[2 * pr], e2 = pe[2 * pr + 1];
         double2& h1 = y[(top * P + pr) * 2];

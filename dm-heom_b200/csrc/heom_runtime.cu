@@ -141,7 +141,7 @@ dmma_fn_t pick_dslt(int slt)
 template <int N, int HK>
 dmma_fn_t pick_dmode(int slt, bool multi, bool adj)
 {
-    if (adj) return pick_dslt<N, HK, false, true>(slt);
+    if (adj) return multi ? pick_dslt<N, HK, true, true>(slt) : pick_dslt<N, HK, false, true>(slt);
     return multi ? pick_dslt<N, HK, true, false>(slt) : pick_dslt<N, HK, false, false>(slt);
 }
 
@@ -533,7 +533,6 @@ int resolve_stage(heom_handle* h, const void** fn_out, int* blocks_out = nullptr
     const void* fn = nullptr;
     size_t smem = 0;
     int threads = 0;
-    if (adj && h->n_inst > 1) return fail(HEOM_E_UNSUPPORTED, "the adjoint runs on single-instance handles");
     if (h->N <= 8) {
         fn = (const void*)pick_dmma(h->N, h->hkind, h->SLT, h->n_inst > 1, adj);
         smem = heomk::dmma_smem_bytes(h->P, h->W, h->NW, h->TWB, h->LS);
@@ -1931,43 +1930,66 @@ struct heom_adjoint {
     AdjTabs tabs{};
     DevBuf<double2> pss_adj, g0_adj, hs_adj;
     DevBuf<double> hfrag_adj, hr_adj;
-    DevBuf<double> dpss;     // [nodes] d pf_same_sum / d gamma (internal order)
-    DevBuf<double2> dg0;     // [2][N*N]
-    DevBuf<double> dchat;    // [2][W]
-    DevBuf<double2> dkhat;   // [2][3][W]
-    DevBuf<double2> obs;     // [N*N]
-    DevBuf<double2> partial; // [grid][N*N + 2]
-    int grid = 0;
+    DevBuf<double> dpss;       // [nodes] d pf_same_sum / d gamma (internal order)
+    DevBuf<double2> dg0;       // [2][N*N]
+    DevBuf<double> dchat;      // [2][W]
+    DevBuf<double2> dkhat;     // [2][3][W]
+    DevBuf<double2> obs;       // [K][N*N]
+    DevBuf<double2> partial;   // [grid][N*N + 2]
+    DevBuf<int64_t> inst_base; // [K + 1]
+    int grid = 0, bpi = 0;     // blocks of the gradient kernel, per instance
     size_t grad_smem = 0;
     DevBuf<double2> cps, seg, scratch, ga, gb, toplog;
     int64_t cap_cps = 0, cap_seg = 0, cap_rows = 0;
+    DevBuf<double> d_w;        // loss weights [steps + 1]
+    DevBuf<int64_t> d_base;    // step offset of the segment being run (read by the captured kernels)
+    int64_t cap_w = 0;
+    // captured graphs per segment length: [0] forward with tops, [1] stage-input recompute, [2] backward
+    struct Graphs {
+        int64_t len = 0;
+        cudaGraphExec_t g[3] = {nullptr, nullptr, nullptr};
+    };
+    std::vector<Graphs> graphs;
+    double graph_dt = 0.0;
+    void drop_graphs()
+    {
+        for (auto& e : graphs)
+            for (auto& x : e.g)
+                if (x) cudaGraphExecDestroy(x);
+        graphs.clear();
+    }
     ~heom_adjoint()
     {
+        drop_graphs();
         if (h) heom_destroy(h);
     }
 };
 
 namespace {
 
+// L^H tables of every instance and the derivative tables (shared bath tables)
 int adj_tables(heom_adjoint* A, const heomhost::system_params& sp)
 {
     heom_handle* h = A->h;
-    const int N = h->N, W = h->W, M = h->M, B = h->B;
+    const int N = h->N, W = h->W, M = h->M, K = h->n_inst;
     // L^H: conj(pf_same_sum), conj(gamma0), -H^H
     std::vector<double2> pss(h->nodes);
     for (int64_t r = 0; r < h->nodes; ++r)
         pss[h->int_of_ref[r]] = make_double2(h->pss[2 * r], -h->pss[2 * r + 1]);
     std::vector<double2> g0 = gamma0_table(h, h->pf_same);
     for (auto& v : g0) v.y = -v.y;
-    std::vector<double> hadj(2 * N * N);
-    for (int i = 0; i < N; ++i)
-        for (int j = 0; j < N; ++j) {
-            hadj[2 * (i * N + j)] = -h->ham[2 * (j * N + i)];
-            hadj[2 * (i * N + j) + 1] = h->ham[2 * (j * N + i) + 1];
-        }
-    std::vector<double2> hs(N * N);
-    std::vector<double> hr(N * (N + 1), 0.0), frag(256, 0.0);
-    h_tables(hadj.data(), N, hs.data(), hr.data(), N <= 8 ? frag.data() : nullptr);
+    std::vector<double2> hs((size_t)K * N * N);
+    std::vector<double> hr((size_t)K * N * (N + 1), 0.0), frag((size_t)K * 256, 0.0), hadj(2 * N * N);
+    for (int k = 0; k < K; ++k) {
+        const double* hk = h->ham.data() + (size_t)k * 2 * N * N;
+        for (int i = 0; i < N; ++i)
+            for (int j = 0; j < N; ++j) {
+                hadj[2 * (i * N + j)] = -hk[2 * (j * N + i)];
+                hadj[2 * (i * N + j) + 1] = hk[2 * (j * N + i) + 1];
+            }
+        h_tables(hadj.data(), N, hs.data() + (size_t)k * N * N, hr.data() + (size_t)k * N * (N + 1),
+                 N <= 8 ? frag.data() + (size_t)k * 256 : nullptr);
+    }
     if (int rc = A->pss_adj.alloc(pss.size())) return rc;
     if (int rc = A->g0_adj.alloc(g0.size())) return rc;
     if (int rc = A->hs_adj.alloc(hs.size())) return rc;
@@ -2004,7 +2026,6 @@ int adj_tables(heom_adjoint* A, const heomhost::system_params& sp)
         const std::vector<double2> g = gamma0_table(h, bd.pf_same[th]);
         std::copy(g.begin(), g.end(), dg0.begin() + th * N * N);
     }
-    (void)B;
     for (int64_t r = 0; r < h->nodes; ++r) {
         double v = 0.0;
         for (int b = 0; b < h->B; ++b) v -= h->tuples[r * W + b * M];
@@ -2038,7 +2059,8 @@ int adj_grad(heom_adjoint* A, const double2* a, const double2* w, double2 weight
     g.sq = h->d_sq.p;
     g.weight = weight;
     g.partial = A->partial.p;
-    g.nodes = h->nodes;
+    g.inst_base = A->inst_base.p;
+    g.blocks_per_inst = A->bpi;
     g.N = h->N;
     g.P = h->P;
     g.W = h->W;
@@ -2051,13 +2073,109 @@ int adj_grad(heom_adjoint* A, const double2* a, const double2* w, double2 weight
     return 0;
 }
 
-int adj_add_top(heom_adjoint* A, double2* y, double weight)
+// y += weights[*base + j] O at every instance's top
+int adj_add_top(heom_adjoint* A, double2* y, int64_t j)
 {
     heom_handle* h = A->h;
-    if (weight == 0.0) return 0;
-    heomk::heom_add_top<<<1, 128, 0, h->stream>>>(y, A->obs.p, h->d_pair.p, h->top_int[0], h->P, weight);
+    heomk::heom_add_top<<<h->n_inst, 128, 0, h->stream>>>(y, A->obs.p, h->d_pair.p, h->d_top.p, h->N, h->P,
+                                                          A->d_w.p, A->d_base.p, j);
     h->launches++;
     CUDA_TRY(cudaGetLastError());
+    return 0;
+}
+
+// One segment of `len` steps from y (the forward sweep): every step one RK4
+// step and the tops recorded into rows *base + j + 1.
+int adj_seg_forward(heom_adjoint* A, double dt, int64_t len)
+{
+    heom_handle* h = A->h;
+    for (int64_t j = 0; j < len; ++j) {
+        if (int rc = enqueue_step(h, dt)) return rc;
+        heomk::heom_record_top_at<<<h->n_inst, 128, 0, h->stream>>>(A->toplog.p, h->y.data.p, h->d_pair.p,
+                                                                    h->d_top.p, h->N, h->P, A->d_base.p, j + 1);
+        h->launches++;
+        CUDA_TRY(cudaGetLastError());
+    }
+    return 0;
+}
+
+// stage inputs w_k of every step of a segment, from seg[0] (its checkpoint)
+int adj_seg_recompute(heom_adjoint* A, double dt, int64_t len)
+{
+    heom_handle* h = A->h;
+    const size_t st = h->state_elems();
+    for (int64_t j = 0; j < len; ++j)
+        for (int k = 0; k < 4; ++k) {
+            const double2* in = A->seg.p + (4 * j + k) * st;
+            double2* o = k < 3 ? A->seg.p + (4 * j + k + 1) * st
+                               : (j + 1 < len ? A->seg.p + 4 * (j + 1) * st : A->scratch.p);
+            const double2 beta = make_double2(dt * kProdBeta[k][0], dt * kProdBeta[k][1]);
+            if (int rc = launch_stage(h, EPI_AXPY_SELF, in, nullptr, o, nullptr, beta, 0)) return rc;
+        }
+    return 0;
+}
+
+// backward through a segment: four factors per step (gradient contributions,
+// then F_k^H), then the step's loss weight; the adjoint ends in ga (4 swaps a step)
+int adj_seg_backward(heom_adjoint* A, double dt, int64_t len)
+{
+    heom_handle* h = A->h;
+    const size_t st = h->state_elems();
+    double2* gcur = A->ga.p;
+    double2* gnxt = A->gb.p;
+    for (int64_t j = len - 1; j >= 0; --j) {
+        for (int k = 3; k >= 0; --k) {
+            const double2 beta = make_double2(dt * kProdBeta[k][0], dt * kProdBeta[k][1]);
+            if (int rc = adj_grad(A, gcur, A->seg.p + (4 * j + k) * st, beta)) return rc;
+            const double2 cbeta = make_double2(beta.x, -beta.y);
+            if (int rc = launch_stage(h, EPI_AXPY_SELF, gcur, nullptr, gnxt, nullptr, cbeta, 0, &A->tabs)) return rc;
+            std::swap(gcur, gnxt);
+        }
+        if (int rc = adj_add_top(A, gcur, j)) return rc;
+    }
+    return 0;
+}
+
+// run part `which` (0 forward, 1 recompute, 2 backward) of a segment, through
+// a graph captured once per segment length when the handle uses graphs
+int adj_run(heom_adjoint* A, int which, double dt, int64_t len)
+{
+    heom_handle* h = A->h;
+    auto direct = [&]() -> int {
+        return which == 0 ? adj_seg_forward(A, dt, len) : which == 1 ? adj_seg_recompute(A, dt, len)
+                                                                       : adj_seg_backward(A, dt, len);
+    };
+    if (!h->opt.use_graphs) return direct();
+    if (A->graph_dt != dt) {
+        A->drop_graphs();
+        A->graph_dt = dt;
+    }
+    heom_adjoint::Graphs* e = nullptr;
+    for (auto& x : A->graphs)
+        if (x.len == len) e = &x;
+    if (!e) {
+        A->graphs.push_back(heom_adjoint::Graphs());
+        e = &A->graphs.back();
+        e->len = len;
+    }
+    if (!e->g[which]) {
+        const int64_t saved = h->launches;
+        cudaGraph_t graph = nullptr;
+        CUDA_TRY(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = direct();
+        cudaError_t ce = cudaStreamEndCapture(h->stream, &graph);
+        h->launches = saved;
+        if (rc) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        if (ce != cudaSuccess) return fail(HEOM_E_CUDA, "adjoint graph capture failed: %s", cudaGetErrorString(ce));
+        ce = cudaGraphInstantiate(&e->g[which], graph, 0);
+        cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) return fail(HEOM_E_CUDA, "adjoint graph instantiate failed: %s", cudaGetErrorString(ce));
+    }
+    CUDA_TRY(cudaGraphLaunch(e->g[which], h->stream));
+    h->launches += which == 0 ? len * (launches_per_step(h) + 1) : which == 1 ? 4 * len : 9 * len;
     return 0;
 }
 
@@ -2067,14 +2185,22 @@ extern "C" {
 
 int heom_adjoint_create(const heom_system_desc* sys, const heom_options* opt, heom_adjoint** out)
 {
-    if (!sys || !out) return fail(HEOM_E_ARG, "NULL argument");
+    return heom_adjoint_create_batch(sys, 1, opt, out);
+}
+
+int heom_adjoint_create_batch(const heom_system_desc* systems, int32_t count, const heom_options* opt,
+                              heom_adjoint** out)
+{
+    if (!systems || !out || count < 1) return fail(HEOM_E_ARG, "NULL argument or count < 1");
     *out = nullptr;
     std::unique_ptr<heom_adjoint> A(new heom_adjoint());
-    heomhost::system_params sp;
-    heomhost::instance inst;
+    std::vector<heomhost::system_params> sp(count);
+    std::vector<heomhost::instance> inst(count);
     try {
-        sp = heomhost::system_from_desc(*sys);
-        inst = heomhost::make_instance(sp);
+        for (int k = 0; k < count; ++k) {
+            sp[k] = heomhost::system_from_desc(systems[k]);
+            inst[k] = heomhost::make_instance(sp[k]);
+        }
     } catch (const heomhost::config_error& e) {
         return fail(HEOM_E_CONFIG, "%s", e.what());
     } catch (const std::exception& e) {
@@ -2084,15 +2210,22 @@ int heom_adjoint_create(const heom_system_desc* sys, const heom_options* opt, he
     heom_default_options(&o);
     if (opt) o = *opt;
     o.rk4_scheme = HEOM_RK4_PRODUCT; // the backward sweep differentiates the product form
-    const heom_instance_desc d = inst.desc();
-    if (int rc = heom_create(&d, &o, &A->h)) return rc;
+    std::vector<heom_instance_desc> d(count);
+    for (int k = 0; k < count; ++k) d[k] = inst[k].desc();
+    if (int rc = heom_create_batch(d.data(), count, &o, &A->h)) return rc;
     heom_handle* h = A->h;
     CUDA_TRY(cudaSetDevice(h->device));
-    if (int rc = adj_tables(A.get(), sp)) return rc;
-    if (int rc = A->obs.alloc((size_t)h->N * h->N)) return rc;
-    A->grid = (int)std::max<int64_t>(1, std::min<int64_t>((h->nodes + heomk::kCtaWarps - 1) / heomk::kCtaWarps,
-                                                        (int64_t)h->sm_count * 2));
+    if (int rc = adj_tables(A.get(), sp[0])) return rc;
+    if (int rc = A->obs.alloc((size_t)count * h->N * h->N)) return rc;
+    // gradient kernel: every instance gets the same number of blocks, about two waves in all
+    int64_t max_nodes = 1;
+    for (int k = 0; k < count; ++k) max_nodes = std::max(max_nodes, h->inst_base[k + 1] - h->inst_base[k]);
+    A->bpi = (int)std::max<int64_t>(1, std::min<int64_t>((max_nodes + heomk::kCtaWarps - 1) / heomk::kCtaWarps,
+                                                        (2 * (int64_t)h->sm_count + count - 1) / count));
+    A->grid = A->bpi * count;
     if (int rc = A->partial.alloc((size_t)A->grid * (h->N * h->N + 2))) return rc;
+    if (int rc = A->inst_base.alloc(count + 1)) return rc;
+    CUDA_TRY(cudaMemcpy(A->inst_base.p, h->inst_base.data(), (count + 1) * 8, cudaMemcpyHostToDevice));
     A->grad_smem = heomk::grad_smem_bytes(h->N);
     if (int rc = allow_dynamic_smem((const void*)heomk::heom_adjoint_grad, A->grad_smem)) return rc;
     *out = A.release();
@@ -2108,6 +2241,7 @@ int heom_adjoint_destroy(heom_adjoint* A)
 }
 
 heom_handle* heom_adjoint_handle(heom_adjoint* A) { return A ? A->h : nullptr; }
+int32_t heom_adjoint_instances(const heom_adjoint* A) { return A && A->h ? A->h->n_inst : 0; }
 
 int heom_adjoint_gradient(heom_adjoint* A, const double* rho0, const double* observable, const double* weights,
                           double dt, int64_t steps, double* loss, double* grad_h, double* grad_lambda,
@@ -2117,7 +2251,7 @@ int heom_adjoint_gradient(heom_adjoint* A, const double* rho0, const double* obs
         return fail(HEOM_E_ARG, "bad argument");
     heom_handle* h = A->h;
     CUDA_TRY(cudaSetDevice(h->device));
-    const int N = h->N, NN = N * N;
+    const int N = h->N, NN = N * N, K = h->n_inst;
     const size_t st = h->state_elems();
     const int64_t S = std::max<int64_t>(1, (int64_t)std::ceil(std::sqrt((double)steps)));
     const int64_t ncp = (steps + S - 1) / S;
@@ -2130,6 +2264,8 @@ int heom_adjoint_gradient(heom_adjoint* A, const double* rho0, const double* obs
             return fail(HEOM_E_NOMEM, "adjoint needs %.3f GB of device memory (%lld checkpoints, segments of %lld steps)",
                         need_states * st * 16 / 1e9, (long long)ncp, (long long)S);
     }
+    // the captured graphs hold buffer addresses: any reallocation drops them
+    if (ncp > A->cap_cps || 4 * S > A->cap_seg || steps + 1 > A->cap_rows || steps + 1 > A->cap_w) A->drop_graphs();
     if (ncp > A->cap_cps) {
         if (int rc = A->cps.alloc(ncp * st)) return rc;
         A->cap_cps = ncp;
@@ -2144,96 +2280,96 @@ int heom_adjoint_gradient(heom_adjoint* A, const double* rho0, const double* obs
         if (int rc = A->scratch.alloc(st)) return rc;
     }
     if (steps + 1 > A->cap_rows) {
-        if (int rc = A->toplog.alloc((steps + 1) * NN)) return rc;
+        if (int rc = A->toplog.alloc((steps + 1) * NN * K)) return rc;
         A->cap_rows = steps + 1;
     }
+    if (steps + 1 > A->cap_w) {
+        if (int rc = A->d_w.alloc(steps + 1)) return rc;
+        A->cap_w = steps + 1;
+    }
+    if (!A->d_base.p)
+        if (int rc = A->d_base.alloc(1)) return rc;
     if (int rc = prepare_scheme(h)) return rc;
-    CUDA_TRY(cudaMemcpy(A->obs.p, observable, NN * 16, cudaMemcpyHostToDevice));
+    {
+        // resolve both stage kernels' launch shapes outside of any capture
+        const void* fn = nullptr;
+        if (int rc = resolve_stage(h, &fn)) return rc;
+        if (int rc = resolve_stage(h, &fn, nullptr, true)) return rc;
+    }
+    CUDA_TRY(cudaMemcpy(A->obs.p, observable, (size_t)K * NN * 16, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(A->d_w.p, weights, (steps + 1) * 8, cudaMemcpyHostToDevice));
+    std::vector<int64_t> starts(ncp + 1);
+    for (int64_t s2 = 0; s2 <= ncp; ++s2) starts[s2] = s2 * S;
+    auto set_base = [&](int64_t s2) -> int {
+        CUDA_TRY(cudaMemcpyAsync(A->d_base.p, &starts[s2], 8, cudaMemcpyHostToDevice, h->stream));
+        return 0;
+    };
 
     // ---- forward: checkpoints and the observed tops ----
     CUDA_TRY(cudaMemsetAsync(h->y.data.p, 0, st * 16, h->stream));
-    CUDA_TRY(cudaMemcpyAsync(h->topbuf.p, rho0, NN * 16, cudaMemcpyHostToDevice, h->stream));
-    heomk::heom_write_top<<<1, 128, 0, h->stream>>>(h->y.data.p, h->topbuf.p, h->d_pair.p, h->d_top.p, N, h->P);
+    CUDA_TRY(cudaMemcpyAsync(h->topbuf.p, rho0, (size_t)K * NN * 16, cudaMemcpyHostToDevice, h->stream));
+    heomk::heom_write_top<<<K, 128, 0, h->stream>>>(h->y.data.p, h->topbuf.p, h->d_pair.p, h->d_top.p, N, h->P);
     h->launches++;
-    auto record = [&](int64_t row) -> int {
-        heomk::heom_record_top<<<1, 128, 0, h->stream>>>(A->toplog.p, h->y.data.p, h->d_pair.p, h->d_top.p, N, h->P,
-                                                         row);
-        h->launches++;
-        CUDA_TRY(cudaGetLastError());
-        return 0;
-    };
-    if (int rc = record(0)) return rc;
-    for (int64_t n = 0; n < steps; ++n) {
-        if (n % S == 0)
-            CUDA_TRY(cudaMemcpyAsync(A->cps.p + (n / S) * st, h->y.data.p, st * 16, cudaMemcpyDeviceToDevice,
-                                     h->stream));
-        if (int rc = run_steps(h, dt, 1)) return rc;
-        if (int rc = record(n + 1)) return rc;
+    heomk::heom_record_top<<<K, 128, 0, h->stream>>>(A->toplog.p, h->y.data.p, h->d_pair.p, h->d_top.p, N, h->P, 0);
+    h->launches++;
+    CUDA_TRY(cudaGetLastError());
+    for (int64_t sgm = 0; sgm < ncp; ++sgm) {
+        const int64_t len = std::min(S, steps - sgm * S);
+        CUDA_TRY(cudaMemcpyAsync(A->cps.p + sgm * st, h->y.data.p, st * 16, cudaMemcpyDeviceToDevice, h->stream));
+        if (int rc = set_base(sgm)) return rc;
+        if (int rc = adj_run(A, 0, dt, len)) return rc;
     }
-    std::vector<double> tops((steps + 1) * NN * 2);
+    std::vector<double> tops((steps + 1) * NN * K * 2);
     CUDA_TRY(cudaMemcpyAsync(tops.data(), A->toplog.p, tops.size() * 8, cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     if (int rc = check_kernel_error(h)) return rc;
-    long double J = 0.0L;
-    for (int64_t n = 0; n <= steps; ++n) {
-        long double v = 0.0L;
-        for (int q = 0; q < NN; ++q)
-            v += (long double)observable[2 * q] * tops[(n * NN + q) * 2] +
-                 (long double)observable[2 * q + 1] * tops[(n * NN + q) * 2 + 1];
-        J += (long double)weights[n] * v;
+    for (int k = 0; k < K; ++k) {
+        long double J = 0.0L;
+        const double* o = observable + (size_t)k * NN * 2;
+        for (int64_t n = 0; n <= steps; ++n) {
+            const double* tp = tops.data() + ((size_t)n * K + k) * NN * 2;
+            long double v = 0.0L;
+            for (int q = 0; q < NN; ++q) v += (long double)o[2 * q] * tp[2 * q] + (long double)o[2 * q + 1] * tp[2 * q + 1];
+            J += (long double)weights[n] * v;
+        }
+        if (loss) loss[k] = (double)J;
     }
-    if (loss) *loss = (double)J;
 
     // ---- backward ----
     CUDA_TRY(cudaMemsetAsync(A->partial.p, 0, (size_t)A->grid * (NN + 2) * 16, h->stream));
     double2* gcur = A->ga.p;
-    double2* gnxt = A->gb.p;
     CUDA_TRY(cudaMemsetAsync(gcur, 0, st * 16, h->stream));
-    if (int rc = adj_add_top(A, gcur, weights[steps])) return rc;
+    if (int rc = set_base(ncp)) return rc; // starts[ncp] = ncp * S >= steps
+    if (int rc = adj_add_top(A, gcur, steps - ncp * S)) return rc;
     for (int64_t sgm = ncp - 1; sgm >= 0; --sgm) {
-        const int64_t start = sgm * S, len = std::min(S, steps - start);
-        // stage inputs w_k of every step of the segment
+        const int64_t len = std::min(S, steps - sgm * S);
         CUDA_TRY(cudaMemcpyAsync(A->seg.p, A->cps.p + sgm * st, st * 16, cudaMemcpyDeviceToDevice, h->stream));
-        for (int64_t j = 0; j < len; ++j)
-            for (int k = 0; k < 4; ++k) {
-                const double2* in = A->seg.p + (4 * j + k) * st;
-                double2* o = k < 3 ? A->seg.p + (4 * j + k + 1) * st
-                                   : (j + 1 < len ? A->seg.p + 4 * (j + 1) * st : A->scratch.p);
-                const double2 beta = make_double2(dt * kProdBeta[k][0], dt * kProdBeta[k][1]);
-                if (int rc = launch_stage(h, EPI_AXPY_SELF, in, nullptr, o, nullptr, beta, 0)) return rc;
-            }
-        for (int64_t j = len - 1; j >= 0; --j) {
-            for (int k = 3; k >= 0; --k) {
-                const double2 beta = make_double2(dt * kProdBeta[k][0], dt * kProdBeta[k][1]);
-                if (int rc = adj_grad(A, gcur, A->seg.p + (4 * j + k) * st, beta)) return rc;
-                const double2 cbeta = make_double2(beta.x, -beta.y);
-                if (int rc = launch_stage(h, EPI_AXPY_SELF, gcur, nullptr, gnxt, nullptr, cbeta, 0, &A->tabs))
-                    return rc;
-                std::swap(gcur, gnxt);
-            }
-            if (int rc = adj_add_top(A, gcur, weights[start + j])) return rc;
-        }
+        if (int rc = set_base(sgm)) return rc;
+        if (int rc = adj_run(A, 1, dt, len)) return rc;
+        if (int rc = adj_run(A, 2, dt, len)) return rc;
     }
     std::vector<double> part((size_t)A->grid * (NN + 2) * 2);
     CUDA_TRY(cudaMemcpyAsync(part.data(), A->partial.p, part.size() * 8, cudaMemcpyDeviceToHost, h->stream));
-    std::vector<double> g0top(NN * 2);
-    heomk::heom_record_top<<<1, 128, 0, h->stream>>>(h->topbuf.p, gcur, h->d_pair.p, h->d_top.p, N, h->P, 0);
+    std::vector<double> g0top((size_t)K * NN * 2);
+    heomk::heom_record_top<<<K, 128, 0, h->stream>>>(h->topbuf.p, gcur, h->d_pair.p, h->d_top.p, N, h->P, 0);
     h->launches++;
-    CUDA_TRY(cudaMemcpyAsync(g0top.data(), h->topbuf.p, NN * 16, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaMemcpyAsync(g0top.data(), h->topbuf.p, g0top.size() * 8, cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     if (int rc = check_kernel_error(h)) return rc;
-    std::vector<long double> sum((NN + 2) * 2, 0.0L);
-    for (int b = 0; b < A->grid; ++b)
-        for (size_t q = 0; q < sum.size(); ++q) sum[q] += part[(size_t)b * (NN + 2) * 2 + q];
     // config units: H and lambda per cm^-1, gamma = 1/invnu per fs^-1
     const long double c = heomhost::invcm_to_joule;
-    if (grad_h)
-        for (int q = 0; q < NN; ++q) {
-            grad_h[2 * q] = (double)(-sum[2 * q + 1] / kHbar * c); // Re(i Z / hbar)
-            grad_h[2 * q + 1] = (double)(-sum[2 * q] / kHbar * c); // Re(i i Z / hbar)
-        }
-    if (grad_lambda) *grad_lambda = (double)(sum[2 * NN] * c);
-    if (grad_gamma) *grad_gamma = (double)(sum[2 * NN + 2] * 1e15L);
+    for (int k = 0; k < K; ++k) {
+        std::vector<long double> sum((NN + 2) * 2, 0.0L);
+        for (int b = k * A->bpi; b < (k + 1) * A->bpi; ++b)
+            for (size_t q = 0; q < sum.size(); ++q) sum[q] += part[(size_t)b * (NN + 2) * 2 + q];
+        if (grad_h)
+            for (int q = 0; q < NN; ++q) {
+                grad_h[((size_t)k * NN + q) * 2] = (double)(-sum[2 * q + 1] / kHbar * c); // Re(i Z / hbar)
+                grad_h[((size_t)k * NN + q) * 2 + 1] = (double)(-sum[2 * q] / kHbar * c); // Re(i i Z / hbar)
+            }
+        if (grad_lambda) grad_lambda[k] = (double)(sum[2 * NN] * c);
+        if (grad_gamma) grad_gamma[k] = (double)(sum[2 * NN + 2] * 1e15L);
+    }
     if (grad_rho0) std::copy(g0top.begin(), g0top.end(), grad_rho0);
     return 0;
 }

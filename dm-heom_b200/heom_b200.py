@@ -45,7 +45,8 @@ EXPORTS = [
     "heom_ensemble_propagate", "heom_ensemble_top_row_len", "heom_ensemble_top_offset",
     "heom_ensemble_kernel_launches", "heom_ensemble_stream",
     "heom_adjoint_create", "heom_adjoint_destroy", "heom_adjoint_handle", "heom_adjoint_gradient",
-    "heom_adjoint_kernel_launches", "heom_bath_derivatives",
+    "heom_adjoint_kernel_launches", "heom_bath_derivatives", "heom_adjoint_create_batch",
+    "heom_adjoint_instances",
 ]
 
 
@@ -165,6 +166,9 @@ def lib():
         L.heom_adjoint_kernel_launches.restype = i64
         L.heom_adjoint_kernel_launches.argtypes = [vp]
         L.heom_bath_derivatives.argtypes = [C.POINTER(SystemDesc), i32, vp, vp, vp]
+        L.heom_adjoint_create_batch.argtypes = [C.POINTER(SystemDesc), i32, C.POINTER(Options), C.POINTER(vp)]
+        L.heom_adjoint_instances.restype = i32
+        L.heom_adjoint_instances.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -565,32 +569,44 @@ def bath_derivatives(system: System, theta: int):
 
 class Adjoint:
     """Adjoint gradients of a time-integrated observable (heom_adjoint_*):
-    J = sum_n weights[n] Re(sum_ij conj(O_ij) rho_n(i,j))."""
+    J = sum_n weights[n] Re(sum_ij conj(O_ij) rho_n(i,j)).  Given a list of
+    systems (shared states and baths) it sweeps the whole batch at once and
+    returns per-instance results with a leading instance axis."""
 
-    def __init__(self, system: System, device=0, graphs=True):
-        self.system = system
-        d = system.desc()
+    def __init__(self, system, device=0, graphs=True):
+        self.batch = isinstance(system, (list, tuple))
+        systems = list(system) if self.batch else [system]
+        self.systems = systems
+        ds = (SystemDesc * len(systems))(*[x.desc() for x in systems])
         o = make_options(device, "lex", "product", graphs)
         self.h = C.c_void_p()
-        _check(lib().heom_adjoint_create(C.byref(d), C.byref(o), C.byref(self.h)))
-        self.states = system.sites
+        _check(lib().heom_adjoint_create_batch(ds, len(systems), C.byref(o), C.byref(self.h)))
+        self.states = systems[0].sites
+        self.instances = len(systems)
 
     def gradient(self, rho0, observable, weights, dt, steps):
-        n = self.states
-        rho0 = np.ascontiguousarray(np.asarray(rho0, np.complex128).reshape(n, n)).view(np.float64).reshape(-1)
-        obs = np.ascontiguousarray(np.asarray(observable, np.complex128).reshape(n, n)).view(np.float64).reshape(-1)
+        n, K = self.states, self.instances
+
+        def per_instance(a):
+            a = np.asarray(a, np.complex128)
+            if a.size == n * n:
+                a = np.broadcast_to(a.reshape(1, n, n), (K, n, n))
+            return np.ascontiguousarray(a.reshape(K, n, n)).view(np.float64).reshape(-1)
+
+        rho0 = per_instance(rho0)
+        obs = per_instance(observable)
         w = np.ascontiguousarray(np.asarray(weights, np.float64))
         assert w.size == steps + 1
-        loss = C.c_double()
-        gl, gg = C.c_double(), C.c_double()
-        gh = np.zeros(2 * n * n)
-        gr = np.zeros(2 * n * n)
-        _check(lib().heom_adjoint_gradient(self.h, _ptr(rho0), _ptr(obs), _ptr(w), dt, steps, C.byref(loss),
-                                           _ptr(gh), C.byref(gl), C.byref(gg), _ptr(gr)))
-        return {"loss": loss.value,
-                "h": gh.view(np.complex128).reshape(n, n),      # dJ/dRe H + i dJ/dIm H, per cm^-1
-                "lambda": gl.value, "gamma": gg.value,
-                "rho0": gr.view(np.complex128).reshape(n, n)}
+        loss, gl, gg = np.zeros(K), np.zeros(K), np.zeros(K)
+        gh = np.zeros(2 * K * n * n)
+        gr = np.zeros(2 * K * n * n)
+        _check(lib().heom_adjoint_gradient(self.h, _ptr(rho0), _ptr(obs), _ptr(w), dt, steps, _ptr(loss),
+                                           _ptr(gh), _ptr(gl), _ptr(gg), _ptr(gr)))
+        out = {"loss": loss, "h": gh.view(np.complex128).reshape(K, n, n),  # dJ/dRe H + i dJ/dIm H, per cm^-1
+               "lambda": gl, "gamma": gg, "rho0": gr.view(np.complex128).reshape(K, n, n)}
+        if not self.batch:
+            out = {k: (v[0] if k != "loss" and k not in ("lambda", "gamma") else float(v[0])) for k, v in out.items()}
+        return out
 
     def kernel_launches(self):
         return lib().heom_adjoint_kernel_launches(self.h)

@@ -342,6 +342,15 @@ int heom_tables_mask(const heom_tables* t, const char* strategy, int64_t first_l
  * Any output pointer may be NULL.  Masks are not supported. */
 typedef struct heom_adjoint heom_adjoint;
 int heom_adjoint_create(const heom_system_desc* sys, const heom_options* opt, heom_adjoint** out);
+/* A batch of K systems that share states, baths and bath parameters (they
+ * may differ in H and depth) in one sweep: every array argument and output
+ * of heom_adjoint_gradient then holds the K instances back to back (rho0,
+ * observable, grad_h, grad_rho0: K x states^2 complex; loss, grad_lambda,
+ * grad_gamma: K values, instance k's share of the shared-parameter
+ * gradient); weights, dt and steps are common. */
+int heom_adjoint_create_batch(const heom_system_desc* systems, int32_t count, const heom_options* opt,
+                              heom_adjoint** out);
+int32_t heom_adjoint_instances(const heom_adjoint* a);
 int heom_adjoint_destroy(heom_adjoint* a);
 /* the forward handle (borrowed): tables, stream, launch count */
 heom_handle* heom_adjoint_handle(heom_adjoint* a);

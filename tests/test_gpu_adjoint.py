@@ -229,3 +229,51 @@ def test_adjoint_through_torch_autograd():
     assert np.allclose(cpl.grad.numpy(), gr[iu] + gr.T[iu], rtol=1e-13, atol=0)
     assert abs(float(lam.grad) - out["lambda"]) <= 1e-13 * abs(out["lambda"])
     assert abs(float(gam.grad) - out["gamma"]) <= 1e-13 * abs(out["gamma"])
+
+
+def test_batched_adjoint_matches_single_instance_sweeps():
+    # static-disorder realisations (different H, two depths) in one sweep
+    n, m, steps, dt_fs = 5, 2, 40, 1.0
+    base = ho.synthetic_hamiltonian(n, 31)
+    rng = np.random.default_rng(5)
+    systems = []
+    for k in range(3):
+        h = base.copy()
+        h[np.diag_indices(n)] += rng.normal(0.0, 100.0, size=n)
+        systems.append(hb.System(h, [35.0] * n, [50.0] * n, [0.0] * n, m, 300.0, 2 + k % 2))
+    rho0 = np.zeros((n, n), complex)
+    rho0[0, 0] = 1.0
+    obs = np.zeros((3, n, n), complex)
+    for k in range(3):
+        obs[k, k, k] = 1.0  # a different site population per instance
+    w = hb.trapezoid_weights(steps, dt_fs)
+    with hb.Adjoint(systems) as A:
+        out = A.gradient(rho0, obs, w, dt_fs * 1e-15, steps)
+    for k in range(3):
+        with hb.Adjoint(systems[k]) as A1:
+            ref = A1.gradient(rho0, obs[k], w, dt_fs * 1e-15, steps)
+        assert abs(out["loss"][k] - ref["loss"]) <= 1e-14 * abs(ref["loss"])
+        assert np.max(np.abs(out["h"][k] - ref["h"])) <= 1e-12 * np.max(np.abs(ref["h"]))
+        assert abs(out["lambda"][k] - ref["lambda"]) <= 1e-12 * abs(ref["lambda"])
+        assert abs(out["gamma"][k] - ref["gamma"]) <= 1e-12 * abs(ref["gamma"])
+        assert np.max(np.abs(out["rho0"][k] - ref["rho0"])) <= 1e-13 * np.max(np.abs(ref["rho0"]))
+
+
+def test_adjoint_graphs_equal_eager_launches_and_survive_regrowth():
+    # the captured per-segment graphs and eager launches run the same kernels in
+    # the same order; a longer second call reallocates and recaptures
+    n, steps = 4, 50
+    system = hb.System(ho.synthetic_hamiltonian(n, 8), [35.0] * n, [50.0] * n, [0.0] * n, 2, 300.0, 3)
+    rho0 = np.zeros((n, n), complex)
+    rho0[0, 0] = 1.0
+    obs = np.zeros((n, n), complex)
+    obs[1, 1] = 1.0
+    outs = []
+    for graphs in (True, False):
+        with hb.Adjoint(system, graphs=graphs) as A:
+            A.gradient(rho0, obs, hb.trapezoid_weights(10, 1.0), 1e-15, 10)
+            outs.append(A.gradient(rho0, obs, hb.trapezoid_weights(steps, 1.0), 1e-15, steps))
+    a, b = outs
+    assert a["loss"] == b["loss"]
+    assert np.array_equal(a["h"], b["h"]) and np.array_equal(a["rho0"], b["rho0"])
+    assert a["lambda"] == b["lambda"] and a["gamma"] == b["gamma"]
