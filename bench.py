@@ -261,6 +261,18 @@ def shard(sizes, world, rank):
     return sorted(mine)
 
 
+def reduce_throughput(dist, ados_steps, secs, device):
+    """Whole-job ADO-updates and the slowest rank's time: one sum and one max
+    all-reduce (the only collectives of a sharded ensemble)."""
+    import torch
+    a = torch.tensor([float(ados_steps)], dtype=torch.float64, device=device)
+    t = torch.tensor([float(secs)], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(a)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(a.item()), float(t.item())
+
+
 def run_batched(args, world, rank, local_rank):
     import torch
     import heom_b200 as hb
@@ -317,14 +329,8 @@ def run_batched(args, world, rank, local_rank):
     launches = E.kernel_launches() - launches0
     ms = start.elapsed_time(stop)
     secs_local = ms / 1e3
-    agg = torch.tensor([total_nodes * args.steps, secs_local], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        s_nodes = agg[:1].clone()
-        dist.all_reduce(s_nodes)
-        s_time = agg[1:].clone()
-        dist.all_reduce(s_time, op=dist.ReduceOp.MAX)
-        agg = torch.cat([s_nodes, s_time])
-    value = float(agg[0]) / float(agg[1])
+    job_ados, job_secs = reduce_throughput(dist, total_nodes * args.steps, secs_local, "cuda")
+    value = job_ados / job_secs
 
     # e2e through the C ABI: initial tops from the host, propagate with every
     # observation copied back, ensemble mean of the site populations
@@ -377,7 +383,7 @@ def run_batched(args, world, rank, local_rank):
     classes = E.classes()
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": float(agg[1]) * 1e3 / args.steps,
+                "warmup": args.warmup, "ms_per_step": job_secs * 1e3 / args.steps,
                 "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded H, Drude-Lorentz baths)",
                 "config": {"workload": workload, "instances": count, "ados": total_nodes * world,

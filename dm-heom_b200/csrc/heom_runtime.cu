@@ -1433,6 +1433,7 @@ struct heom_ensemble {
     cudaGraphExec_t step_graph = nullptr;
     double graph_dt = 0.0;
     bool tuned = false;
+    bool serial = false; // classes one after another in the step graph (else side by side)
     double tuned_us = 0.0;
 
     ~heom_ensemble()
@@ -1484,13 +1485,16 @@ size_t class_footprint(const heom_instance_desc* descs, const std::vector<int32_
 int ens_enqueue_step(heom_ensemble* e, double dt)
 {
     CUDA_TRY(cudaEventRecord(e->fork, e->stream));
+    cudaEvent_t prev = e->fork;
     for (size_t c = 0; c < e->cls.size(); ++c) {
         heom_handle* h = e->cls[c];
-        CUDA_TRY(cudaStreamWaitEvent(h->stream, e->fork, 0));
+        CUDA_TRY(cudaStreamWaitEvent(h->stream, e->serial ? prev : e->fork, 0));
         if (int rc = enqueue_step(h, dt)) return rc;
         CUDA_TRY(cudaEventRecord(e->join[c], h->stream));
-        CUDA_TRY(cudaStreamWaitEvent(e->stream, e->join[c], 0));
+        if (e->serial) prev = e->join[c];
+        else CUDA_TRY(cudaStreamWaitEvent(e->stream, e->join[c], 0));
     }
+    if (e->serial) CUDA_TRY(cudaStreamWaitEvent(e->stream, prev, 0));
     return 0;
 }
 
@@ -1511,15 +1515,18 @@ int ens_probe_graph(heom_ensemble* e, cudaGraphExec_t* out)
     CUDA_TRY(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
     int rc = 0;
     cudaError_t ce = cudaEventRecord(e->fork, e->stream);
+    cudaEvent_t prev = e->fork;
     for (size_t c = 0; c < e->cls.size() && !rc && ce == cudaSuccess; ++c) {
         heom_handle* h = e->cls[c];
-        ce = cudaStreamWaitEvent(h->stream, e->fork, 0);
+        ce = cudaStreamWaitEvent(h->stream, e->serial ? prev : e->fork, 0);
         if (ce == cudaSuccess)
             rc = launch_stage(h, EPI_AXPY_SELF, h->work[0].p, nullptr, h->work[1].p, nullptr,
                               make_double2(1e-30, 0.0), 0);
         if (!rc && ce == cudaSuccess) ce = cudaEventRecord(e->join[c], h->stream);
-        if (!rc && ce == cudaSuccess) ce = cudaStreamWaitEvent(e->stream, e->join[c], 0);
+        if (e->serial) prev = e->join[c];
+        else if (!rc && ce == cudaSuccess) ce = cudaStreamWaitEvent(e->stream, e->join[c], 0);
     }
+    if (e->serial && !rc && ce == cudaSuccess) ce = cudaStreamWaitEvent(e->stream, prev, 0);
     cudaError_t ce2 = cudaStreamEndCapture(e->stream, &graph);
     for (size_t c = 0; c < e->cls.size(); ++c) e->cls[c]->launches = saved[c];
     if (rc || ce != cudaSuccess || ce2 != cudaSuccess) {
@@ -1535,7 +1542,13 @@ int ens_probe_graph(heom_ensemble* e, cudaGraphExec_t* out)
 }
 
 std::mutex g_tune_mu;
-std::vector<std::pair<std::string, std::vector<int>>> g_tune_cache;
+struct TuneEntry {
+    std::string sig;
+    std::vector<int> blocks;
+    bool serial;
+    double us;
+};
+std::vector<TuneEntry> g_tune_cache;
 
 std::string ens_signature(const heom_ensemble* e)
 {
@@ -1571,8 +1584,10 @@ int ens_autotune(heom_ensemble* e, double* best_us)
     {
         std::lock_guard<std::mutex> lock(g_tune_mu);
         for (auto& entry : g_tune_cache)
-            if (entry.first == sig) {
-                for (size_t c = 0; c < C; ++c) e->cls[c]->grid_override = entry.second[c];
+            if (entry.sig == sig) {
+                for (size_t c = 0; c < C; ++c) e->cls[c]->grid_override = entry.blocks[c];
+                e->serial = entry.serial;
+                e->tuned_us = entry.us;
                 e->tuned = true;
                 ens_drop_graph(e);
                 if (best_us) *best_us = e->tuned_us;
@@ -1596,6 +1611,15 @@ int ens_autotune(heom_ensemble* e, double* best_us)
         for (size_t c = 0; c < C; ++c) v[c] = std::min(v[c], std::max(groups[c], 1));
     std::sort(cand.begin(), cand.end());
     cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+    // every shape side by side; with more than one class also the full waves one class after another
+    // (a class of large instances fills the device alone; side by side they share L2)
+    std::vector<std::pair<std::vector<int>, bool>> shapes;
+    for (auto& v : cand) shapes.push_back({v, false});
+    if (C > 1) {
+        std::vector<int> fullc = full;
+        for (size_t c = 0; c < C; ++c) fullc[c] = std::min(fullc[c], std::max(groups[c], 1));
+        shapes.push_back({fullc, true});
+    }
 
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     CUDA_TRY(cudaEventCreate(&t0));
@@ -1603,8 +1627,9 @@ int ens_autotune(heom_ensemble* e, double* best_us)
     double best = 1e300;
     size_t pick = 0;
     int rc = 0;
-    for (size_t q = 0; q < cand.size() && !rc; ++q) {
-        for (size_t c = 0; c < C; ++c) e->cls[c]->grid_override = cand[q][c];
+    for (size_t q = 0; q < shapes.size() && !rc; ++q) {
+        for (size_t c = 0; c < C; ++c) e->cls[c]->grid_override = shapes[q].first[c];
+        e->serial = shapes[q].second;
         cudaGraphExec_t g = nullptr;
         if ((rc = ens_probe_graph(e, &g))) break;
         const int warm = 2, reps = 5;
@@ -1633,13 +1658,14 @@ int ens_autotune(heom_ensemble* e, double* best_us)
     if (rc) return rc;
     for (heom_handle* h : e->cls)
         if (int rc2 = check_kernel_error(h)) return rc2;
-    for (size_t c = 0; c < C; ++c) e->cls[c]->grid_override = cand[pick][c];
+    for (size_t c = 0; c < C; ++c) e->cls[c]->grid_override = shapes[pick].first[c];
+    e->serial = shapes[pick].second;
     e->tuned = true;
     e->tuned_us = best;
     ens_drop_graph(e);
     {
         std::lock_guard<std::mutex> lock(g_tune_mu);
-        g_tune_cache.emplace_back(sig, cand[pick]);
+        g_tune_cache.push_back({sig, shapes[pick].first, shapes[pick].second, best});
     }
     if (best_us) *best_us = best;
     return 0;
