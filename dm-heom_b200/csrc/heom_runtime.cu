@@ -214,6 +214,8 @@ struct heom_handle {
     // sizes shared by every instance of the handle
     int N = 0, M = 0, B = 0, BPS = 0, W = 0, D = 0; // D = largest depth
     int64_t nodes = 0;                              // ADOs of all instances
+    int64_t n_active = 0;                           // ADOs the stage kernels sweep (internal [0, n_active))
+    bool compact = false;                           // masked ADOs moved behind the active ones and not swept
     int LS = 0, SL = 0, SLT = 2;
     int P = 0;          // 32-byte sectors per ADO (pair layout)
     int NW = 0, TWB = 0; // padded widths of the neighbour and tuple rows
@@ -493,7 +495,7 @@ PairParams base_params(const heom_handle* h)
     p.inst = h->n_inst > 1 ? h->d_inst.p : nullptr;
     p.gamma0 = h->d_gamma0.p;
     p.slots = h->d_slots.p;
-    p.nodes = h->nodes;
+    p.nodes = h->n_active;
     p.W = h->W;
     p.NW = h->NW;
     p.TWB = h->TWB;
@@ -551,7 +553,7 @@ int resolve_stage(heom_handle* h, const void** fn_out, int* blocks_out = nullptr
         if (per_sm < 1) return fail(HEOM_E_UNSUPPORTED, "stage kernel cannot be resident");
     }
     const int teams = h->N <= 8 ? heomk::kCtaWarps : cta_teams(h->N);
-    const int64_t groups = (h->nodes + teams - 1) / teams;
+    const int64_t groups = std::max<int64_t>(1, (h->n_active + teams - 1) / teams);
     const int64_t want = h->grid_override > 0 ? h->grid_override : (int64_t)per_sm * h->sm_count;
     if (blocks_out) *blocks_out = (int)std::max<int64_t>(1, std::min<int64_t>(groups, want));
     h->stage_smem = smem;
@@ -881,8 +883,25 @@ void build_order(heom_handle* h)
             for (int64_t r = 0; r < nodes; ++r) h->int_of_ref[base + r] = base + r;
         h->top_int[k] = h->int_of_ref[base];
     }
+    h->n_active = h->nodes;
+    if (h->compact) {
+        // active ADOs first, masked ones behind, each group in the order above
+        std::vector<int64_t> by_int(h->nodes);
+        for (int64_t r = 0; r < h->nodes; ++r) by_int[h->int_of_ref[r]] = r;
+        int64_t a = 0;
+        for (int64_t q = 0; q < h->nodes; ++q)
+            if (h->mask[by_int[q]]) ++a;
+        h->n_active = a;
+        int64_t ia = 0, im = a;
+        for (int64_t q = 0; q < h->nodes; ++q) {
+            const int64_t r = by_int[q];
+            h->int_of_ref[r] = h->mask[r] ? ia++ : im++;
+        }
+        for (int k = 0; k < h->n_inst; ++k) h->top_int[k] = h->int_of_ref[h->inst_base[k]];
+    }
     for (int64_t r = 0; r < h->nodes; ++r) h->ref_of_int[h->int_of_ref[r]] = r;
 }
+
 
 int conv_blocks(const heom_handle* h, int64_t count)
 {
@@ -921,6 +940,25 @@ int from_internal(heom_handle* h, double* host, const double2* src)
     }
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     return 0;
+}
+
+// rebuild the internal order (and everything indexed by it) after a change of
+// the mask or of the compaction mode; the propagation state keeps its values
+int reorder(heom_handle* h)
+{
+    std::vector<double> ref((size_t)h->nodes * h->N * h->N * 2);
+    if (int rc = from_internal(h, ref.data(), h->y.data.p)) return rc;
+    build_order(h);
+    CUDA_TRY(cudaMemcpy(h->d_int_of_ref.p, h->int_of_ref.data(), h->nodes * 8, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(h->d_top.p, h->top_int.data(), h->n_inst * 8, cudaMemcpyHostToDevice));
+    if (int rc = build_neighbours(h)) return rc;
+    for (auto& w : h->work)
+        if (w.p) CUDA_TRY(cudaMemset(w.p, 0, h->state_elems() * sizeof(double2)));
+    if (h->step_graph) {
+        cudaGraphExecDestroy(h->step_graph);
+        h->step_graph = nullptr;
+    }
+    return to_internal(h, h->y.data.p, ref.data());
 }
 
 // ---------------------------------------------------------------------------
@@ -1138,8 +1176,28 @@ int heom_set_mask(heom_handle* h, const uint8_t* mask)
     for (int64_t q = 0; q < h->nodes; ++q)
         if (mask[q] > 2) return fail(HEOM_E_ARG, "mask[%lld] = %d is not a mask value", (long long)q, mask[q]);
     h->mask.assign(mask, mask + h->nodes);
+    if (h->compact) {
+        h->compact = false;
+        return reorder(h);
+    }
     return build_neighbours(h);
 }
+
+int heom_set_mask_compact(heom_handle* h, const uint8_t* mask)
+{
+    if (!h || !mask) return fail(HEOM_E_ARG, "NULL argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    for (int64_t q = 0; q < h->nodes; ++q)
+        if (mask[q] > 2) return fail(HEOM_E_ARG, "mask[%lld] = %d is not a mask value", (long long)q, mask[q]);
+    for (int k = 0; k < h->n_inst; ++k)
+        if (!mask[h->inst_base[k]]) return fail(HEOM_E_ARG, "instance %d: the top ADO is masked", k);
+    h->mask.assign(mask, mask + h->nodes);
+    h->compact = true;
+    return reorder(h);
+}
+
+int64_t heom_active_matrices(const heom_handle* h) { return h ? h->n_active : 0; }
 
 size_t heom_buffer_size_byte(const heom_handle* h) { return h ? h->state_elems() * sizeof(double2) : 0; }
 

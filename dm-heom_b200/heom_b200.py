@@ -46,7 +46,7 @@ EXPORTS = [
     "heom_ensemble_kernel_launches", "heom_ensemble_stream",
     "heom_adjoint_create", "heom_adjoint_destroy", "heom_adjoint_handle", "heom_adjoint_gradient",
     "heom_adjoint_kernel_launches", "heom_bath_derivatives", "heom_adjoint_create_batch",
-    "heom_adjoint_instances",
+    "heom_adjoint_instances", "heom_set_mask_compact", "heom_active_matrices",
 ]
 
 
@@ -93,6 +93,9 @@ def lib():
             getattr(L, name).argtypes = [vp]
         L.heom_set_hamiltonian.argtypes = [vp, vp]
         L.heom_set_mask.argtypes = [vp, vp]
+        L.heom_set_mask_compact.argtypes = [vp, vp]
+        L.heom_active_matrices.restype = i64
+        L.heom_active_matrices.argtypes = [vp]
         L.heom_buffer_create.argtypes = [vp, C.POINTER(vp)]
         L.heom_buffer_destroy.argtypes = [vp]
         L.heom_buffer_write.argtypes = [vp, vp, vp]
@@ -346,9 +349,14 @@ class Heom:
         assert ham.size == self.states * self.states * 2
         _check(lib().heom_set_instance_hamiltonian(self.h, k, _ptr(ham)))
 
-    def set_mask(self, mask):
+    def set_mask(self, mask, compact=False):
+        """compact: masked ADOs are not swept (heom_set_mask_compact)."""
         mask = np.ascontiguousarray(mask, dtype=np.uint8)
-        _check(lib().heom_set_mask(self.h, _ptr(mask)))
+        fn = lib().heom_set_mask_compact if compact else lib().heom_set_mask
+        _check(fn(self.h, _ptr(mask)))
+
+    def active_matrices(self):
+        return lib().heom_active_matrices(self.h)
 
     # -- stepping ------------------------------------------------------------
     def rk4_steps(self, dt, steps):

@@ -135,6 +135,16 @@ int heom_destroy(heom_handle* h);
 
 int heom_set_hamiltonian(heom_handle* h, const double* hamiltonian);
 int heom_set_mask(heom_handle* h, const uint8_t* mask);
+/* The mask with compaction (no counterpart in the reference): masked ADOs are
+ * moved behind the active ones in device memory and no stage kernel sweeps
+ * them, so a filtered hierarchy costs only its active ADOs.  The active ADOs
+ * (and so every observed top) evolve exactly as with heom_set_mask (bit for
+ * bit): the reference computes masked ADOs but never reads them.  Masked
+ * entries of the state keep the values they had.  The top ADO of every
+ * instance must be active.  heom_set_mask returns to the uncompacted mode. */
+int heom_set_mask_compact(heom_handle* h, const uint8_t* mask);
+/* ADOs the stage kernels sweep (heom_matrices without compaction). */
+int64_t heom_active_matrices(const heom_handle* h);
 
 int heom_buffer_create(heom_handle* h, heom_buffer** out);
 int heom_buffer_destroy(heom_buffer* b);

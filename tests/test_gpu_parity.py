@@ -207,3 +207,42 @@ def test_nonfinite_state_is_reported():
         with pytest.raises(hb.HeomError) as e:
             H.propagate(1e-15, 2, 1)
         assert "heom error -6" in str(e.value)
+
+
+@pytest.mark.parametrize("n,m,depth,layer", [(4, 2, 4, 1), (7, 1, 4, 2), (9, 1, 3, 1)])
+def test_compacted_mask_is_bit_identical_on_active_ados(n, m, depth, layer):
+    """heom_set_mask_compact sweeps only the active ADOs; they (and every top)
+    evolve exactly as under heom_set_mask, masked entries keep their values."""
+    sysd = hb.System(ho.synthetic_hamiltonian(n, 40 + n), [35.0] * n, [50.0] * n, [0.0] * n, m, 300.0, depth)
+    mask = hb.tables_mask(sysd, "single_excitation", layer)
+    assert 0 < mask.sum() < mask.size
+    y0 = np.zeros(hb.build_tables(sysd)["matrices"] * n * n * 2)
+    y0[0] = 1.0
+    y0[-2] = 0.25  # an entry of the last ADO (masked for these systems)
+    runs = []
+    for compact in (False, True):
+        with hb.from_system(sysd) as H:
+            H.set_state(y0)
+            H.set_mask(mask, compact=compact)
+            assert H.active_matrices() == (mask.sum() if compact else mask.size)
+            tops = H.propagate(1e-15, 60, 10)
+            runs.append((tops, H.get_state()))
+    (t1, s1), (t2, s2) = runs
+    assert np.array_equal(t1, t2)
+    act = np.repeat(mask.astype(bool), n * n * 2)
+    assert np.array_equal(s1[act], s2[act])
+    assert np.array_equal(s2[~act], y0[~act])
+
+
+def test_compaction_switches_back_and_keeps_the_state():
+    n = 4
+    sysd = hb.System(ho.synthetic_hamiltonian(n, 3), [35.0] * n, [50.0] * n, [0.0] * n, 2, 300.0, 3)
+    mask = hb.tables_mask(sysd, "single_excitation", 1)
+    with hb.from_system(sysd) as H:
+        y = np.random.default_rng(0).normal(size=H.state_len)
+        H.set_state(y)
+        H.set_mask(mask, compact=True)
+        assert np.array_equal(H.get_state(), y)  # reordering keeps every entry
+        H.set_mask(mask)
+        assert H.active_matrices() == mask.size
+        assert np.array_equal(H.get_state(), y)
