@@ -1128,6 +1128,27 @@ __global__ void heom_add_top(double2* __restrict__ y, const double2* __restrict_
     }
 }
 
+// Frobenius norm squared of every ADO, sum |sigma(i,j)|^2 (hierarchy_norm.cl:15-45),
+// written at the ADO's reference index.  One warp per ADO; a padding half of
+// an odd diagonal pair counts once.
+__global__ void heom_hierarchy_norm(double* __restrict__ norms, const double2* __restrict__ y,
+                                    const int64_t* __restrict__ ref_of_int, const int16_t* __restrict__ pe,
+                                    int64_t nodes, int P)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t stride = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t u = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); u < nodes; u += stride) {
+        double acc = 0.0;
+        for (int pr = lane; pr < P; pr += 32) {
+            const double2 a = y[(u * P + pr) * 2], b = y[(u * P + pr) * 2 + 1];
+            acc += a.x * a.x + a.y * a.y;
+            if (pe[2 * pr + 1] != pe[2 * pr]) acc += b.x * b.x + b.y * b.y;
+        }
+        for (int off = 16; off > 0; off >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, off);
+        if (lane == 0) norms[ref_of_int[u]] = acc;
+    }
+}
+
 // Sets *flag when any element is not finite.
 __global__ void heom_check_finite(const double* __restrict__ y, int64_t len, int* flag)
 {

@@ -247,7 +247,7 @@ struct heom_handle {
     DevBuf<double> d_chat, d_sq;     // factored coefficients (DMMA kernel)
     DevBuf<double2> d_khat;
     DevBuf<int16_t> d_pos;
-    DevBuf<int64_t> d_int_of_ref;
+    DevBuf<int64_t> d_int_of_ref, d_ref_of_int;
     DevBuf<int16_t> d_pair;          // [P][2] element indices of the sector halves
     std::vector<int16_t> pair_tab;   // host copy
     heomk::LaneTab lane_tab{};       // DMMA kernel lane tables (N <= 8)
@@ -950,6 +950,7 @@ int reorder(heom_handle* h)
     if (int rc = from_internal(h, ref.data(), h->y.data.p)) return rc;
     build_order(h);
     CUDA_TRY(cudaMemcpy(h->d_int_of_ref.p, h->int_of_ref.data(), h->nodes * 8, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(h->d_ref_of_int.p, h->ref_of_int.data(), h->nodes * 8, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(h->d_top.p, h->top_int.data(), h->n_inst * 8, cudaMemcpyHostToDevice));
     if (int rc = build_neighbours(h)) return rc;
     for (auto& w : h->work)
@@ -1115,6 +1116,8 @@ int heom_create_batch(const heom_instance_desc* descs, int32_t count, const heom
     build_order(h.get());
     if (int rc = h->d_int_of_ref.alloc(h->nodes)) return rc;
     CUDA_TRY(cudaMemcpy(h->d_int_of_ref.p, h->int_of_ref.data(), h->nodes * 8, cudaMemcpyHostToDevice));
+    if (int rc = h->d_ref_of_int.alloc(h->nodes)) return rc;
+    CUDA_TRY(cudaMemcpy(h->d_ref_of_int.p, h->ref_of_int.data(), h->nodes * 8, cudaMemcpyHostToDevice));
     if (int rc = h->d_top.alloc(count)) return rc;
     CUDA_TRY(cudaMemcpy(h->d_top.p, h->top_int.data(), count * 8, cudaMemcpyHostToDevice));
     if (int rc = build_neighbours(h.get())) return rc;
@@ -1198,6 +1201,41 @@ int heom_set_mask_compact(heom_handle* h, const uint8_t* mask)
 }
 
 int64_t heom_active_matrices(const heom_handle* h) { return h ? h->n_active : 0; }
+
+int heom_get_mask(const heom_handle* h, uint8_t* mask)
+{
+    if (!h || !mask) return fail(HEOM_E_ARG, "NULL argument");
+    std::copy(h->mask.begin(), h->mask.end(), mask);
+    return 0;
+}
+
+int heom_hierarchy_norm(heom_handle* h, double threshold, double* norms)
+{
+    if (!h) return fail(HEOM_E_ARG, "NULL handle");
+    CUDA_TRY(cudaSetDevice(h->device));
+    DevBuf<double> d_norm;
+    if (int rc = d_norm.alloc(h->nodes)) return rc;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((h->nodes + 7) / 8, (int64_t)h->sm_count * 8));
+    heomk::heom_hierarchy_norm<<<blocks, 256, 0, h->stream>>>(d_norm.p, h->y.data.p, h->d_ref_of_int.p, h->d_pair.p,
+                                                              h->nodes, h->P);
+    h->launches++;
+    CUDA_TRY(cudaGetLastError());
+    std::vector<double> nv(h->nodes);
+    CUDA_TRY(cudaMemcpyAsync(nv.data(), d_norm.p, h->nodes * 8, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (norms) std::copy(nv.begin(), nv.end(), norms);
+    if (threshold < 0.0) return 0;
+    // deactivate unprotected ADOs at or below the threshold (hierarchy_norm.cl:42-44)
+    std::vector<uint8_t> mask = h->mask;
+    bool changed = false;
+    for (int64_t r = 0; r < h->nodes; ++r)
+        if (nv[r] - threshold <= 0.0 && mask[r] != 2 && mask[r] != 0) {
+            mask[r] = 0;
+            changed = true;
+        }
+    if (!changed) return 0;
+    return h->compact ? heom_set_mask_compact(h, mask.data()) : heom_set_mask(h, mask.data());
+}
 
 size_t heom_buffer_size_byte(const heom_handle* h) { return h ? h->state_elems() * sizeof(double2) : 0; }
 

@@ -11,8 +11,9 @@
 // runtime config is accepted and ignored.
 //
 // Observers write the files named in program.observations with the headers of
-// matrix_diagonal_observer.hpp:51-61, matrix_complete_observer.hpp and
-// matrix_trace_observer.hpp:111-116 (one line per observation: time, then the
+// matrix_diagonal_observer.hpp:51-61, matrix_complete_observer.hpp,
+// matrix_trace_observer.hpp:111-116, hierarchy_norm_observer.hpp:61-68 and
+// hierarchy_complete_observer.hpp:58-70 (one line per observation: time, then the
 // values), tab separated, numbers with 17 significant digits.
 #include <chrono>
 #include <cstdio>
@@ -83,15 +84,41 @@ std::string fmt(double v)
 
 const char kDelim = '\t';
 
+bool whole_hierarchy(const std::string& type) { return type == "hierarchy_norm" || type == "hierarchy_complete"; }
+
+void check(int rc)
+{
+    if (rc != 0) throw std::runtime_error(std::string("heom error: ") + heom_last_error());
+}
+
 struct file_observer {
     std::string type;
     std::ofstream out;
     int n;
-    file_observer(const observation& o, int states) : type(o.type), out(o.filename), n(states)
+    heom_handle* h;
+    int64_t matrices;
+    std::vector<double> buf;
+    file_observer(const observation& o, int states, heom_handle* handle, const hierarchy_graph& g)
+        : type(o.type), out(o.filename), n(states), h(handle), matrices(g.nodes())
     {
         if (!out.is_open()) throw std::runtime_error("file_observer_wrapper(): error: could not open output file: " + o.filename);
         out << "time";
-        if (type == "matrix_diagonal") {
+        if (type == "hierarchy_norm") { // hierarchy_norm_observer.hpp:61-68: one column per ADO tuple
+            const int64_t w = g.width();
+            for (int64_t u = 0; u < matrices; ++u) {
+                out << kDelim << '{';
+                for (int64_t k = 0; k < w; ++k) out << (k ? ", " : "") << g.tuples()[u * w + k];
+                out << '}';
+            }
+            buf.resize(matrices);
+        } else if (type == "hierarchy_complete") { // hierarchy_complete_observer.hpp:58-70
+            for (int64_t u = 0; u < matrices; ++u)
+                for (int i = 0; i < n; ++i)
+                    for (int j = 0; j < n; ++j)
+                        for (int k = 0; k < 2; ++k)
+                            out << kDelim << "mat_" << u << "_elem_" << i << "_" << j << (k == 0 ? "_real" : "_imag");
+            buf.resize((size_t)matrices * n * n * 2);
+        } else if (type == "matrix_diagonal") {
             for (int i = 0; i < n; ++i) out << kDelim << "site_" << i;
         } else if (type == "matrix_complete") {
             for (int i = 0; i < n; ++i)
@@ -105,7 +132,13 @@ struct file_observer {
     void observe(double time, const double* top)
     {
         out << fmt(time);
-        if (type == "matrix_diagonal") {
+        if (type == "hierarchy_norm") {
+            check(heom_hierarchy_norm(h, -1.0, buf.data()));
+            for (double v : buf) out << kDelim << fmt(v);
+        } else if (type == "hierarchy_complete") {
+            check(heom_get_state(h, buf.data()));
+            for (double v : buf) out << kDelim << fmt(v);
+        } else if (type == "matrix_diagonal") {
             for (int i = 0; i < n; ++i) out << kDelim << fmt(top[(n + 1) * 2 * i]);
         } else if (type == "matrix_complete") {
             for (int q = 0; q < 2 * n * n; ++q) out << kDelim << fmt(top[q]);
@@ -121,11 +154,6 @@ struct file_observer {
     }
 };
 
-void check(int rc)
-{
-    if (rc != 0) throw std::runtime_error(std::string("heom error: ") + heom_last_error());
-}
-
 } // namespace
 
 int main(int argc, char* argv[])
@@ -140,9 +168,13 @@ int main(int argc, char* argv[])
         runtime_config rc = read_runtime_config(argv[1]);
         std::cout << "Parsing HEOM configuration from file: " << argv[2] << std::endl;
         heomhost::config cfg(argv[2]);
-        for (const auto& o : cfg.observations())
-            if (o.type != "matrix_diagonal" && o.type != "matrix_complete" && o.type != "matrix_trace_id")
+        bool per_observation = false; // observers that read the whole hierarchy
+        for (const auto& o : cfg.observations()) {
+            if (o.type != "matrix_diagonal" && o.type != "matrix_complete" && o.type != "matrix_trace_id" &&
+                !whole_hierarchy(o.type))
                 throw config_error("observation type " + o.type + " is not supported by this application");
+            per_observation = per_observation || whole_hierarchy(o.type);
+        }
 
         instance inst = make_instance(cfg.system());
         const int n = inst.sys.states;
@@ -164,7 +196,7 @@ int main(int argc, char* argv[])
         check(heom_set_top(h, top.data()));
 
         std::vector<std::unique_ptr<file_observer>> obs;
-        for (const auto& o : cfg.observations()) obs.emplace_back(new file_observer(o, n));
+        for (const auto& o : cfg.observations()) obs.emplace_back(new file_observer(o, n, h, g));
 
         const int64_t observe_steps = cfg.observe_steps();
         const int64_t iterations = cfg.steps() / observe_steps;
@@ -173,12 +205,21 @@ int main(int argc, char* argv[])
         std::vector<double> tops((size_t)(chunk + 1) * 2 * n * n);
         for (auto& o : obs) o->observe(0.0, top.data()); // observer_list.observe(0.0)
         const auto ts = std::chrono::steady_clock::now();
-        for (int64_t i = 0; i < iterations; i += chunk) {
-            const int64_t rows = std::min(chunk, iterations - i);
-            check(heom_propagate(h, dt, rows * observe_steps, observe_steps, tops.data()));
-            for (int64_t r = 1; r <= rows; ++r) {
-                const double time = (double)((i + r) * observe_steps) * dt;
-                for (auto& o : obs) o->observe(time, tops.data() + r * 2 * n * n);
+        if (per_observation) {
+            // every observation reads from the device: one stepping call per observation
+            for (int64_t i = 1; i <= iterations; ++i) {
+                check(heom_rk4_steps(h, dt, observe_steps));
+                check(heom_get_top(h, top.data()));
+                for (auto& o : obs) o->observe((double)(i * observe_steps) * dt, top.data());
+            }
+        } else {
+            for (int64_t i = 0; i < iterations; i += chunk) {
+                const int64_t rows = std::min(chunk, iterations - i);
+                check(heom_propagate(h, dt, rows * observe_steps, observe_steps, tops.data()));
+                for (int64_t r = 1; r <= rows; ++r) {
+                    const double time = (double)((i + r) * observe_steps) * dt;
+                    for (auto& o : obs) o->observe(time, tops.data() + r * 2 * n * n);
+                }
             }
         }
         const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - ts).count();

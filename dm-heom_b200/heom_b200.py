@@ -46,7 +46,8 @@ EXPORTS = [
     "heom_ensemble_kernel_launches", "heom_ensemble_stream",
     "heom_adjoint_create", "heom_adjoint_destroy", "heom_adjoint_handle", "heom_adjoint_gradient",
     "heom_adjoint_kernel_launches", "heom_bath_derivatives", "heom_adjoint_create_batch",
-    "heom_adjoint_instances", "heom_set_mask_compact", "heom_active_matrices",
+    "heom_adjoint_instances", "heom_set_mask_compact", "heom_active_matrices", "heom_get_mask",
+    "heom_hierarchy_norm",
 ]
 
 
@@ -96,6 +97,8 @@ def lib():
         L.heom_set_mask_compact.argtypes = [vp, vp]
         L.heom_active_matrices.restype = i64
         L.heom_active_matrices.argtypes = [vp]
+        L.heom_get_mask.argtypes = [vp, vp]
+        L.heom_hierarchy_norm.argtypes = [vp, dbl, vp]
         L.heom_buffer_create.argtypes = [vp, C.POINTER(vp)]
         L.heom_buffer_destroy.argtypes = [vp]
         L.heom_buffer_write.argtypes = [vp, vp, vp]
@@ -357,6 +360,17 @@ class Heom:
 
     def active_matrices(self):
         return lib().heom_active_matrices(self.h)
+
+    def get_mask(self):
+        m = np.zeros(self.matrices, np.uint8)
+        _check(lib().heom_get_mask(self.h, _ptr(m)))
+        return m
+
+    def hierarchy_norm(self, threshold=-1.0):
+        """Per-ADO sum |sigma_ij|^2 (uid order); threshold >= 0 also filters the mask."""
+        v = np.empty(self.matrices)
+        _check(lib().heom_hierarchy_norm(self.h, threshold, _ptr(v)))
+        return v
 
     # -- stepping ------------------------------------------------------------
     def rk4_steps(self, dt, steps):

@@ -145,6 +145,15 @@ int heom_set_mask(heom_handle* h, const uint8_t* mask);
 int heom_set_mask_compact(heom_handle* h, const uint8_t* mask);
 /* ADOs the stage kernels sweep (heom_matrices without compaction). */
 int64_t heom_active_matrices(const heom_handle* h);
+/* The current mask (reference uid order, all instances). */
+int heom_get_mask(const heom_handle* h, uint8_t* mask);
+/* solver_base::update_hierarchy_norm + hierarchy_norm (solver_base.hpp:225-228,
+ * 270-273; hierarchy_norm.cl:15-45): norms[u] = sum_ij |sigma_u(i,j)|^2 of the
+ * propagation state, in uid order (norms may be NULL).  With threshold >= 0
+ * every ADO at or below it whose mask entry is not protected (2) is switched
+ * off, as the reference kernel does to its filter (the compaction mode of the
+ * handle is kept); threshold < 0 leaves the mask alone. */
+int heom_hierarchy_norm(heom_handle* h, double threshold, double* norms);
 
 int heom_buffer_create(heom_handle* h, heom_buffer** out);
 int heom_buffer_destroy(heom_buffer* b);

@@ -1,0 +1,75 @@
+"""GPU: the population-dynamics application end to end (reference command
+line and config files, all five observer types) and the hierarchy norm."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import heom_b200 as hb
+import heom_oracle as ho
+from test_host import FMO_CFG
+
+pytestmark = pytest.mark.gpu
+
+APP = os.path.join(os.path.dirname(hb.__file__), "bin", "heom_population_dynamics")
+
+
+def read_dat(path):
+    lines = open(path).read().strip().split("\n")
+    return lines[0].split("\t"), np.array([[float(x) for x in l.split("\t")] for l in lines[1:]])
+
+
+def test_app_observers_match_oracle(tmp_path):
+    cfg = FMO_CFG.replace(
+        "observations={(matrix_complete, m.dat), (matrix_diagonal, d.dat), (matrix_trace_id, t.dat)}",
+        "observations={(matrix_complete, m.dat), (matrix_diagonal, d.dat), (matrix_trace_id, t.dat), "
+        "(hierarchy_norm, n.dat), (hierarchy_complete, c.dat)}")
+    (tmp_path / "heom.cfg").write_text(cfg)
+    (tmp_path / "rt.cfg").write_text("[opencl]\nplatform_index=0\n[cuda]\ndevice_index=0\nrk4_scheme=product\n")
+    r = subprocess.run([APP, "rt.cfg", "heom.cfg"], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    h = np.array([[12410.0, -87.7, 5.5], [-87.7, 12530.0, 30.8], [5.5, 30.8, 12210.0]])
+    prob = ho.build_problem(ho.make_system(h, [35] * 3, [50] * 3, [0] * 3, 2, 77.0, 3))
+    _, ref = ho.propagate(prob, 1e-15, 20, 5)
+    hd, d = read_dat(tmp_path / "d.dat")
+    assert hd == ["time", "site_0", "site_1", "site_2"]
+    assert np.max(np.abs(d[:, 1:] - ref)) <= 1e-10
+    assert np.allclose(d[:, 0], np.arange(5) * 5e-15, rtol=1e-15, atol=0)
+    _, t = read_dat(tmp_path / "t.dat")
+    assert np.max(np.abs(t[:, 1] - 1.0)) <= 1e-12
+    # hierarchy_complete: the whole state in uid order; hierarchy_norm: sum |sigma_ij|^2 per ADO
+    hc, c = read_dat(tmp_path / "c.dat")
+    nodes = prob.graph.nodes
+    assert len(hc) == 1 + nodes * 9 * 2 and hc[1] == "mat_0_elem_0_0_real"
+    hn, nrm = read_dat(tmp_path / "n.dat")
+    assert len(hn) == 1 + nodes and hn[1] == "{0, 0, 0, 0, 0, 0}"
+    states = c[:, 1:].reshape(len(c), nodes, 18)
+    assert np.max(np.abs(nrm[:, 1:] - (states ** 2).sum(axis=2))) <= 1e-14 * max(1.0, nrm[:, 1:].max())
+    # the top of the last complete state is the last matrix_complete line
+    _, m = read_dat(tmp_path / "m.dat")
+    assert np.array_equal(m[-1, 1:], states[-1, 0])
+
+
+def test_hierarchy_norm_and_threshold_filter():
+    n = 4
+    sysd = hb.System(ho.synthetic_hamiltonian(n, 2), [35.0] * n, [50.0] * n, [0.0] * n, 2, 300.0, 3)
+    with hb.from_system(sysd) as H:
+        top = np.zeros(n * n * 2)
+        top[0] = 1.0
+        H.set_top(top)
+        H.rk4_steps(1e-15, 30)
+        y = H.get_state().reshape(H.matrices, n * n * 2)
+        norms = H.hierarchy_norm()
+        assert np.max(np.abs(norms - (y ** 2).sum(axis=1))) <= 1e-15 * norms.max()
+        # filter: protect two ADOs, switch off every other at or below the median
+        mask = np.ones(H.matrices, np.uint8)
+        low = np.argsort(norms)[:3]
+        mask[low[:2]] = 2
+        H.set_mask(mask)
+        thr = float(np.median(norms))
+        H.hierarchy_norm(thr)
+        got = H.get_mask()
+        want = mask.copy()
+        want[(norms <= thr) & (mask != 2)] = 0
+        assert np.array_equal(got, want)
