@@ -1128,6 +1128,82 @@ __global__ void heom_add_top(double2* __restrict__ y, const double2* __restrict_
     }
 }
 
+// ---------------------------------------------------------------------------
+// Time-dependent Hamiltonian (the e_field pre-evaluate action of the
+// reference, e_field.hpp:63-85): H(t) = H - E(t) D- - conj(E(t)) D+ with
+// E(t) = sum over the pulses of e0 exp(-(t - tc)^2 / (2 w^2)) exp(i (phi + omega t)).
+// One block builds the operand tables of H(t) for `nt` times t0 + c_s dt of
+// every instance: stage times c = (0, 1/2, 1) of an RK4 step when `time` is
+// given (t0 = *time, then *time += dt), or the single time t0 of an explicit
+// evaluation.
+// ---------------------------------------------------------------------------
+struct Pulse {
+    double e0, tc, w, omega, phi;
+};
+struct FieldParams {
+    const double2* h0;     // [K][N*N] H / hbar of every instance
+    const double2* dplus;  // [N*N] D+ / hbar
+    const double2* dminus; // [N*N] D- / hbar
+    Pulse pulse[2];        // pump, probe
+    double* time;          // step mode: device time of the propagation state (advanced by dt)
+    double t0, dt;         // explicit mode: the evaluation time t0 (time == nullptr)
+    double2* hs_t;         // [nt][K][N*N]
+    double* hr_t;          // [nt][K][N*(N+1)]
+    double* frag_t;        // [nt][K][256] (N <= 8)
+    int K, N, nt;
+};
+
+__device__ inline double2 field_at(const FieldParams& f, double t)
+{
+    double er = 0.0, ei = 0.0;
+    for (int q = 0; q < 2; ++q) {
+        const Pulse& pl = f.pulse[q];
+        const double d = t - pl.tc;
+        const double env = pl.e0 * exp(-d * d / (2.0 * pl.w * pl.w));
+        double sn, cs;
+        sincos(pl.phi + pl.omega * t, &sn, &cs);
+        er += env * cs;
+        ei += env * sn;
+    }
+    return make_double2(er, ei);
+}
+
+__global__ void heom_field_tables(const FieldParams f)
+{
+    const int N = f.N, NN = N * N;
+    const double t0 = f.time ? *f.time : f.t0;
+    const double cst[3] = {0.0, 0.5, 1.0};
+    for (int s = 0; s < f.nt; ++s) {
+        const double2 E = field_at(f, t0 + cst[s] * f.dt);
+        for (int k = 0; k < f.K; ++k) {
+            double2* hs = f.hs_t + ((size_t)s * f.K + k) * NN;
+            for (int q = threadIdx.x; q < NN; q += blockDim.x) {
+                const double2 h = f.h0[(size_t)k * NN + q], dm = f.dminus[q], dp = f.dplus[q];
+                // H - E D- - conj(E) D+
+                const double re = h.x - (E.x * dm.x - E.y * dm.y) - (E.x * dp.x + E.y * dp.y);
+                const double im = h.y - (E.x * dm.y + E.y * dm.x) - (E.x * dp.y - E.y * dp.x);
+                hs[q] = make_double2(re, im);
+                f.hr_t[((size_t)s * f.K + k) * N * (N + 1) + (q / N) * (N + 1) + q % N] = re;
+            }
+            __syncthreads();
+            if (N <= 8)
+                for (int q = threadIdx.x; q < 256; q += blockDim.x) {
+                    // operand fragments as in the host tables: part q >> 5 (re hb s0, s1 | im hb | re ha | im ha)
+                    const int l = q & 31, part = q >> 5, sl = part & 1, kind = part >> 1;
+                    const int r = l >> 2, c = 4 * sl + (l & 3);
+                    double v = 0.0;
+                    if (r < N && c < N) {
+                        const double2 hcr = hs[c * N + r], hrc = hs[r * N + c];
+                        v = kind == 0 ? hcr.x : kind == 1 ? hcr.y : kind == 2 ? -hrc.x : -hrc.y;
+                    }
+                    f.frag_t[((size_t)s * f.K + k) * 256 + q] = v;
+                }
+            __syncthreads();
+        }
+    }
+    if (f.time && threadIdx.x == 0) *f.time = t0 + f.dt;
+}
+
 // Frobenius norm squared of every ADO, sum |sigma(i,j)|^2 (hierarchy_norm.cl:15-45),
 // written at the ADO's reference index.  One warp per ADO; a padding half of
 // an odd diagonal pair counts once.

@@ -165,13 +165,16 @@ dmma_fn_t pick_dmma(int n, int hk, int slt, bool multi, bool adj)
     }
 }
 
-// tables of the adjoint operator L^H that replace the handle's own
+// tables that replace the handle's own in one stage launch: those of the
+// adjoint operator L^H (adjoint = true: conj(pf_same_sum), conj(gamma0), -H^H),
+// or those of a time-dependent H(t) (adjoint = false, handle's pss and gamma0)
 struct AdjTabs {
     const double2* pss;    // conj(pf_same_sum)
     const double2* gamma0; // conj(gamma0)
     const double* hfrag;   // fragments of -H^H
     const double* hr;      // -H (real symmetric H)
     const double2* hs;     // -H^H
+    bool adjoint = true;
 };
 
 // stage write modes (runtime parameters of the one stage kernel)
@@ -180,6 +183,7 @@ enum Epi : int {
     EPI_AXPY_SELF = 1, // out = w + beta L(w)
     EPI_AXPY_Y = 2,    // out = y + beta L(w)   (out may alias y)
     EPI_ACC = 3,       // out = L(w); acc = (acc_init ? w : acc) + beta L(w)
+    EPI_AXPY_ACC = 4,  // out = (y ? y : w) + beta L(w); acc = (acc_init ? w : acc) + acc_beta L(w)
 };
 
 // number of tuples over d coordinates with sum <= r
@@ -267,6 +271,15 @@ struct heom_handle {
     int per_sm[2][2] = {{0, 0}, {0, 0}}; // resident stage CTAs per SM, per [adjoint][H kind]
     int grid_override = 0;   // stage grid chosen by an autotuner (0: one full wave)
     size_t stage_smem = 0;
+
+    // time-dependent H (heom_set_field): H(t) = H - E(t) D- - conj(E(t)) D+
+    bool field_on = false;
+    heomk::Pulse pulses[2] = {};
+    DevBuf<double2> d_dplus, d_dminus;     // D+ / hbar, D- / hbar
+    DevBuf<double2> field_hs;              // [3][K][N*N]
+    DevBuf<double> field_hr, field_frag;   // [3][K][N*(N+1)], [3][K][256]
+    DevBuf<double> d_time;                 // time of the propagation state (device, advanced by field steps)
+    double time = 0.0;                     // host mirror
 
     // cached graph of one RK4 step
     cudaGraphExec_t step_graph = nullptr;
@@ -390,8 +403,9 @@ int upload_hamiltonian(heom_handle* h)
                  N <= 8 ? frag.data() + (size_t)k * 256 : nullptr);
         real_sym = real_sym && real_symmetric(hk, N);
     }
-    // real symmetric H (every instance) takes the cheaper kernel variants
-    h->hkind = real_sym ? heomk::H_REAL_SYM : heomk::H_GENERIC;
+    // real symmetric H (every instance) takes the cheaper kernel variants; a
+    // time-dependent H(t) is complex
+    h->hkind = real_sym && !h->field_on ? heomk::H_REAL_SYM : heomk::H_GENERIC;
     const std::vector<double2> g0 = gamma0_table(h, h->pf_same);
     if (!h->d_hs.p) {
         if (int rc = h->d_hs.alloc(hs.size())) return rc;
@@ -562,11 +576,12 @@ int resolve_stage(heom_handle* h, const void** fn_out, int* blocks_out = nullptr
 }
 
 int launch_stage(heom_handle* h, int epi, const double2* in, const double2* y, double2* out,
-                 double2* acc, double2 beta, int acc_init, const AdjTabs* adj = nullptr)
+                 double2* acc, double2 beta, int acc_init, const AdjTabs* adj = nullptr,
+                 double2 acc_beta = make_double2(0.0, 0.0))
 {
     const void* fn = nullptr;
     int blocks = 0;
-    if (int rc = resolve_stage(h, &fn, &blocks, adj != nullptr)) return rc;
+    if (int rc = resolve_stage(h, &fn, &blocks, adj && adj->adjoint)) return rc;
     PairParams p = base_params(h);
     if (adj) {
         p.pss = adj->pss;
@@ -590,6 +605,15 @@ int launch_stage(heom_handle* h, int epi, const double2* in, const double2* y, d
         p.y = y;
         p.alpha = make_double2(1.0, 0.0);
         p.beta = beta;
+        break;
+    case EPI_AXPY_ACC:
+        p.y = y;
+        p.alpha = make_double2(1.0, 0.0);
+        p.beta = beta;
+        p.acc = acc;
+        p.use_acc = 1;
+        p.acc_beta = acc_beta;
+        p.acc_init = acc_init;
         break;
     default: // EPI_ACC
         p.alpha = make_double2(0.0, 0.0);
@@ -648,11 +672,68 @@ int ensure_work(heom_handle* h, int count)
     return 0;
 }
 
+heomk::FieldParams field_params(heom_handle* h, int nt)
+{
+    heomk::FieldParams f{};
+    f.h0 = h->d_hs.p;
+    f.dplus = h->d_dplus.p;
+    f.dminus = h->d_dminus.p;
+    f.pulse[0] = h->pulses[0];
+    f.pulse[1] = h->pulses[1];
+    f.hs_t = h->field_hs.p;
+    f.hr_t = h->field_hr.p;
+    f.frag_t = h->field_frag.p;
+    f.K = h->n_inst;
+    f.N = h->N;
+    f.nt = nt;
+    return f;
+}
+
+// the tables of H at field time slot s (built by heom_field_tables)
+AdjTabs field_tabs(const heom_handle* h, int s)
+{
+    AdjTabs t;
+    t.pss = h->d_pss.p;
+    t.gamma0 = h->d_gamma0.p;
+    t.hfrag = h->field_frag.p + (size_t)s * h->n_inst * 256;
+    t.hr = h->field_hr.p + (size_t)s * h->n_inst * h->N * (h->N + 1);
+    t.hs = h->field_hs.p + (size_t)s * h->n_inst * h->N * h->N;
+    t.adjoint = false;
+    return t;
+}
+
+// one classical RK4 step with a time-dependent H: the tables of H(t),
+// H(t + dt/2), H(t + dt) from the device time, then four fused stages
+//   s1 = y + dt/2 L(t) y            acc = y + dt/6 L(t) y
+//   s2 = y + dt/2 L(t+dt/2) s1      acc += dt/3 L(t+dt/2) s1
+//   s1 = y + dt L(t+dt/2) s2        acc += dt/3 L(t+dt/2) s2
+//   y  = acc + dt/6 L(t+dt) s1
+int enqueue_field_step(heom_handle* h, double dt)
+{
+    heomk::FieldParams f = field_params(h, 3);
+    f.time = h->d_time.p;
+    f.dt = dt;
+    heomk::heom_field_tables<<<1, 256, 0, h->stream>>>(f);
+    h->launches++;
+    CUDA_TRY(cudaGetLastError());
+    double2* y = h->y.data.p;
+    double2* s1 = h->work[0].p;
+    double2* s2 = h->work[1].p;
+    double2* acc = h->work[2].p;
+    const AdjTabs t0 = field_tabs(h, 0), th = field_tabs(h, 1), t1 = field_tabs(h, 2);
+    auto c = [](double v) { return make_double2(v, 0.0); };
+    if (int rc = launch_stage(h, EPI_AXPY_ACC, y, nullptr, s1, acc, c(dt / 2), 1, &t0, c(dt / 6))) return rc;
+    if (int rc = launch_stage(h, EPI_AXPY_ACC, s1, y, s2, acc, c(dt / 2), 0, &th, c(dt / 3))) return rc;
+    if (int rc = launch_stage(h, EPI_AXPY_ACC, s2, y, s1, acc, c(dt), 0, &th, c(dt / 3))) return rc;
+    return launch_stage(h, EPI_AXPY_Y, s1, acc, y, nullptr, c(dt / 6), 0, &t1);
+}
+
 // enqueue one RK4 step of y_n (in place) on the handle's stream
 int enqueue_step(heom_handle* h, double dt)
 {
     double2* y = h->y.data.p;
     const double2 zero = make_double2(0.0, 0.0);
+    if (h->field_on) return enqueue_field_step(h, dt);
     switch (h->opt.rk4_scheme) {
     case HEOM_RK4_PRODUCT: {
         double2* a = h->work[0].p;
@@ -699,6 +780,7 @@ int enqueue_step(heom_handle* h, double dt)
 
 int prepare_scheme(heom_handle* h)
 {
+    if (h->field_on) return ensure_work(h, 3);
     switch (h->opt.rk4_scheme) {
     case HEOM_RK4_PRODUCT:
     case HEOM_RK4_HORNER: return ensure_work(h, 2);
@@ -709,6 +791,7 @@ int prepare_scheme(heom_handle* h)
 
 int launches_per_step(const heom_handle* h)
 {
+    if (h->field_on) return 5;
     return h->opt.rk4_scheme == HEOM_RK4_REFERENCE ? 8 : 4;
 }
 
@@ -716,6 +799,7 @@ int run_steps(heom_handle* h, double dt, int64_t steps)
 {
     if (steps <= 0) return 0;
     if (int rc = prepare_scheme(h)) return rc;
+    h->time += (double)steps * dt; // host mirror of the state's time (the device copy moves with field steps)
     if (!h->opt.use_graphs) {
         for (int64_t s = 0; s < steps; ++s)
             if (int rc = enqueue_step(h, dt)) return rc;
@@ -1202,6 +1286,63 @@ int heom_set_mask_compact(heom_handle* h, const uint8_t* mask)
 
 int64_t heom_active_matrices(const heom_handle* h) { return h ? h->n_active : 0; }
 
+int heom_set_field(heom_handle* h, const double* dipole_plus, const double* dipole_minus, const heom_pulse* pump,
+                   const heom_pulse* probe)
+{
+    if (!h || !dipole_plus || !dipole_minus || !pump || !probe) return fail(HEOM_E_ARG, "NULL argument");
+    const heom_pulse* pl[2] = {pump, probe};
+    for (int q = 0; q < 2; ++q)
+        if (!(pl[q]->time_width > 0.0) || !std::isfinite(pl[q]->efield) || !std::isfinite(pl[q]->time_center) ||
+            !std::isfinite(pl[q]->frequency) || !std::isfinite(pl[q]->phase))
+            return fail(HEOM_E_ARG, "pulse %d: width must be > 0 and every value finite", q);
+    CUDA_TRY(cudaSetDevice(h->device));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    const int N = h->N, K = h->n_inst;
+    std::vector<double2> dp(N * N), dm(N * N);
+    for (int q = 0; q < N * N; ++q) {
+        dp[q] = make_double2(dipole_plus[2 * q] / kHbar, dipole_plus[2 * q + 1] / kHbar);
+        dm[q] = make_double2(dipole_minus[2 * q] / kHbar, dipole_minus[2 * q + 1] / kHbar);
+    }
+    for (int q = 0; q < 2; ++q)
+        h->pulses[q] = heomk::Pulse{pl[q]->efield, pl[q]->time_center, pl[q]->time_width, pl[q]->frequency,
+                                    pl[q]->phase};
+    if (!h->d_dplus.p) {
+        if (int rc = h->d_dplus.alloc(N * N)) return rc;
+        if (int rc = h->d_dminus.alloc(N * N)) return rc;
+        if (int rc = h->field_hs.alloc((size_t)3 * K * N * N)) return rc;
+        if (int rc = h->field_hr.alloc((size_t)3 * K * N * (N + 1))) return rc;
+        if (int rc = h->field_frag.alloc((size_t)3 * K * 256)) return rc;
+        if (int rc = h->d_time.alloc(1)) return rc;
+        CUDA_TRY(cudaMemset(h->field_hr.p, 0, (size_t)3 * K * N * (N + 1) * 8));
+    }
+    CUDA_TRY(cudaMemcpy(h->d_dplus.p, dp.data(), N * N * 16, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(h->d_dminus.p, dm.data(), N * N * 16, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(h->d_time.p, &h->time, 8, cudaMemcpyHostToDevice));
+    h->field_on = true;
+    return upload_hamiltonian(h); // complex kernel variant; drops the step graph
+}
+
+int heom_clear_field(heom_handle* h)
+{
+    if (!h) return fail(HEOM_E_ARG, "NULL handle");
+    CUDA_TRY(cudaSetDevice(h->device));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    h->field_on = false;
+    return upload_hamiltonian(h);
+}
+
+int heom_set_time(heom_handle* h, double time)
+{
+    if (!h || !std::isfinite(time)) return fail(HEOM_E_ARG, "bad argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    h->time = time;
+    if (h->d_time.p) CUDA_TRY(cudaMemcpy(h->d_time.p, &h->time, 8, cudaMemcpyHostToDevice));
+    return 0;
+}
+
+double heom_time(const heom_handle* h) { return h ? h->time : 0.0; }
+
 int heom_get_mask(const heom_handle* h, uint8_t* mask)
 {
     if (!h || !mask) return fail(HEOM_E_ARG, "NULL argument");
@@ -1274,28 +1415,40 @@ int heom_buffer_read(heom_handle* h, const heom_buffer* b, double* host)
     return from_internal(h, host, b->data.p);
 }
 
-int heom_solve(heom_handle* h, double, double, const heom_buffer* in, heom_buffer* out,
+int heom_solve(heom_handle* h, double time, double step_size, const heom_buffer* in, heom_buffer* out,
                double out_coeff, heom_buffer* acc, double acc_coeff, int acc_init, int mode)
 {
     if (!h || !in || in->owner != h) return fail(HEOM_E_ARG, "bad input buffer");
     CUDA_TRY(cudaSetDevice(h->device));
     int rc = 0;
+    // pre-evaluate action (ode.cpp:99, e_field.hpp:69): H at time + step_size
+    AdjTabs ft;
+    const AdjTabs* tabs = nullptr;
+    if (h->field_on) {
+        heomk::FieldParams f = field_params(h, 1);
+        f.t0 = time + step_size;
+        heomk::heom_field_tables<<<1, 256, 0, h->stream>>>(f);
+        h->launches++;
+        CUDA_TRY(cudaGetLastError());
+        ft = field_tabs(h, 0);
+        tabs = &ft;
+    }
     switch (mode) {
     case HEOM_SOLVE_PURE:
         if (!out || out->owner != h || out == in) return fail(HEOM_E_ARG, "bad output buffer");
         rc = launch_stage(h, EPI_PURE, in->data.p, nullptr, out->data.p, nullptr,
-                          make_double2(0.0, 0.0), 0);
+                          make_double2(0.0, 0.0), 0, tabs);
         break;
     case HEOM_SOLVE_ACCUMULATE:
         if (!out || out->owner != h || out == in || !acc || acc->owner != h || acc == in || acc == out)
             return fail(HEOM_E_ARG, "bad output/accumulation buffer");
         rc = launch_stage(h, EPI_ACC, in->data.p, nullptr, out->data.p, acc->data.p,
-                          make_double2(acc_coeff, 0.0), acc_init ? 1 : 0);
+                          make_double2(acc_coeff, 0.0), acc_init ? 1 : 0, tabs);
         break;
     case HEOM_SOLVE_SUBDIAGONAL:
         if (!acc || acc->owner != h || acc == in) return fail(HEOM_E_ARG, "bad accumulation buffer");
         rc = launch_stage(h, EPI_AXPY_SELF, in->data.p, nullptr, acc->data.p, nullptr,
-                          make_double2(out_coeff, 0.0), 0);
+                          make_double2(out_coeff, 0.0), 0, tabs);
         break;
     default: return fail(HEOM_E_ARG, "unknown solve mode %d", mode);
     }

@@ -47,7 +47,7 @@ EXPORTS = [
     "heom_adjoint_create", "heom_adjoint_destroy", "heom_adjoint_handle", "heom_adjoint_gradient",
     "heom_adjoint_kernel_launches", "heom_bath_derivatives", "heom_adjoint_create_batch",
     "heom_adjoint_instances", "heom_set_mask_compact", "heom_active_matrices", "heom_get_mask",
-    "heom_hierarchy_norm",
+    "heom_hierarchy_norm", "heom_set_field", "heom_clear_field", "heom_set_time", "heom_time",
 ]
 
 
@@ -70,6 +70,11 @@ class SystemDesc(C.Structure):
                 ("baths", C.c_int32), ("baths_max_per_site", C.c_int32),
                 ("baths_coupling", C.c_void_p), ("lambda_", C.c_void_p), ("invnu", C.c_void_p),
                 ("omega", C.c_void_p), ("matsubaras", C.c_int32), ("temperature", C.c_double)]
+
+
+class Pulse(C.Structure):
+    _fields_ = [("efield", C.c_double), ("time_center", C.c_double), ("time_width", C.c_double),
+                ("frequency", C.c_double), ("phase", C.c_double)]
 
 
 class Options(C.Structure):
@@ -99,6 +104,11 @@ def lib():
         L.heom_active_matrices.argtypes = [vp]
         L.heom_get_mask.argtypes = [vp, vp]
         L.heom_hierarchy_norm.argtypes = [vp, dbl, vp]
+        L.heom_set_field.argtypes = [vp, vp, vp, C.POINTER(Pulse), C.POINTER(Pulse)]
+        L.heom_clear_field.argtypes = [vp]
+        L.heom_set_time.argtypes = [vp, dbl]
+        L.heom_time.restype = dbl
+        L.heom_time.argtypes = [vp]
         L.heom_buffer_create.argtypes = [vp, C.POINTER(vp)]
         L.heom_buffer_destroy.argtypes = [vp]
         L.heom_buffer_write.argtypes = [vp, vp, vp]
@@ -365,6 +375,24 @@ class Heom:
         m = np.zeros(self.matrices, np.uint8)
         _check(lib().heom_get_mask(self.h, _ptr(m)))
         return m
+
+    def set_field(self, dipole_plus, dipole_minus, pump, probe):
+        """Time-dependent H(t) = H - E(t) D- - conj(E(t)) D+ (SI; pump/probe:
+        dicts or tuples of efield, time_center, time_width, frequency, phase)."""
+        n = self.states
+        dp = np.ascontiguousarray(np.asarray(dipole_plus, np.complex128).reshape(n, n)).view(np.float64)
+        dm = np.ascontiguousarray(np.asarray(dipole_minus, np.complex128).reshape(n, n)).view(np.float64)
+        mk = lambda x: Pulse(**x) if isinstance(x, dict) else Pulse(*x)
+        _check(lib().heom_set_field(self.h, _ptr(dp), _ptr(dm), C.byref(mk(pump)), C.byref(mk(probe))))
+
+    def clear_field(self):
+        _check(lib().heom_clear_field(self.h))
+
+    def set_time(self, t):
+        _check(lib().heom_set_time(self.h, t))
+
+    def time(self):
+        return lib().heom_time(self.h)
 
     def hierarchy_norm(self, threshold=-1.0):
         """Per-ADO sum |sigma_ij|^2 (uid order); threshold >= 0 also filters the mask."""

@@ -143,6 +143,30 @@ int heom_set_mask(heom_handle* h, const uint8_t* mask);
  * entries of the state keep the values they had.  The top ADO of every
  * instance must be active.  heom_set_mask returns to the uncompacted mode. */
 int heom_set_mask_compact(heom_handle* h, const uint8_t* mask);
+/* Time-dependent Hamiltonian: the e_field pre-evaluate action of the
+ * reference (ode::add_pre_evaluate_action, ode.hpp:57-59; e_field.hpp:63-85).
+ * While a field is set, every derivative evaluation at time t uses
+ *     H(t) = H - E(t) D- - conj(E(t)) D+,
+ *     E(t) = sum over the pump and the probe pulse of
+ *            efield exp(-(t - time_center)^2 / (2 time_width^2)) exp(i (phase + frequency t)),
+ * built on the device before each evaluation (heom_solve: at time + step_size,
+ * as the reference's action; the stepping calls: at t, t + dt/2, t + dt of
+ * every step, which is then the classical RK4 whatever the handle's scheme).
+ * SI units: times in s, frequency in rad/s, the dipole matrices
+ * (states*states complex, interleaved) in J per unit field.  The propagation
+ * state carries its time (heom_set_time; advanced by every step). */
+typedef struct heom_pulse {
+    double efield;
+    double time_center;
+    double time_width;
+    double frequency;
+    double phase;
+} heom_pulse;
+int heom_set_field(heom_handle* h, const double* dipole_plus, const double* dipole_minus, const heom_pulse* pump,
+                   const heom_pulse* probe);
+int heom_clear_field(heom_handle* h);
+int heom_set_time(heom_handle* h, double time);
+double heom_time(const heom_handle* h);
 /* ADOs the stage kernels sweep (heom_matrices without compaction). */
 int64_t heom_active_matrices(const heom_handle* h);
 /* The current mask (reference uid order, all instances). */
