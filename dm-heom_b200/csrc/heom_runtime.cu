@@ -175,6 +175,11 @@ struct AdjTabs {
     const double* hr;      // -H (real symmetric H)
     const double2* hs;     // -H^H
     bool adjoint = true;
+    // optional bath-coefficient tables (flow tracking: a zero table switches a term off)
+    const double* chat = nullptr;   // DMMA kernel
+    const double2* khat = nullptr;
+    const double* cplus = nullptr;  // SIMT kernel
+    const double2* kmin = nullptr;
 };
 
 // stage write modes (runtime parameters of the one stage kernel)
@@ -280,6 +285,12 @@ struct heom_handle {
     DevBuf<double> field_hr, field_frag;   // [3][K][N*(N+1)], [3][K][256]
     DevBuf<double> d_time;                 // time of the propagation state (device, advanced by field steps)
     double time = 0.0;                     // host mirror
+
+    // flow tracking (heom_set_flow_buffers): acc_coeff x the plus / minus terms of every heom_solve
+    heom_buffer* flow_above = nullptr;
+    heom_buffer* flow_below = nullptr;
+    DevBuf<double2> flow_scratch;
+    DevBuf<double> d_zero;                 // zeros, as long as the longest table they replace
 
     // cached graph of one RK4 step
     cudaGraphExec_t step_graph = nullptr;
@@ -589,6 +600,8 @@ int launch_stage(heom_handle* h, int epi, const double2* in, const double2* y, d
         p.hfrag = adj->hfrag;
         p.hr = adj->hr;
         p.hs = adj->hs;
+        if (adj->cplus) p.cplus = adj->cplus;
+        if (adj->kmin) p.kmin = adj->kmin;
     }
     p.in = in;
     p.out = out;
@@ -628,8 +641,8 @@ int launch_stage(heom_handle* h, int epi, const double2* in, const double2* y, d
         heomk::DmmaParams dp;
         dp.p = p;
         dp.lt = h->lane_tab;
-        dp.ct.chat = h->d_chat.p;
-        dp.ct.khat = h->d_khat.p;
+        dp.ct.chat = adj && adj->chat ? adj->chat : h->d_chat.p;
+        dp.ct.khat = adj && adj->khat ? adj->khat : h->d_khat.p;
         dp.ct.sq = h->d_sq.p;
         dp.ct.pos = h->d_pos.p;
         dp.err = h->d_err.p;
@@ -1397,6 +1410,8 @@ int heom_buffer_destroy(heom_buffer* b)
     if (!b) return 0;
     if (b->borrowed) return fail(HEOM_E_ARG, "cannot destroy a borrowed buffer view");
     cudaSetDevice(b->owner->device);
+    if (b->owner->flow_above == b) b->owner->flow_above = nullptr;
+    if (b->owner->flow_below == b) b->owner->flow_below = nullptr;
     delete b;
     return 0;
 }
@@ -1453,8 +1468,61 @@ int heom_solve(heom_handle* h, double time, double step_size, const heom_buffer*
     default: return fail(HEOM_E_ARG, "unknown solve mode %d", mode);
     }
     if (rc) return rc;
+    if (h->flow_above || h->flow_below) {
+        // heom_ode.cl:436-441: flow_from_above += acc_coeff * plus term, flow_from_below += acc_coeff * minus
+        // term; each term alone is L with H, the same term and the other term's coefficients zeroed
+        const double2* z2 = reinterpret_cast<const double2*>(h->d_zero.p);
+        const double* z1 = h->d_zero.p;
+        for (int part = 0; part < 2; ++part) {
+            heom_buffer* dst = part == 0 ? h->flow_above : h->flow_below;
+            if (!dst) continue;
+            AdjTabs t;
+            t.pss = z2;
+            t.gamma0 = z2;
+            t.hfrag = z1;
+            t.hr = z1;
+            t.hs = z2;
+            t.adjoint = false;
+            if (part == 0) {
+                t.khat = z2;
+                t.kmin = z2;
+            } else {
+                t.chat = z1;
+                t.cplus = z1;
+            }
+            if (tabs) { // keep the time-dependent H out of the bath terms too
+                t.hfrag = z1;
+                t.hr = z1;
+                t.hs = z2;
+            }
+            rc = launch_stage(h, EPI_ACC, in->data.p, nullptr, h->flow_scratch.p, dst->data.p,
+                              make_double2(acc_coeff, 0.0), 0, &t);
+            if (rc) return rc;
+        }
+    }
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     return check_kernel_error(h);
+}
+
+int heom_set_flow_buffers(heom_handle* h, heom_buffer* flow_from_above, heom_buffer* flow_from_below)
+{
+    if (!h) return fail(HEOM_E_ARG, "NULL handle");
+    if ((flow_from_above && flow_from_above->owner != h) || (flow_from_below && flow_from_below->owner != h))
+        return fail(HEOM_E_ARG, "flow buffers must belong to the handle");
+    if (flow_from_above && flow_from_above == flow_from_below)
+        return fail(HEOM_E_ARG, "the two flow buffers must differ");
+    CUDA_TRY(cudaSetDevice(h->device));
+    if ((flow_from_above || flow_from_below) && !h->d_zero.p) {
+        const size_t K = h->n_inst, N = h->N;
+        size_t len = std::max<size_t>({K * 256, K * N * (N + 1), 2 * K * N * N, (size_t)6 * h->W * h->LS,
+                                       (size_t)6 * h->W, (size_t)2 * h->nodes});
+        if (int rc = h->d_zero.alloc(len)) return rc;
+        CUDA_TRY(cudaMemset(h->d_zero.p, 0, len * 8));
+        if (int rc = h->flow_scratch.alloc(h->state_elems())) return rc;
+    }
+    h->flow_above = flow_from_above;
+    h->flow_below = flow_from_below;
+    return 0;
 }
 
 int heom_weighted_add(heom_handle* h, int n, double step, heom_buffer* out, const heom_buffer* y,

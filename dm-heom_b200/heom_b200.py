@@ -48,6 +48,7 @@ EXPORTS = [
     "heom_adjoint_kernel_launches", "heom_bath_derivatives", "heom_adjoint_create_batch",
     "heom_adjoint_instances", "heom_set_mask_compact", "heom_active_matrices", "heom_get_mask",
     "heom_hierarchy_norm", "heom_set_field", "heom_clear_field", "heom_set_time", "heom_time",
+    "heom_set_flow_buffers",
 ]
 
 
@@ -107,6 +108,7 @@ def lib():
         L.heom_set_field.argtypes = [vp, vp, vp, C.POINTER(Pulse), C.POINTER(Pulse)]
         L.heom_clear_field.argtypes = [vp]
         L.heom_set_time.argtypes = [vp, dbl]
+        L.heom_set_flow_buffers.argtypes = [vp, vp, vp]
         L.heom_time.restype = dbl
         L.heom_time.argtypes = [vp]
         L.heom_buffer_create.argtypes = [vp, C.POINTER(vp)]
@@ -443,6 +445,9 @@ class Heom:
               acc: Buffer | None = None, acc_coeff=1.0, acc_init=False, time=0.0, step_size=0.0):
         _check(lib().heom_solve(self.h, time, step_size, inb.h, out.h if out else None, out_coeff,
                                 acc.h if acc else None, acc_coeff, int(acc_init), mode))
+
+    def set_flow_buffers(self, above: Buffer | None, below: Buffer | None):
+        _check(lib().heom_set_flow_buffers(self.h, above.h if above else None, below.h if below else None))
 
     def weighted_add(self, step, out: Buffer, y: Buffer, coeffs, ks):
         c = np.ascontiguousarray(np.asarray(coeffs, np.float64))

@@ -191,6 +191,14 @@ size_t heom_buffer_size_byte(const heom_handle* h);
 int heom_solve(heom_handle* h, double time, double step_size, const heom_buffer* in,
                heom_buffer* out, double out_coeff, heom_buffer* acc, double acc_coeff,
                int acc_init, int mode);
+/* ode::set_flow_buffers (ode.cpp:213-219): while set, every heom_solve adds
+ * acc_coeff times the plus term of the derivative to flow_from_above and
+ * acc_coeff times the minus term to flow_from_below (heom_ode.cl:436-441,
+ * element by element, reference layout in the buffers).  NULL buffers switch
+ * tracking off.  (The reference kernel tests NOMA_NUM_ODE_TRACK_FLOWS while its
+ * solver defines HEOM_ODE_TRACK_FLOWS; this build tracks whenever the buffers
+ * are set.) */
+int heom_set_flow_buffers(heom_handle* h, heom_buffer* flow_from_above, heom_buffer* flow_from_below);
 /* out = y + step_size * sum_l coeffs[l] * k[l] (0 <= n <= 7), terms with a zero
  * coefficient skipped, in rk_weighted_add's operation order. */
 int heom_weighted_add(heom_handle* h, int n, double step_size, heom_buffer* out,

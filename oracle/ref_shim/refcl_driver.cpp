@@ -32,6 +32,8 @@ typedef unsigned char mask_t;
 void refcl_heom_ode_pure(REFCL_ODE_ARGS);
 void refcl_heom_ode_acc(REFCL_ODE_ARGS);
 void refcl_heom_ode_subdiag(REFCL_ODE_ARGS);
+void refcl_heom_ode_noplus(REFCL_ODE_ARGS);
+void refcl_heom_ode_nominus(REFCL_ODE_ARGS);
 void refcl_rk_weighted_add(const int n, const double h, double* __restrict out,
                            const double* __restrict y_n, double c1, const double* __restrict k1,
                            double c2, const double* __restrict k2, double c3,
@@ -41,7 +43,8 @@ void refcl_rk_weighted_add(const int n, const double h, double* __restrict out,
 
 extern "C" {
 
-/* mode: 0 = pure evaluation, 1 = NOMA_NUM_ODE_ACCUMULATE, 2 = NOMA_NUM_ODE_SUBDIAGONAL */
+/* mode: 0 = pure evaluation, 1 = NOMA_NUM_ODE_ACCUMULATE, 2 = NOMA_NUM_ODE_SUBDIAGONAL,
+ * 3 = pure evaluation with HEOM_ODE_DISABLE_PLUS, 4 = pure evaluation with HEOM_ODE_DISABLE_MINUS */
 int refcl_heom_ode(int mode, int states, int matsubaras, int baths_per_state, int ado_width,
                    int64_t nodes, int first_non_plus_id, const int* coupling,
                    double step_size, double* out, double out_coeff, double* acc,
@@ -58,7 +61,8 @@ int refcl_heom_ode(int mode, int states, int matsubaras, int baths_per_state, in
     refcl_ado_width = ado_width;
     std::memcpy(refcl_baths_coupling_storage, coupling, sizeof(int) * states * baths_per_state);
     typedef void (*fn_t)(REFCL_ODE_ARGS);
-    fn_t fn = mode == 0 ? refcl_heom_ode_pure : mode == 1 ? refcl_heom_ode_acc : refcl_heom_ode_subdiag;
+    fn_t fn = mode == 0 ? refcl_heom_ode_pure : mode == 1 ? refcl_heom_ode_acc : mode == 2 ? refcl_heom_ode_subdiag
+            : mode == 3 ? refcl_heom_ode_noplus : refcl_heom_ode_nominus;
 #pragma omp parallel for num_threads(threads) schedule(static)
     for (int64_t u = 0; u < nodes; ++u) {
         refcl_gid = (std::size_t)u;

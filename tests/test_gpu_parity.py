@@ -246,3 +246,30 @@ def test_compaction_switches_back_and_keeps_the_state():
         H.set_mask(mask)
         assert H.active_matrices() == mask.size
         assert np.array_equal(H.get_state(), y)
+
+
+@pytest.mark.parametrize("case", ["complex_m2", "n12_m1", "cfg1_real_m1"])
+def test_flow_buffers_match_reference_kernel_terms(case):
+    """heom_set_flow_buffers: each heom_solve adds acc_coeff x the plus term and
+    acc_coeff x the minus term (heom_ode.cl:436-441); the terms are taken from
+    the reference's own kernel built with HEOM_ODE_DISABLE_PLUS / _MINUS."""
+    prob = CASES[case]()
+    y = np.random.default_rng(4).normal(size=prob.state_len)
+    full, _ = ho.ref_derivative(prob, y)
+    plus = full - ho.ref_derivative(prob, y, mode=3)[0]
+    minus = full - ho.ref_derivative(prob, y, mode=4)[0]
+    with hb.Heom.from_problem(prob) as H:
+        bi, bo, fa, fb = H.buffer(), H.buffer(), H.buffer(), H.buffer()
+        bi.write(y)
+        H.set_flow_buffers(fa, fb)
+        H.solve(bi, bo, hb.SOLVE_PURE, acc_coeff=0.7)
+        H.solve(bi, bo, hb.SOLVE_PURE, acc_coeff=0.3)
+        above, below, out = fa.read(), fb.read(), bo.read()
+        H.set_flow_buffers(None, None)
+        H.solve(bi, bo, hb.SOLVE_PURE, acc_coeff=5.0)
+        assert np.array_equal(fa.read(), above)  # tracking off
+        for b in (bi, bo, fa, fb):
+            b.close()
+    assert rel_err(out, full) <= DERIV_TOL
+    assert np.max(np.abs(above - plus)) <= 1e-12 * np.max(np.abs(plus))
+    assert np.max(np.abs(below - minus)) <= 1e-12 * np.max(np.abs(minus))
