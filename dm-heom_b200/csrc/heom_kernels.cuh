@@ -1204,6 +1204,75 @@ __global__ void heom_field_tables(const FieldParams f)
     if (f.time && threadIdx.x == 0) *f.time = t0 + f.dt;
 }
 
+// ---------------------------------------------------------------------------
+// Hierarchy arithmetic (hierarchy_arithmetic_{add,subtract,scale,dot_product,
+// mmult_left,mmult_right}.cl) on whole state buffers in the pair layout, in
+// the reference's operation order (complex products as a.x*b.x - a.y*b.y,
+// sums in k order, no contraction).  out may alias a or b.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double2 cmul_rn(double2 a, double2 b)
+{
+    return make_double2(__dsub_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)),
+                        __dadd_rn(__dmul_rn(a.x, b.y), __dmul_rn(a.y, b.x)));
+}
+
+// op 0: a + b, 1: a - b, 2: a * conj(b), 3: f * a
+__global__ void heom_hier_elementwise(double2* out, const double2* a, const double2* b, double2 f, int64_t len, int op)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += stride) {
+        const double2 x = a[e];
+        double2 r;
+        if (op == 0) {
+            const double2 y = b[e];
+            r = make_double2(__dadd_rn(x.x, y.x), __dadd_rn(x.y, y.y));
+        } else if (op == 1) {
+            const double2 y = b[e];
+            r = make_double2(__dsub_rn(x.x, y.x), __dsub_rn(x.y, y.y));
+        } else if (op == 2) {
+            const double2 y = b[e];
+            r = cmul_rn(x, make_double2(y.x, -y.y));
+        } else {
+            r = cmul_rn(f, x);
+        }
+        out[e] = r;
+    }
+}
+
+// every ADO: out_u = M a_u (left) or a_u M (right); one warp per ADO, the
+// tile staged in shared memory ([warp][N*N] double2)
+__global__ void heom_hier_mmult(double2* out, const double2* a, const double2* __restrict__ m,
+                                const int16_t* __restrict__ pe, int64_t nodes, int n, int P, int left)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, NN = n * n;
+    double2* t = reinterpret_cast<double2*>(smem) + warp * 2 * NN;
+    double2* r = t + NN;
+    const int64_t stride = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t u = (int64_t)blockIdx.x * (blockDim.x >> 5) + warp; u < nodes; u += stride) {
+        for (int pr = lane; pr < P; pr += 32) {
+            t[pe[2 * pr]] = a[(u * P + pr) * 2];
+            t[pe[2 * pr + 1]] = a[(u * P + pr) * 2 + 1];
+        }
+        __syncwarp();
+        for (int q = lane; q < NN; q += 32) {
+            const int i = q / n, j = q - i * n;
+            double2 v = make_double2(0.0, 0.0);
+            for (int k = 0; k < n; ++k) {
+                const double2 p = left ? cmul_rn(m[i * n + k], t[k * n + j]) : cmul_rn(t[i * n + k], m[k * n + j]);
+                v = make_double2(__dadd_rn(v.x, p.x), __dadd_rn(v.y, p.y));
+            }
+            r[q] = v;
+        }
+        __syncwarp();
+        for (int pr = lane; pr < P; pr += 32) {
+            out[(u * P + pr) * 2] = r[pe[2 * pr]];
+            out[(u * P + pr) * 2 + 1] = r[pe[2 * pr + 1]];
+        }
+        __syncwarp();
+    }
+}
+
 // Frobenius norm squared of every ADO, sum |sigma(i,j)|^2 (hierarchy_norm.cl:15-45),
 // written at the ADO's reference index.  One warp per ADO; a padding half of
 // an odd diagonal pair counts once.

@@ -286,6 +286,9 @@ struct heom_handle {
     DevBuf<double> d_time;                 // time of the propagation state (device, advanced by field steps)
     double time = 0.0;                     // host mirror
 
+    // host pre-evaluate actions (ode::add_pre_evaluate_action), run before every heom_solve
+    std::vector<std::pair<heom_pre_evaluate_fn, void*>> actions;
+
     // flow tracking (heom_set_flow_buffers): acc_coeff x the plus / minus terms of every heom_solve
     heom_buffer* flow_above = nullptr;
     heom_buffer* flow_below = nullptr;
@@ -811,6 +814,9 @@ int launches_per_step(const heom_handle* h)
 int run_steps(heom_handle* h, double dt, int64_t steps)
 {
     if (steps <= 0) return 0;
+    if (!h->actions.empty())
+        return fail(HEOM_E_UNSUPPORTED, "host pre-evaluate actions run with heom_solve only; the stepping calls take "
+                                        "a device-side time dependence (heom_set_field)");
     if (int rc = prepare_scheme(h)) return rc;
     h->time += (double)steps * dt; // host mirror of the state's time (the device copy moves with field steps)
     if (!h->opt.use_graphs) {
@@ -1107,6 +1113,48 @@ int check_kernel_error(heom_handle* h)
     return 0;
 }
 
+int hier_check(const heom_handle* h, const heom_buffer* a, const heom_buffer* b, const heom_buffer* out)
+{
+    if (!h || !a || !out || a->owner != h || out->owner != h || (b && b->owner != h))
+        return fail(HEOM_E_ARG, "buffers must belong to the handle");
+    return 0;
+}
+
+int hier_elementwise(heom_handle* h, const heom_buffer* a, const heom_buffer* b, heom_buffer* out, double2 f, int op)
+{
+    if (int rc = hier_check(h, a, b, out)) return rc;
+    if (op != 3 && !b) return fail(HEOM_E_ARG, "NULL buffer");
+    CUDA_TRY(cudaSetDevice(h->device));
+    const int64_t len = (int64_t)h->state_elems();
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((len + 255) / 256, (int64_t)h->sm_count * 8));
+    heomk::heom_hier_elementwise<<<blocks, 256, 0, h->stream>>>(out->data.p, a->data.p, b ? b->data.p : a->data.p, f,
+                                                                len, op);
+    h->launches++;
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int hier_mmult(heom_handle* h, const heom_buffer* a, const double* m, heom_buffer* out, int left)
+{
+    if (int rc = hier_check(h, a, nullptr, out)) return rc;
+    if (!m) return fail(HEOM_E_ARG, "NULL matrix");
+    CUDA_TRY(cudaSetDevice(h->device));
+    const int NN = h->N * h->N;
+    DevBuf<double2> dm;
+    if (int rc = dm.alloc(NN)) return rc;
+    CUDA_TRY(cudaMemcpyAsync(dm.p, m, NN * 16, cudaMemcpyHostToDevice, h->stream));
+    const size_t smem = (size_t)8 * 2 * NN * 16;
+    if (int rc = allow_dynamic_smem((const void*)heomk::heom_hier_mmult, smem)) return rc;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((h->nodes + 7) / 8, (int64_t)h->sm_count * 8));
+    heomk::heom_hier_mmult<<<blocks, 256, smem, h->stream>>>(out->data.p, a->data.p, dm.p, h->d_pair.p, h->nodes, h->N,
+                                                             h->P, left);
+    h->launches++;
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
 } // namespace
 
 extern "C" {
@@ -1356,6 +1404,45 @@ int heom_set_time(heom_handle* h, double time)
 
 double heom_time(const heom_handle* h) { return h ? h->time : 0.0; }
 
+int heom_hierarchy_add(heom_handle* h, const heom_buffer* a, const heom_buffer* b, heom_buffer* out)
+{
+    return hier_elementwise(h, a, b, out, make_double2(0.0, 0.0), 0);
+}
+int heom_hierarchy_subtract(heom_handle* h, const heom_buffer* a, const heom_buffer* b, heom_buffer* out)
+{
+    return hier_elementwise(h, a, b, out, make_double2(0.0, 0.0), 1);
+}
+int heom_hierarchy_dot_product(heom_handle* h, const heom_buffer* a, const heom_buffer* b, heom_buffer* out)
+{
+    return hier_elementwise(h, a, b, out, make_double2(0.0, 0.0), 2);
+}
+int heom_hierarchy_scale(heom_handle* h, const heom_buffer* a, double re, double im, heom_buffer* out)
+{
+    return hier_elementwise(h, a, nullptr, out, make_double2(re, im), 3);
+}
+int heom_hierarchy_mmult_left(heom_handle* h, const heom_buffer* a, const double* m, heom_buffer* out)
+{
+    return hier_mmult(h, a, m, out, 1);
+}
+int heom_hierarchy_mmult_right(heom_handle* h, const heom_buffer* a, const double* m, heom_buffer* out)
+{
+    return hier_mmult(h, a, m, out, 0);
+}
+
+int heom_add_pre_evaluate_action(heom_handle* h, heom_pre_evaluate_fn fn, void* user)
+{
+    if (!h || !fn) return fail(HEOM_E_ARG, "NULL argument");
+    h->actions.push_back({fn, user});
+    return 0;
+}
+
+int heom_clear_pre_evaluate_actions(heom_handle* h)
+{
+    if (!h) return fail(HEOM_E_ARG, "NULL handle");
+    h->actions.clear();
+    return 0;
+}
+
 int heom_get_mask(const heom_handle* h, uint8_t* mask)
 {
     if (!h || !mask) return fail(HEOM_E_ARG, "NULL argument");
@@ -1436,7 +1523,11 @@ int heom_solve(heom_handle* h, double time, double step_size, const heom_buffer*
     if (!h || !in || in->owner != h) return fail(HEOM_E_ARG, "bad input buffer");
     CUDA_TRY(cudaSetDevice(h->device));
     int rc = 0;
-    // pre-evaluate action (ode.cpp:99, e_field.hpp:69): H at time + step_size
+    // host pre-evaluate actions in registration order (ode.cpp:17-22)
+    for (auto& a : h->actions)
+        if (int arc = a.first(a.second, h, time, step_size, in, out))
+            return fail(arc < 0 ? arc : HEOM_E_ARG, "pre-evaluate action returned %d", arc);
+    // device field (ode.cpp:99, e_field.hpp:69): H at time + step_size
     AdjTabs ft;
     const AdjTabs* tabs = nullptr;
     if (h->field_on) {

@@ -48,8 +48,12 @@ EXPORTS = [
     "heom_adjoint_kernel_launches", "heom_bath_derivatives", "heom_adjoint_create_batch",
     "heom_adjoint_instances", "heom_set_mask_compact", "heom_active_matrices", "heom_get_mask",
     "heom_hierarchy_norm", "heom_set_field", "heom_clear_field", "heom_set_time", "heom_time",
-    "heom_set_flow_buffers",
+    "heom_set_flow_buffers", "heom_add_pre_evaluate_action", "heom_clear_pre_evaluate_actions",
+    "heom_hierarchy_add", "heom_hierarchy_subtract", "heom_hierarchy_dot_product", "heom_hierarchy_scale",
+    "heom_hierarchy_mmult_left", "heom_hierarchy_mmult_right",
 ]
+
+PRE_EVALUATE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_void_p)
 
 
 class HeomError(RuntimeError):
@@ -109,6 +113,13 @@ def lib():
         L.heom_clear_field.argtypes = [vp]
         L.heom_set_time.argtypes = [vp, dbl]
         L.heom_set_flow_buffers.argtypes = [vp, vp, vp]
+        L.heom_add_pre_evaluate_action.argtypes = [vp, PRE_EVALUATE_FN, vp]
+        L.heom_clear_pre_evaluate_actions.argtypes = [vp]
+        for name in ["heom_hierarchy_add", "heom_hierarchy_subtract", "heom_hierarchy_dot_product"]:
+            getattr(L, name).argtypes = [vp, vp, vp, vp]
+        L.heom_hierarchy_scale.argtypes = [vp, vp, dbl, dbl, vp]
+        L.heom_hierarchy_mmult_left.argtypes = [vp, vp, vp, vp]
+        L.heom_hierarchy_mmult_right.argtypes = [vp, vp, vp, vp]
         L.heom_time.restype = dbl
         L.heom_time.argtypes = [vp]
         L.heom_buffer_create.argtypes = [vp, C.POINTER(vp)]
@@ -445,6 +456,28 @@ class Heom:
               acc: Buffer | None = None, acc_coeff=1.0, acc_init=False, time=0.0, step_size=0.0):
         _check(lib().heom_solve(self.h, time, step_size, inb.h, out.h if out else None, out_coeff,
                                 acc.h if acc else None, acc_coeff, int(acc_init), mode))
+
+    def add_pre_evaluate_action(self, fn):
+        """fn(handle, time, step_size) before every solve(); return 0 to continue."""
+        cb = PRE_EVALUATE_FN(lambda user, h, t, dt, i, o: int(fn(self, t, dt) or 0))
+        self._actions = getattr(self, "_actions", []) + [cb]  # keep the callbacks alive
+        _check(lib().heom_add_pre_evaluate_action(self.h, cb, None))
+
+    def clear_pre_evaluate_actions(self):
+        _check(lib().heom_clear_pre_evaluate_actions(self.h))
+        self._actions = []
+
+    def hierarchy_op(self, op, a: Buffer, b: Buffer | None, out: Buffer, factor=1.0 + 0j, matrix=None):
+        """op: add | subtract | dot_product | scale | mmult_left | mmult_right."""
+        L = lib()
+        if op in ("add", "subtract", "dot_product"):
+            _check(getattr(L, "heom_hierarchy_" + op)(self.h, a.h, b.h, out.h))
+        elif op == "scale":
+            _check(L.heom_hierarchy_scale(self.h, a.h, float(np.real(factor)), float(np.imag(factor)), out.h))
+        else:
+            n = self.states
+            m = np.ascontiguousarray(np.asarray(matrix, np.complex128).reshape(n, n)).view(np.float64)
+            _check(getattr(L, "heom_hierarchy_" + op)(self.h, a.h, _ptr(m), out.h))
 
     def set_flow_buffers(self, above: Buffer | None, below: Buffer | None):
         _check(lib().heom_set_flow_buffers(self.h, above.h if above else None, below.h if below else None))

@@ -143,6 +143,29 @@ int heom_set_mask(heom_handle* h, const uint8_t* mask);
  * entries of the state keep the values they had.  The top ADO of every
  * instance must be active.  heom_set_mask returns to the uncompacted mode. */
 int heom_set_mask_compact(heom_handle* h, const uint8_t* mask);
+/* Host pre-evaluate actions (ode::add_pre_evaluate_action, ode.hpp:57-59,
+ * ode.cpp:17-22): fn(user, h, time, step_size, in, out) runs before every
+ * heom_solve, in registration order, and may change the handle (say
+ * heom_set_hamiltonian); a non-zero return aborts the solve with that code.
+ * The stepping calls refuse to run while host actions are registered (their
+ * stages never return to the host); heom_set_field is the device-side
+ * time dependence they take. */
+typedef int (*heom_pre_evaluate_fn)(void* user, heom_handle* h, double time, double step_size,
+                                    const heom_buffer* in, heom_buffer* out);
+int heom_add_pre_evaluate_action(heom_handle* h, heom_pre_evaluate_fn fn, void* user);
+int heom_clear_pre_evaluate_actions(heom_handle* h);
+
+/* Hierarchy arithmetic (hierarchy_arithmetic_*.cl) on whole buffers of the
+ * handle, in the reference's operation order; out may alias an input.
+ * dot_product writes the element products a * conj(b) (as the reference's
+ * kernel); m is a states*states complex matrix in host memory. */
+int heom_hierarchy_add(heom_handle* h, const heom_buffer* a, const heom_buffer* b, heom_buffer* out);
+int heom_hierarchy_subtract(heom_handle* h, const heom_buffer* a, const heom_buffer* b, heom_buffer* out);
+int heom_hierarchy_dot_product(heom_handle* h, const heom_buffer* a, const heom_buffer* b, heom_buffer* out);
+int heom_hierarchy_scale(heom_handle* h, const heom_buffer* a, double re, double im, heom_buffer* out);
+int heom_hierarchy_mmult_left(heom_handle* h, const heom_buffer* a, const double* m, heom_buffer* out);
+int heom_hierarchy_mmult_right(heom_handle* h, const heom_buffer* a, const double* m, heom_buffer* out);
+
 /* Time-dependent Hamiltonian: the e_field pre-evaluate action of the
  * reference (ode::add_pre_evaluate_action, ode.hpp:57-59; e_field.hpp:63-85).
  * While a field is set, every derivative evaluation at time t uses
