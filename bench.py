@@ -719,7 +719,7 @@ def main():
                 "e2e": e2e,
                 "gpu_launches": int(launches), "roofline": roofline, "clocks": clk}
         if world == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_reference_sample(steps_cap=1)
+            line["cpu_baseline"] = cpu_reference_sample(steps_cap=3)
         print(json.dumps(line), flush=True)
 
     H.close()
