@@ -1,5 +1,6 @@
 // host_capi.cpp -- C ABI of the host set-up (graph, tables, config, masks).
 #include <cstring>
+#include <fstream>
 #include <memory>
 
 #include "heom_host.hpp"
@@ -8,6 +9,8 @@ using namespace heomhost;
 
 struct heom_tables {
     instance inst;
+    std::vector<double> state; // hierarchy read from an instance file (empty: none)
+    double time = 0.0;
 };
 
 struct heom_config {
@@ -77,6 +80,153 @@ int heom_bath_derivatives(const heom_system_desc* sys, int32_t theta, double* d_
         if (d_cbk) std::memcpy(d_cbk, d.cbk[theta].data(), d.cbk[theta].size() * 8);
         return 0;
     });
+}
+
+// The reference's binary instance file (instance::write_file / read_file,
+// instance.cpp:281-377, format version 1): the fields one after another in
+// native layout, no padding -- int32 version, bool hierarchy_top_only, int32
+// hierarchy and hamiltonian layouts, the sites_to_states mode (an int), double
+// time, int32 first_non_plus_id, int64 states, matrices, matsubaras,
+// baths_per_state, baths, ado_width, ado_depth, then the hierarchy (all ADOs,
+// or the top only), H, tuples, plus, minus, pf_same_sum, pf_same, pf_circ,
+// cbk, cbk_sqrt.  The bath coupling is not in the file.
+} // extern "C"
+
+namespace {
+template <typename T>
+void put(std::ofstream& f, const T& v)
+{
+    f.write(reinterpret_cast<const char*>(&v), sizeof v);
+}
+template <typename T>
+void put_n(std::ofstream& f, const T* p, size_t n)
+{
+    f.write(reinterpret_cast<const char*>(p), n * sizeof(T));
+}
+template <typename T>
+void get(std::ifstream& f, T& v)
+{
+    f.read(reinterpret_cast<char*>(&v), sizeof v);
+}
+template <typename T>
+void get_n(std::ifstream& f, T* p, size_t n)
+{
+    f.read(reinterpret_cast<char*>(p), n * sizeof(T));
+}
+} // namespace
+
+extern "C" {
+
+int heom_instance_write(const heom_tables* t, const double* state, int32_t top_only, double time, const char* path)
+{
+    if (!t || !path) return set_error(HEOM_E_ARG, "NULL argument");
+    return guarded([&] {
+        const instance& in = t->inst;
+        std::ofstream f(path, std::ios::out | std::ios::binary | std::ios::trunc);
+        if (!f) throw config_error(std::string("could not open instance file for writing: ") + path);
+        const int64_t N = in.sys.states, nodes = in.matrices, W = in.width, B = in.sys.baths, M = in.sys.matsubaras;
+        put(f, int32_t(0));           // version V_1
+        put(f, bool(top_only != 0));  // hierarchy_top_only
+        put(f, int32_t(0));           // hierarchy layout VANILLA
+        put(f, int32_t(0));           // hamiltonian layout VANILLA
+        put(f, int(0));               // sites_to_states identity
+        put(f, time);
+        put(f, int32_t(in.first_non_plus));
+        for (int64_t v : {N, nodes, M, (int64_t)in.sys.baths_per_state, B, W, (int64_t)in.sys.depth}) put(f, v);
+        const size_t hsz = (size_t)(top_only ? 1 : nodes) * N * N * 2;
+        std::vector<double> zero;
+        if (!state) zero.assign(hsz, 0.0);
+        put_n(f, state ? state : zero.data(), hsz);
+        put_n(f, in.hamiltonian.data(), (size_t)N * N * 2);
+        put_n(f, in.tuples.data(), (size_t)nodes * W);
+        put_n(f, in.plus.data(), (size_t)nodes * W);
+        put_n(f, in.minus.data(), (size_t)nodes * W);
+        put_n(f, in.pf_same_sum.data(), (size_t)nodes * 2);
+        put_n(f, in.pf_same.data(), (size_t)B * 2);
+        put_n(f, in.pf_circ.data(), (size_t)B * 2);
+        put_n(f, in.cbk.data(), (size_t)B * M * 2);
+        put_n(f, in.cbk_sqrt.data(), (size_t)B * M);
+        if (!f) throw config_error(std::string("writing the instance file failed: ") + path);
+        return 0;
+    });
+}
+
+int heom_instance_read(const char* path, const int32_t* coupling, heom_tables** out)
+{
+    if (!path || !out) return set_error(HEOM_E_ARG, "NULL argument");
+    *out = nullptr;
+    return guarded([&] {
+        std::ifstream f(path, std::ios::in | std::ios::binary);
+        if (!f) throw config_error(std::string("could not open instance file: ") + path);
+        int32_t version = -1, hl = 0, ml = 0, fnp = 0;
+        bool top_only = false;
+        int sts = 0;
+        double time = 0.0;
+        int64_t N = 0, nodes = 0, M = 0, bps = 0, B = 0, W = 0, D = 0;
+        get(f, version);
+        get(f, top_only);
+        get(f, hl);
+        get(f, ml);
+        get(f, sts);
+        get(f, time);
+        get(f, fnp);
+        for (int64_t* v : {&N, &nodes, &M, &bps, &B, &W, &D}) get(f, *v);
+        if (!f || version != 0) throw config_error("not an instance file of format version 1");
+        if (hl != 0 || ml != 0 || sts != 0) throw config_error("instance file: unsupported layout or sites_to_states mode");
+        if (N < 1 || N > 64 || nodes < 1 || nodes > INT32_MAX || M < 1 || B < 1 || bps < 1 || W != B * M || D < 1)
+            throw config_error("instance file: inconsistent sizes");
+        std::unique_ptr<heom_tables> t(new heom_tables());
+        instance& in = t->inst;
+        in.sys.states = (int32_t)N;
+        in.sys.depth = (int32_t)D;
+        in.sys.baths = (int32_t)B;
+        in.sys.baths_per_state = (int32_t)bps;
+        in.sys.matsubaras = (int32_t)M;
+        in.matrices = nodes;
+        in.width = (int32_t)W;
+        in.first_non_plus = fnp;
+        in.sys.coupling.resize((size_t)N * bps);
+        if (coupling) {
+            std::copy(coupling, coupling + N * bps, in.sys.coupling.begin());
+        } else {
+            if (bps != 1 || B != N) throw config_error("instance file: give the bath coupling (it is not in the file)");
+            for (int64_t i = 0; i < N; ++i) in.sys.coupling[i] = (int32_t)i;
+        }
+        const size_t hsz = (size_t)(top_only ? 1 : nodes) * N * N * 2;
+        t->state.assign((size_t)nodes * N * N * 2, 0.0);
+        get_n(f, t->state.data(), hsz);
+        in.hamiltonian.resize((size_t)N * N * 2);
+        get_n(f, in.hamiltonian.data(), in.hamiltonian.size());
+        in.tuples.resize((size_t)nodes * W);
+        in.plus.resize((size_t)nodes * W);
+        in.minus.resize((size_t)nodes * W);
+        get_n(f, in.tuples.data(), in.tuples.size());
+        get_n(f, in.plus.data(), in.plus.size());
+        get_n(f, in.minus.data(), in.minus.size());
+        in.pf_same_sum.resize((size_t)nodes * 2);
+        get_n(f, in.pf_same_sum.data(), in.pf_same_sum.size());
+        in.pf_same.resize((size_t)B * 2);
+        in.pf_circ.resize((size_t)B * 2);
+        in.cbk.resize((size_t)B * M * 2);
+        in.cbk_sqrt.resize((size_t)B * M);
+        get_n(f, in.pf_same.data(), in.pf_same.size());
+        get_n(f, in.pf_circ.data(), in.pf_circ.size());
+        get_n(f, in.cbk.data(), in.cbk.size());
+        get_n(f, in.cbk_sqrt.data(), in.cbk_sqrt.size());
+        if (!f) throw config_error("instance file is truncated");
+        t->time = time;
+        *out = t.release();
+        return 0;
+    });
+}
+
+int heom_tables_state(const heom_tables* t, double* state, double* time)
+{
+    if (!t || !state) return set_error(HEOM_E_ARG, "NULL argument");
+    if (t->state.empty()) return set_error(HEOM_E_ARG, "these tables were not read from an instance file");
+    std::copy(t->state.begin(), t->state.end(), state);
+    if (time) *time = t->time;
+    return 0;
 }
 
 int heom_tables_mask(const heom_tables* t, const char* strategy, int64_t first_layer, uint8_t* mask)

@@ -50,7 +50,8 @@ EXPORTS = [
     "heom_hierarchy_norm", "heom_set_field", "heom_clear_field", "heom_set_time", "heom_time",
     "heom_set_flow_buffers", "heom_add_pre_evaluate_action", "heom_clear_pre_evaluate_actions",
     "heom_hierarchy_add", "heom_hierarchy_subtract", "heom_hierarchy_dot_product", "heom_hierarchy_scale",
-    "heom_hierarchy_mmult_left", "heom_hierarchy_mmult_right",
+    "heom_hierarchy_mmult_left", "heom_hierarchy_mmult_right", "heom_instance_write", "heom_instance_read",
+    "heom_tables_state",
 ]
 
 PRE_EVALUATE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_void_p)
@@ -147,6 +148,9 @@ def lib():
         L.heom_tables_build.argtypes = [C.POINTER(SystemDesc), C.POINTER(vp)]
         L.heom_tables_view.argtypes = [vp, C.POINTER(InstanceDesc)]
         L.heom_tables_free.argtypes = [vp]
+        L.heom_instance_write.argtypes = [vp, vp, i32, dbl, C.c_char_p]
+        L.heom_instance_read.argtypes = [C.c_char_p, vp, C.POINTER(vp)]
+        L.heom_tables_state.argtypes = [vp, vp, C.POINTER(dbl)]
         L.heom_tables_free.restype = None
         L.heom_tables_mask.argtypes = [vp, C.c_char_p, i64, vp]
         L.heom_create_from_system.argtypes = [C.POINTER(SystemDesc), C.POINTER(Options), C.POINTER(vp)]
@@ -722,6 +726,56 @@ def trapezoid_weights(steps, dt_fs):
     w = np.full(steps + 1, float(dt_fs))
     w[0] = w[-1] = 0.5 * dt_fs
     return w
+
+
+def _tables_dict(t):
+    v = InstanceDesc()
+    _check(lib().heom_tables_view(t, C.byref(v)))
+    n, w, b, m, s = v.matrices, v.ado_width, v.baths, v.matsubaras, v.states
+
+    def get(ptr, count, ct, dt):
+        return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ct)), shape=(count,)).astype(dt).copy()
+
+    return dict(states=s, matsubaras=m, baths=b, baths_per_state=v.baths_per_state,
+                ado_width=w, ado_depth=v.ado_depth, matrices=n, first_non_plus_id=v.first_non_plus_id,
+                baths_coupling=get(v.baths_coupling, s * v.baths_per_state, C.c_int32, np.int32),
+                hamiltonian=get(v.hamiltonian, s * s * 2, C.c_double, np.float64),
+                ado_tuples=get(v.ado_tuples, n * w, C.c_int32, np.int32),
+                ado_plus=get(v.ado_plus, n * w, C.c_int32, np.int32),
+                ado_minus=get(v.ado_minus, n * w, C.c_int32, np.int32),
+                pf_same_sum=get(v.pf_same_sum, n * 2, C.c_double, np.float64),
+                pf_same=get(v.pf_same, b * 2, C.c_double, np.float64),
+                pf_circ=get(v.pf_circ, b * 2, C.c_double, np.float64),
+                cbk=get(v.cbk, b * m * 2, C.c_double, np.float64),
+                cbk_sqrt=get(v.cbk_sqrt, b * m, C.c_double, np.float64))
+
+
+def write_instance(system: System, path, state=None, top_only=False, time=0.0):
+    """The reference's binary instance file of a system (and a state)."""
+    t = C.c_void_p()
+    d = system.desc()
+    _check(lib().heom_tables_build(C.byref(d), C.byref(t)))
+    try:
+        st = None if state is None else np.ascontiguousarray(state, np.float64)
+        _check(lib().heom_instance_write(t, _ptr(st) if st is not None else None, int(top_only), time,
+                                         str(path).encode()))
+    finally:
+        lib().heom_tables_free(t)
+
+
+def read_instance(path, coupling=None):
+    """(tables dict, state, time) of a reference instance file."""
+    t = C.c_void_p()
+    cp = None if coupling is None else np.ascontiguousarray(np.asarray(coupling, np.int32).reshape(-1))
+    _check(lib().heom_instance_read(str(path).encode(), _ptr(cp) if cp is not None else None, C.byref(t)))
+    try:
+        tabs = _tables_dict(t)
+        state = np.empty(tabs["matrices"] * tabs["states"] ** 2 * 2)
+        tm = C.c_double()
+        _check(lib().heom_tables_state(t, _ptr(state), C.byref(tm)))
+        return tabs, state, tm.value
+    finally:
+        lib().heom_tables_free(t)
 
 
 def tables_mask(system: System, strategy="none", first_layer=-1):

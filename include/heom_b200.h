@@ -390,6 +390,15 @@ int heom_config_system(const heom_config* c, heom_system_desc* view);
 int heom_config_rho_init(const heom_config* c, double* out);
 /* Raw text of "section.key" copied into buf (NUL-terminated). */
 int heom_config_get(const heom_config* c, const char* key, char* buf, size_t len);
+/* The reference's binary instance file (instance::write_file / read_file,
+ * instance.cpp:281-377, format version 1, native byte order): the tables, H
+ * and a hierarchy state (NULL: zeros; top_only != 0 stores the top only) at
+ * time `time`.  The bath coupling is not part of the format: heom_instance_read
+ * takes it (states * baths_per_state, NULL for one bath per state), and
+ * heom_tables_state returns the state and time read. */
+int heom_instance_write(const heom_tables* t, const double* state, int32_t top_only, double time, const char* path);
+int heom_instance_read(const char* path, const int32_t* coupling, heom_tables** out);
+int heom_tables_state(const heom_tables* t, double* state, double* time);
 /* Mask of a filtering strategy ("none" or "single_excitation",
  * hierarchy_mask.cpp:20-110) for the hierarchy of the tables, written to
  * mask[matrices]. */

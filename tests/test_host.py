@@ -215,3 +215,37 @@ def test_bath_derivatives_match_central_differences(m, omega):
             fd = (tabs(lam, 1e15 / (g + d)) - tabs(lam, 1e15 / (g - d))) / (2 * d)
         scale = np.max(np.abs(ana))
         assert np.max(np.abs(ana - fd)) <= 1e-7 * scale, (theta, np.max(np.abs(ana - fd)) / scale)
+
+
+def test_instance_file_round_trip_and_byte_layout(tmp_path):
+    """heom_instance_write / read in the reference's binary layout
+    (instance.cpp:281-377): fields back to back, native order, no padding."""
+    import struct
+    sysd = hb.System(ho.synthetic_hamiltonian(3, 6), [35] * 3, [50] * 3, [0] * 3, 2, 300.0, 2)
+    t = hb.build_tables(sysd)
+    y = np.random.default_rng(0).normal(size=t["matrices"] * 9 * 2)
+    path = tmp_path / "inst.bin"
+    hb.write_instance(sysd, path, state=y, time=1.25e-13)
+    raw = path.read_bytes()
+    head = struct.pack("<i?iiidi7q", 0, False, 0, 0, 0, 1.25e-13, t["first_non_plus_id"], 3, t["matrices"], 2, 1,
+                       3, 6, 2)
+    body = b"".join(np.ascontiguousarray(a).tobytes() for a in (
+        y, t["hamiltonian"], t["ado_tuples"], t["ado_plus"], t["ado_minus"], t["pf_same_sum"], t["pf_same"],
+        t["pf_circ"], t["cbk"], t["cbk_sqrt"]))
+    assert raw == head + body
+    tabs, state, tm = hb.read_instance(path)
+    assert tm == 1.25e-13 and np.array_equal(state, y)
+    for k, v in t.items():
+        assert np.array_equal(np.asarray(tabs[k]), np.asarray(v)), k
+    # top only: the rest of the state reads back as zeros
+    hb.write_instance(sysd, path, state=y[:18], top_only=True)
+    _, state, _ = hb.read_instance(path)
+    assert np.array_equal(state[:18], y[:18]) and not state[18:].any()
+
+
+def test_instance_file_rejects_garbage(tmp_path):
+    p = tmp_path / "bad.bin"
+    p.write_bytes(b"\x07\x00\x00\x00" + b"\x00" * 100)
+    with pytest.raises(hb.HeomError) as e:
+        hb.read_instance(p)
+    assert "heom error -7" in str(e.value)
