@@ -31,12 +31,10 @@
 // sectors; both elements of a sector need the same neighbours.  For N = 8 an
 // ADO is exactly 32 sectors (1 KB): one warp per ADO, one sector per lane.
 //
-// Work mapping: a team of 32*TW threads (TW = ceil(P/32) warps) owns one ADO
-// at a time, thread p of the team owns sector p.  Teams loop over ADOs
-// (grid-stride) with a two-slot shared-memory pipeline: while ADO k is
-// computed, the tile and index row of ADO k+1 arrive by cp.async; one team
-// barrier per ADO.  The tile in shared memory is row-major with a padded row
-// (N+1 elements) for conflict-free row and column reads in the commutator.
+// Work mapping: N <= 8 one warp per ADO (heom_dmma_stage), N = 9..16 a team
+// of TW = ceil(P/32) warps per ADO (heom_pair_stage); in both the commutator
+// runs on the FP64 tensor pipe (m8n8k4) and the lane that owns a sector does
+// its bath terms and the stage write.
 #pragma once
 
 #include <cstdint>
@@ -95,7 +93,7 @@ struct PairParams {
     const double2* __restrict__ kmin;  // [3][W][LS]: kappa_i, kappa_j, kappa_d
     const double2* __restrict__ hs;    // [n_inst][N*N] H / hbar (complex H, SIMT kernel)
     const double* __restrict__ hr;     // [n_inst][N*(N+1)] real symmetric H / hbar, padded rows (SIMT kernel)
-    const double* __restrict__ hfrag;  // [n_inst][8][32] MMA operand fragments of H / hbar (DMMA kernel)
+    const double* __restrict__ hfrag;  // [n_inst][frag_doubles(N)] MMA operand fragments of H / hbar
     const int32_t* __restrict__ inst;  // [nodes] instance of each ADO; NULL when the handle holds one instance
     const double2* __restrict__ gamma0;// [N*N]
     const int16_t* __restrict__ slots; // [N][SL], -1 padded
@@ -105,36 +103,56 @@ struct PairParams {
 
 enum HKind : int { H_REAL_SYM = 0, H_GENERIC = 1 };
 
-// bytes of one instance's Hamiltonian as the SIMT kernel stages it
-__host__ __device__ constexpr int pair_h_bytes(int n, int hk) { return hk == H_REAL_SYM ? n * (n + 1) * 8 : n * n * 16; }
+// MMA operand fragments of H / hbar, per instance: N <= 8 one 8 x 8 block and
+// two k-slices, N = 9..16 a zero-padded 16 x 16 grid of 2 x 2 blocks and four
+// k-slices.  Layout [kind][block b][k-slice s][lane], lane l = 4g + t:
+// kind 0/1 = Re/Im of hb = H(4s+t, 8b+g) (B operand of w H for block column b),
+// kind 2/3 = Re/Im of ha = -H(8b+g, 4s+t) (A operand of -H w for block row b).
+__host__ __device__ constexpr int frag_blocks(int n) { return n <= 8 ? 1 : 2; }
+__host__ __device__ constexpr int frag_slices(int n) { return n <= 8 ? 2 : 4; }
+__host__ __device__ constexpr int frag_doubles(int n) { return 4 * frag_blocks(n) * frag_slices(n) * 32; }
+__host__ __device__ constexpr int frag_index(int n, int kind, int b, int s, int lane)
+{
+    return ((kind * frag_blocks(n) + b) * frag_slices(n) + s) * 32 + lane;
+}
+
+// SIMT-team kernel (N = 9..16): the staged ADO is row-major with row stride
+// TS = 4 (mod 8) double2 and the columns of rows with bit 1 set swapped in
+// pairs (k ^ 2), so that the quarter-warp reads of both MMA operands,
+// A = w(8I+g, 4s+t) and B = w(4s+t, 8J+g), hit eight distinct 16-byte bank groups.
+__host__ __device__ constexpr int tile_stride(int n) { return (n + 3) / 8 * 8 + 4; }
+__host__ __device__ constexpr int tile_pos(int n, int i, int k) { return i * tile_stride(n) + (k ^ (i & 2)); }
+// exchange tile of the commutator: 16 rows of 17 double2 (conflict-free C writes)
+constexpr int kXchStride = 17;
+constexpr int kXchBytes = 16 * kXchStride * 16;
 
 // dynamic shared memory carve-up (bytes); everything 16-B aligned
 struct PairSmem {
     int lut;     // kmin 3*W*LS double2 + cplus W*LS doubles
-    int team;    // per team: 2 slots
-    int slot;    // per slot: tile + nbr + tup + pss + H of the slot's instance
-    int tile_off, nbr_off, tup_off, pss_off, h_off;
+    int team;    // per team: 2 slots + the exchange tile
+    int slot;    // per slot: tile + nbr + tup + pss
+    int tile_off, nbr_off, tup_off, pss_off, xch_off;
 };
 
-__host__ __device__ inline PairSmem pair_smem_layout(int n, int W, int NW, int TWB, int LS, int hk)
+__host__ __device__ inline PairSmem pair_smem_layout(int n, int W, int NW, int TWB, int LS)
 {
     PairSmem s;
     const int lut = 3 * W * LS * 16 + W * LS * 8;
     s.lut = (lut + 15) & ~15;
-    const int tile = n * (n + 1) * 16;
+    const int tile = n * tile_stride(n) * 16;
     s.tile_off = 0;
     s.nbr_off = tile;
     s.tup_off = s.nbr_off + ((NW * 4 + 15) & ~15);
     s.pss_off = s.tup_off + ((TWB + 15) & ~15);
-    s.h_off = s.pss_off + 16;
-    s.slot = s.h_off + ((pair_h_bytes(n, hk) + 15) & ~15);
-    s.team = 2 * s.slot;
+    s.slot = s.pss_off + 16;
+    s.xch_off = 2 * s.slot;
+    s.team = s.xch_off + kXchBytes;
     return s;
 }
 
-__host__ inline size_t pair_smem_bytes(int n, int W, int NW, int TWB, int LS, int hk)
+__host__ inline size_t pair_smem_bytes(int n, int W, int NW, int TWB, int LS)
 {
-    const PairSmem s = pair_smem_layout(n, W, NW, TWB, LS, hk);
+    const PairSmem s = pair_smem_layout(n, W, NW, TWB, LS);
     const int teams = kCtaWarps / team_warps(n);
     return (size_t)s.lut + (size_t)teams * s.team;
 }
@@ -170,261 +188,6 @@ __device__ __forceinline__ void cmac(double2& acc, const double2 a, const double
 }
 
 __device__ __forceinline__ double2 ldg2(const double2* p) { return __ldg(p); }
-
-// issue the asynchronous copies of ADO u into a team slot; hinst >= 0 also
-// copies the Hamiltonian of instance hinst (the slot holds another instance's)
-template <int N, int HK>
-__device__ __forceinline__ void prefetch_ado(unsigned char* slot, const PairParams& p, const PairSmem& L,
-                                             int64_t u, int lt, int tt, int e1, int e2, bool active, int hinst)
-{
-    if (hinst >= 0) {
-        constexpr int hb = pair_h_bytes(N, HK);
-        const unsigned char* hsrc =
-            HK == H_REAL_SYM ? reinterpret_cast<const unsigned char*>(p.hr + (size_t)hinst * N * (N + 1))
-                             : reinterpret_cast<const unsigned char*>(p.hs + (size_t)hinst * N * N);
-        for (int q = lt * 16; q < hb; q += tt * 16) cp_async16(slot + L.h_off + q, hsrc + q);
-    }
-    double2* tile = reinterpret_cast<double2*>(slot + L.tile_off);
-    if (active) {
-        const double2* src = p.in + u * (2 * pairs_of(N));
-        const int pr = lt; // sector index
-        const int i1 = e1 / N, j1 = e1 - i1 * N, i2 = e2 / N, j2 = e2 - i2 * N;
-        cp_async16(tile + i1 * (N + 1) + j1, src + 2 * pr);
-        cp_async16(tile + i2 * (N + 1) + j2, src + 2 * pr + 1);
-    }
-    int32_t* nb = reinterpret_cast<int32_t*>(slot + L.nbr_off);
-    for (int q = lt * 4; q < p.NW; q += tt * 4) cp_async16(nb + q, p.nbr + u * p.NW + q);
-    unsigned char* tu = slot + L.tup_off;
-    for (int q = lt * 16; q < p.TWB; q += tt * 16) cp_async16(tu + q, p.tup + u * p.TWB + q);
-    if (lt == 0) cp_async16(slot + L.pss_off, p.pss + u);
-}
-
-// ADJ: the adjoint operator L^H (see heom_dmma_stage); the coefficient
-// tables are indexed by the tuple entry n: cplus(n) = chat sqrt(n+1) and
-// kappa(n) = khat sqrt(n), so L^H takes cplus(n-1) and conj(kappa(n+1)).
-template <int N, int HK, int SLT, bool ADJ>
-__global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_pair_stage(const PairParams p)
-{
-    constexpr int P = pairs_of(N);
-    constexpr int TW = team_warps(N);
-    constexpr int TT = 32 * TW;
-    constexpr int TEAMS = kCtaWarps / TW;
-    extern __shared__ __align__(128) unsigned char smem[];
-    const PairSmem L = pair_smem_layout(N, p.W, p.NW, p.TWB, p.LS, HK);
-    const int W = p.W, LS = p.LS, SL = p.SL;
-
-    // look-up tables shared by the CTA; 16-byte arrays first (all offsets multiples of 16)
-    double2* s_kmin = reinterpret_cast<double2*>(smem);              // 3 * W * LS
-    double* s_cplus = reinterpret_cast<double*>(s_kmin + 3 * W * LS); // W * LS
-    for (int q = threadIdx.x; q < W * LS; q += blockDim.x) s_cplus[q] = p.cplus[q];
-    for (int q = threadIdx.x; q < 3 * W * LS; q += blockDim.x) s_kmin[q] = p.kmin[q];
-
-    const int team = threadIdx.x / TT;
-    const int lt = threadIdx.x - team * TT;
-    const bool active = team < TEAMS && lt < P;
-    unsigned char* team_base = smem + L.lut + team * L.team;
-
-    int e1 = 0, e2 = 0, i = 0, j = 0, diag = 0;
-    if (active) pair_elements(N, lt, &e1, &e2, &i, &j, &diag);
-
-    const double2 g1 = active ? p.gamma0[e1] : make_double2(0.0, 0.0);
-    const double2 g2 = active ? p.gamma0[e2] : make_double2(0.0, 0.0);
-    int sli[SLT], slj[SLT];
-#pragma unroll
-    for (int q = 0; q < SLT; ++q) {
-        sli[q] = (active && q < SL) ? p.slots[i * SL + q] : -1;
-        slj[q] = (active && q < SL) ? p.slots[j * SL + q] : -1;
-    }
-    // coefficient tables seen by the two elements of this sector
-    const double2* kap_i1 = s_kmin + (diag ? 2 : 0) * W * LS; // element 1, slots of site i
-    const double2* kap_j1 = s_kmin + 1 * W * LS;              // element 1, slots of site j (off-diagonal)
-    const double2* kap_i2 = s_kmin + 1 * W * LS;              // element 2 = (j,i), slots of site i (its j side)
-    const double2* kap_j2 = s_kmin + (diag ? 2 : 0) * W * LS; // element 2, slots of site j
-
-    __syncthreads();
-    if (team >= TEAMS) return;
-
-    const int64_t nodes = p.nodes;
-    const int64_t stride = (int64_t)gridDim.x * TEAMS;
-    int64_t u = (int64_t)blockIdx.x * TEAMS + team;
-    int cur = 0;
-    // instance whose Hamiltonian each slot holds (team-uniform)
-    int hin0 = -1, hin1 = -1;
-    if (u < nodes) {
-        const int iu = p.inst ? p.inst[u] : 0;
-        prefetch_ado<N, HK>(team_base, p, L, u, lt, TT, e1, e2, active, iu);
-        hin0 = iu;
-    }
-    cp_async_wait_all();
-    team_sync<TW>(team);
-
-    for (; u < nodes; u += stride) {
-        unsigned char* slot = team_base + cur * L.slot;
-        const int64_t un = u + stride;
-        if (un < nodes) {
-            const int iu = p.inst ? p.inst[un] : 0;
-            int& held = cur ? hin0 : hin1;
-            prefetch_ado<N, HK>(team_base + (cur ^ 1) * L.slot, p, L, un, lt, TT, e1, e2, active,
-                                iu != held ? iu : -1);
-            held = iu;
-        }
-
-        if (active) {
-            // rows i and j of a real symmetric H (its columns equal its rows), or the complex H
-            const double* hri = reinterpret_cast<const double*>(slot + L.h_off) + i * (N + 1);
-            const double* hrj = reinterpret_cast<const double*>(slot + L.h_off) + j * (N + 1);
-            const double2* s_h = reinterpret_cast<const double2*>(slot + L.h_off);
-            const double2* t = reinterpret_cast<const double2*>(slot + L.tile_off);
-            const int32_t* nb = reinterpret_cast<const int32_t*>(slot + L.nbr_off);
-            const unsigned char* tu = slot + L.tup_off;
-            const double2 pss = *reinterpret_cast<const double2*>(slot + L.pss_off);
-            const int i1 = e1 / N, j1 = e1 - i1 * N, i2 = e2 / N, j2 = e2 - i2 * N;
-            const double2 s1 = t[i1 * (N + 1) + j1];
-            const double2 s2 = t[i2 * (N + 1) + j2];
-
-            // ---- commutator i * (w H - H w) / hbar for both elements ----
-            double c1r = 0.0, c1i = 0.0, c2r = 0.0, c2i = 0.0;
-#pragma unroll
-            for (int k = 0; k < N; ++k) {
-                const double2 a1 = t[i1 * (N + 1) + k]; // w(i1,k)
-                const double2 b1 = t[k * (N + 1) + j1]; // w(k,j1)
-                const double2 a2 = t[i2 * (N + 1) + k];
-                const double2 b2 = t[k * (N + 1) + j2];
-                if (HK == H_REAL_SYM) {
-                    // element 1 = (i1, j1): H(k,j1) = row j1, H(i1,k) = row i1
-                    // pairs: off-diagonal (i,j),(j,i): i1=i,j1=j,i2=j,j2=i; diagonal: (i,i),(j,j)
-                    const double hk_j1 = diag ? hri[k] : hrj[k];
-                    const double hi1_k = hri[k];
-                    const double hk_j2 = diag ? hrj[k] : hri[k];
-                    const double hi2_k = hrj[k];
-                    c1r = fma(a1.x, hk_j1, c1r);
-                    c1r = fma(-hi1_k, b1.x, c1r);
-                    c1i = fma(a1.y, hk_j1, c1i);
-                    c1i = fma(-hi1_k, b1.y, c1i);
-                    c2r = fma(a2.x, hk_j2, c2r);
-                    c2r = fma(-hi2_k, b2.x, c2r);
-                    c2i = fma(a2.y, hk_j2, c2i);
-                    c2i = fma(-hi2_k, b2.y, c2i);
-                } else {
-                    const double2 hkj1 = s_h[k * N + j1], hi1k = s_h[i1 * N + k];
-                    const double2 hkj2 = s_h[k * N + j2], hi2k = s_h[i2 * N + k];
-                    c1r = fma(a1.x, hkj1.x, c1r);
-                    c1r = fma(-a1.y, hkj1.y, c1r);
-                    c1i = fma(a1.x, hkj1.y, c1i);
-                    c1i = fma(a1.y, hkj1.x, c1i);
-                    c1r = fma(-hi1k.x, b1.x, c1r);
-                    c1r = fma(hi1k.y, b1.y, c1r);
-                    c1i = fma(-hi1k.x, b1.y, c1i);
-                    c1i = fma(-hi1k.y, b1.x, c1i);
-                    c2r = fma(a2.x, hkj2.x, c2r);
-                    c2r = fma(-a2.y, hkj2.y, c2r);
-                    c2i = fma(a2.x, hkj2.y, c2i);
-                    c2i = fma(a2.y, hkj2.x, c2i);
-                    c2r = fma(-hi2k.x, b2.x, c2r);
-                    c2r = fma(hi2k.y, b2.y, c2r);
-                    c2i = fma(-hi2k.x, b2.y, c2i);
-                    c2i = fma(-hi2k.y, b2.x, c2i);
-                }
-            }
-            double2 L1 = make_double2(-c1i, c1r);
-            double2 L2 = make_double2(-c2i, c2r);
-
-            // ---- same term ----
-            cmac(L1, make_double2(pss.x + g1.x, pss.y + g1.y), s1);
-            cmac(L2, make_double2(pss.x + g2.x, pss.y + g2.y), s2);
-
-            // ---- neighbours: per side all loads first, then the updates ----
-            // side 0 = slots of site i, side 1 = slots of site j
-#pragma unroll
-            for (int sd = 0; sd < 2; ++sd) {
-                double2 xp[SLT][2], xm[SLT][2];
-                int ix[SLT], ik[SLT];
-#pragma unroll
-                for (int q = 0; q < SLT; ++q) {
-                    const int sl = sd == 0 ? sli[q] : slj[q];
-                    const int32_t vp = (sl >= 0 && (ADJ || !diag)) ? nb[sl] : -1;
-                    const int32_t vm = (sl >= 0 && (!ADJ || !diag)) ? nb[W + sl] : -1;
-                    ix[q] = sl >= 0 ? (sl * LS + tu[sl]) : 0;
-                    ik[q] = ix[q];
-                    if (ADJ) { // table entries of L^H: cplus at n-1 (minus neighbour), kappa at n+1 (plus neighbour)
-                        ik[q] = vp >= 0 ? ix[q] + 1 : ix[q];
-                        ix[q] = vm >= 0 ? ix[q] - 1 : ix[q];
-                    }
-                    xp[q][0] = xp[q][1] = xm[q][0] = xm[q][1] = make_double2(0.0, 0.0);
-                    if (vp >= 0) {
-                        const double2* src = p.in + (int64_t)vp * (2 * P) + 2 * lt;
-                        xp[q][0] = ldg2(src);
-                        xp[q][1] = ldg2(src + 1);
-                    }
-                    if (vm >= 0) {
-                        const double2* src = p.in + (int64_t)vm * (2 * P) + 2 * lt;
-                        xm[q][0] = ldg2(src);
-                        xm[q][1] = ldg2(src + 1);
-                    }
-                }
-#pragma unroll
-                for (int q = 0; q < SLT; ++q) {
-                    const int sl = sd == 0 ? sli[q] : slj[q];
-                    if (sl < 0) continue;
-                    // L: i-coefficient on the plus neighbour, kappa on the minus one;
-                    // L^H: -i cplus(n-1) on the minus neighbour, conj(kappa(n+1)) on the plus one
-                    const double c = diag ? 0.0 : (ADJ ? -s_cplus[ix[q]] : s_cplus[ix[q]]);
-                    const double2 t1 = ADJ ? xm[q][0] : xp[q][0], t2 = ADJ ? xm[q][1] : xp[q][1];
-                    const double2 k1 = ADJ ? xp[q][0] : xm[q][0], k2 = ADJ ? xp[q][1] : xm[q][1];
-                    auto kap = [&](const double2* tab) {
-                        const double2 v = tab[ik[q]];
-                        return ADJ ? make_double2(v.x, -v.y) : v;
-                    };
-                    if (sd == 0) {
-                        // site i: element 1 (i,j) i-side (+i c, kappa_i); element 2 (j,i) j-side (-i c, kappa_j)
-                        L1.x = fma(-c, t1.y, L1.x);
-                        L1.y = fma(c, t1.x, L1.y);
-                        L2.x = fma(c, t2.y, L2.x);
-                        L2.y = fma(-c, t2.x, L2.y);
-                        cmac(L1, kap(kap_i1), k1);
-                        if (!diag) cmac(L2, kap(kap_i2), k2);
-                    } else {
-                        // site j: element 1 j-side (-i c, kappa_j); element 2 i-side (+i c, kappa_i)
-                        L1.x = fma(c, t1.y, L1.x);
-                        L1.y = fma(-c, t1.x, L1.y);
-                        L2.x = fma(-c, t2.y, L2.x);
-                        L2.y = fma(c, t2.x, L2.y);
-                        if (!diag) cmac(L1, kap(kap_j1), k1);
-                        cmac(L2, kap(kap_j2), k2);
-                    }
-                }
-            }
-
-            // ---- stage write ----
-            const int64_t off = u * (2 * P) + 2 * lt;
-            double2 x1, x2;
-            if (p.y) {
-                x1 = p.y[off];
-                x2 = p.y[off + 1];
-            } else {
-                x1 = s1;
-                x2 = s2;
-            }
-            double2 r1 = make_double2(p.alpha.x * x1.x - p.alpha.y * x1.y, p.alpha.x * x1.y + p.alpha.y * x1.x);
-            double2 r2 = make_double2(p.alpha.x * x2.x - p.alpha.y * x2.y, p.alpha.x * x2.y + p.alpha.y * x2.x);
-            cmac(r1, p.beta, L1);
-            cmac(r2, p.beta, L2);
-            __stcs(p.out + off, r1);
-            __stcs(p.out + off + 1, r2);
-            if (p.use_acc) {
-                double2 a1 = p.acc_init ? s1 : p.acc[off];
-                double2 a2 = p.acc_init ? s2 : p.acc[off + 1];
-                cmac(a1, p.acc_beta, L1);
-                cmac(a2, p.acc_beta, L2);
-                p.acc[off] = a1;
-                p.acc[off + 1] = a2;
-            }
-        }
-        cp_async_wait_all();
-        team_sync<TW>(team);
-        cur ^= 1;
-    }
-}
 
 // ---------------------------------------------------------------------------
 // N <= 8: one warp per ADO, commutator on the FP64 tensor pipe.
@@ -816,6 +579,240 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_dmma_stage(const DmmaP
     }
 }
 
+// ---------------------------------------------------------------------------
+// N = 9..16: a team of TW = ceil(P / 32) warps per ADO, thread p of the team
+// owns sector p.  Teams loop over ADOs (grid-stride) with a two-slot
+// pipeline: while ADO k is computed, its successor's tile (scattered into the
+// row-major tile_pos layout), neighbour row, tuple row and pf_same_sum arrive
+// by cp.async.
+//
+// Commutator on the FP64 tensor pipe: the tile is zero-padded to 16 x 16 and
+// cut into 2 x 2 blocks of 8 x 8; block (I, J) of C = w H - H w takes
+// ceil(N/4) k-slices of m8n8k4 MMAs (A = w(8I+g, 4s+t) against the H
+// fragment hb(J, s); ha(I, s) against B = w(4s+t, 8J+g)).  Warp wt of the
+// team computes blocks [4 wt / TW, 4 (wt+1) / TW) and writes them to the
+// team's exchange tile; after a team barrier every owner reads the two
+// elements of its sector.  The bath terms follow the same formulas as the
+// DMMA kernel, one 32-byte sector load per neighbour.
+// ---------------------------------------------------------------------------
+
+// issue the asynchronous copies of ADO u into a team slot
+template <int N>
+__device__ __forceinline__ void prefetch_ado(unsigned char* slot, const PairParams& p, const PairSmem& L,
+                                             int64_t u, int lt, int tt, int e1, int e2, bool active)
+{
+    double2* tile = reinterpret_cast<double2*>(slot + L.tile_off);
+    if (active) {
+        const double2* src = p.in + u * (2 * pairs_of(N));
+        const int i1 = e1 / N, j1 = e1 - i1 * N, i2 = e2 / N, j2 = e2 - i2 * N;
+        cp_async16(tile + tile_pos(N, i1, j1), src + 2 * lt);
+        cp_async16(tile + tile_pos(N, i2, j2), src + 2 * lt + 1);
+    }
+    int32_t* nb = reinterpret_cast<int32_t*>(slot + L.nbr_off);
+    for (int q = lt * 4; q < p.NW; q += tt * 4) cp_async16(nb + q, p.nbr + u * p.NW + q);
+    unsigned char* tu = slot + L.tup_off;
+    for (int q = lt * 16; q < p.TWB; q += tt * 16) cp_async16(tu + q, p.tup + u * p.TWB + q);
+    if (lt == 0) cp_async16(slot + L.pss_off, p.pss + u);
+}
+
+// ADJ: the adjoint operator L^H (see heom_dmma_stage); the coefficient
+// tables are indexed by the tuple entry n: cplus(n) = chat sqrt(n+1) and
+// kappa(n) = khat sqrt(n), so L^H takes cplus(n-1) and conj(kappa(n+1)).
+template <int N, int HK, int SLT, bool ADJ>
+__global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_pair_stage(const PairParams p)
+{
+    static_assert(N > 8 && N <= 16, "team kernel handles N = 9..16");
+    constexpr int P = pairs_of(N);
+    constexpr int TW = team_warps(N);
+    constexpr int TT = 32 * TW;
+    constexpr int TEAMS = kCtaWarps / TW;
+    constexpr int KS = (N + 3) / 4; // k-slices of the padded commutator
+    constexpr int FD = frag_doubles(N);
+    extern __shared__ __align__(128) unsigned char smem[];
+    const PairSmem L = pair_smem_layout(N, p.W, p.NW, p.TWB, p.LS);
+    const int W = p.W, LS = p.LS, SL = p.SL;
+
+    // look-up tables shared by the CTA; 16-byte arrays first (all offsets multiples of 16)
+    double2* s_kmin = reinterpret_cast<double2*>(smem);              // 3 * W * LS
+    double* s_cplus = reinterpret_cast<double*>(s_kmin + 3 * W * LS); // W * LS
+    for (int q = threadIdx.x; q < W * LS; q += blockDim.x) s_cplus[q] = p.cplus[q];
+    for (int q = threadIdx.x; q < 3 * W * LS; q += blockDim.x) s_kmin[q] = p.kmin[q];
+
+    const int team = threadIdx.x / TT;
+    const int lt = threadIdx.x - team * TT;
+    const bool active = team < TEAMS && lt < P;
+    unsigned char* team_base = smem + L.lut + team * L.team;
+    double2* xch = reinterpret_cast<double2*>(team_base + L.xch_off);
+    const int wt = lt >> 5, lane = lt & 31, g = lane >> 2, t4 = lane & 3;
+    const int blk0 = wt * 4 / TW, blk1 = (wt + 1) * 4 / TW; // commutator blocks of this warp
+
+    int e1 = 0, e2 = 0, i = 0, j = 0, diag = 0;
+    if (active) pair_elements(N, lt, &e1, &e2, &i, &j, &diag);
+
+    const double2 g1 = active ? p.gamma0[e1] : make_double2(0.0, 0.0);
+    const double2 g2 = active ? p.gamma0[e2] : make_double2(0.0, 0.0);
+    int sli[SLT], slj[SLT];
+#pragma unroll
+    for (int q = 0; q < SLT; ++q) {
+        sli[q] = (active && q < SL) ? p.slots[i * SL + q] : -1;
+        slj[q] = (active && q < SL) ? p.slots[j * SL + q] : -1;
+    }
+    // coefficient tables seen by the two elements of this sector
+    const double2* kap_i1 = s_kmin + (diag ? 2 : 0) * W * LS; // element 1, slots of site i
+    const double2* kap_j1 = s_kmin + 1 * W * LS;              // element 1, slots of site j (off-diagonal)
+    const double2* kap_i2 = s_kmin + 1 * W * LS;              // element 2 = (j,i), slots of site i (its j side)
+    const double2* kap_j2 = s_kmin + (diag ? 2 : 0) * W * LS; // element 2, slots of site j
+
+    __syncthreads();
+    if (team >= TEAMS) return;
+
+    const int64_t nodes = p.nodes;
+    const int64_t stride = (int64_t)gridDim.x * TEAMS;
+    int64_t u = (int64_t)blockIdx.x * TEAMS + team;
+    int cur = 0;
+    if (u < nodes) prefetch_ado<N>(team_base, p, L, u, lt, TT, e1, e2, active);
+    cp_async_wait_all();
+    team_sync<TW>(team);
+    int ci = (p.inst && u < nodes) ? __ldg(p.inst + u) : 0; // instance of the current ADO
+
+    for (; u < nodes; u += stride) {
+        unsigned char* slot = team_base + cur * L.slot;
+        const int64_t un = u + stride;
+        int ni = ci;
+        if (un < nodes) {
+            prefetch_ado<N>(team_base + (cur ^ 1) * L.slot, p, L, un, lt, TT, e1, e2, active);
+            if (p.inst) ni = __ldg(p.inst + un);
+        }
+        const double2* t = reinterpret_cast<const double2*>(slot + L.tile_off);
+
+        // ---- commutator w H - H w / hbar on the tensor pipe, into the exchange tile ----
+        const double* fr = p.hfrag + (size_t)ci * FD;
+#pragma unroll
+        for (int blk = 0; blk < 4; ++blk) {
+            if (blk < blk0 || blk >= blk1) continue;
+            const int I = blk >> 1, J = blk & 1;
+            double cr0 = 0.0, cr1 = 0.0, ci0 = 0.0, ci1 = 0.0;
+#pragma unroll
+            for (int s = 0; s < KS; ++s) {
+                const int ra = 8 * I + g, ka = 4 * s + t4; // A = w(ra, ka), B = w(ka, cb)
+                const int cb = 8 * J + g;
+                const double2 z = make_double2(0.0, 0.0);
+                const double2 A = (ra < N && ka < N) ? t[tile_pos(N, ra, ka)] : z;
+                const double2 B = (ka < N && cb < N) ? t[tile_pos(N, ka, cb)] : z;
+                const double hbr = __ldg(fr + frag_index(N, 0, J, s, lane));
+                const double har = __ldg(fr + frag_index(N, 2, I, s, lane));
+                dmma(cr0, cr1, A.x, hbr); // Re(w) Re(H)
+                dmma(ci0, ci1, A.y, hbr); // Im(w) Re(H)
+                dmma(cr0, cr1, har, B.x); // -Re(H) Re(w)
+                dmma(ci0, ci1, har, B.y); // -Re(H) Im(w)
+                if (HK == H_GENERIC) {
+                    const double hbi = __ldg(fr + frag_index(N, 1, J, s, lane));
+                    const double hai = __ldg(fr + frag_index(N, 3, I, s, lane));
+                    dmma(cr0, cr1, -A.y, hbi); // -Im(w) Im(H)
+                    dmma(ci0, ci1, A.x, hbi);  //  Re(w) Im(H)
+                    dmma(cr0, cr1, -hai, B.y); // +Im(H) Im(w)
+                    dmma(ci0, ci1, hai, B.x);  // -Im(H) Re(w)
+                }
+            }
+            double2* xr = xch + (8 * I + g) * kXchStride + 8 * J + 2 * t4;
+            xr[0] = make_double2(cr0, ci0);
+            xr[1] = make_double2(cr1, ci1);
+        }
+        team_sync<TW>(team);
+
+        if (active) {
+            const int32_t* nb = reinterpret_cast<const int32_t*>(slot + L.nbr_off);
+            const unsigned char* tu = slot + L.tup_off;
+            const double2 pss = *reinterpret_cast<const double2*>(slot + L.pss_off);
+            const int i1 = e1 / N, j1 = e1 - i1 * N, i2 = e2 / N, j2 = e2 - i2 * N;
+            const double2 s1 = t[tile_pos(N, i1, j1)];
+            const double2 s2 = t[tile_pos(N, i2, j2)];
+            const double2 c1 = xch[i1 * kXchStride + j1], c2 = xch[i2 * kXchStride + j2];
+            double2 L1 = make_double2(-c1.y, c1.x); // i * (w H - H w) / hbar
+            double2 L2 = make_double2(-c2.y, c2.x);
+
+            // ---- same term ----
+            cmac(L1, make_double2(pss.x + g1.x, pss.y + g1.y), s1);
+            cmac(L2, make_double2(pss.x + g2.x, pss.y + g2.y), s2);
+
+            // ---- neighbours: per side all loads first, then the updates ----
+            // side 0 = slots of site i, side 1 = slots of site j
+#pragma unroll
+            for (int sd = 0; sd < 2; ++sd) {
+                double2 xp[SLT][2], xm[SLT][2];
+                int ix[SLT], ik[SLT];
+#pragma unroll
+                for (int q = 0; q < SLT; ++q) {
+                    const int sl = sd == 0 ? sli[q] : slj[q];
+                    const int32_t vp = (sl >= 0 && (ADJ || !diag)) ? nb[sl] : -1;
+                    const int32_t vm = (sl >= 0 && (!ADJ || !diag)) ? nb[W + sl] : -1;
+                    ix[q] = sl >= 0 ? (sl * LS + tu[sl]) : 0;
+                    ik[q] = ix[q];
+                    if (ADJ) { // table entries of L^H: cplus at n-1 (minus neighbour), kappa at n+1 (plus neighbour)
+                        ik[q] = vp >= 0 ? ix[q] + 1 : ix[q];
+                        ix[q] = vm >= 0 ? ix[q] - 1 : ix[q];
+                    }
+                    xp[q][0] = xp[q][1] = xm[q][0] = xm[q][1] = make_double2(0.0, 0.0);
+                    if (vp >= 0) ld256(p.in + (int64_t)vp * (2 * P) + 2 * lt, xp[q][0], xp[q][1]);
+                    if (vm >= 0) ld256(p.in + (int64_t)vm * (2 * P) + 2 * lt, xm[q][0], xm[q][1]);
+                }
+#pragma unroll
+                for (int q = 0; q < SLT; ++q) {
+                    const int sl = sd == 0 ? sli[q] : slj[q];
+                    if (sl < 0) continue;
+                    // L: i-coefficient on the plus neighbour, kappa on the minus one;
+                    // L^H: -i cplus(n-1) on the minus neighbour, conj(kappa(n+1)) on the plus one
+                    const double c = diag ? 0.0 : (ADJ ? -s_cplus[ix[q]] : s_cplus[ix[q]]);
+                    const double2 t1 = ADJ ? xm[q][0] : xp[q][0], t2 = ADJ ? xm[q][1] : xp[q][1];
+                    const double2 k1 = ADJ ? xp[q][0] : xm[q][0], k2 = ADJ ? xp[q][1] : xm[q][1];
+                    auto kap = [&](const double2* tab) {
+                        const double2 v = tab[ik[q]];
+                        return ADJ ? make_double2(v.x, -v.y) : v;
+                    };
+                    if (sd == 0) {
+                        // site i: element 1 (i,j) i-side (+i c, kappa_i); element 2 (j,i) j-side (-i c, kappa_j)
+                        L1.x = fma(-c, t1.y, L1.x);
+                        L1.y = fma(c, t1.x, L1.y);
+                        L2.x = fma(c, t2.y, L2.x);
+                        L2.y = fma(-c, t2.x, L2.y);
+                        cmac(L1, kap(kap_i1), k1);
+                        if (!diag) cmac(L2, kap(kap_i2), k2);
+                    } else {
+                        // site j: element 1 j-side (-i c, kappa_j); element 2 i-side (+i c, kappa_i)
+                        L1.x = fma(c, t1.y, L1.x);
+                        L1.y = fma(-c, t1.x, L1.y);
+                        L2.x = fma(-c, t2.y, L2.x);
+                        L2.y = fma(c, t2.x, L2.y);
+                        if (!diag) cmac(L1, kap(kap_j1), k1);
+                        cmac(L2, kap(kap_j2), k2);
+                    }
+                }
+            }
+
+            // ---- stage write ----
+            const int64_t off = u * (2 * P) + 2 * lt;
+            double2 x1 = s1, x2 = s2;
+            if (p.y) ld256_cg(p.y + off, x1, x2);
+            double2 r1 = make_double2(p.alpha.x * x1.x - p.alpha.y * x1.y, p.alpha.x * x1.y + p.alpha.y * x1.x);
+            double2 r2 = make_double2(p.alpha.x * x2.x - p.alpha.y * x2.y, p.alpha.x * x2.y + p.alpha.y * x2.x);
+            cmac(r1, p.beta, L1);
+            cmac(r2, p.beta, L2);
+            st256_cs(p.out + off, r1, r2);
+            if (p.use_acc) {
+                double2 a1 = s1, a2 = s2;
+                if (!p.acc_init) ld256_cg(p.acc + off, a1, a2);
+                cmac(a1, p.acc_beta, L1);
+                cmac(a2, p.acc_beta, L2);
+                st256(p.acc + off, a1, a2);
+            }
+        }
+        cp_async_wait_all();
+        team_sync<TW>(team);
+        cur ^= 1;
+        ci = ni;
+    }
+}
+
 // out = y + h * sum_l c_l k_l over doubles, terms with c_l == 0 skipped, in
 // the operation order of rk_weighted_add.cl:78-95 (no contraction).
 struct WaddParams {
@@ -1149,7 +1146,7 @@ struct FieldParams {
     double t0, dt;         // explicit mode: the evaluation time t0 (time == nullptr)
     double2* hs_t;         // [nt][K][N*N]
     double* hr_t;          // [nt][K][N*(N+1)]
-    double* frag_t;        // [nt][K][256] (N <= 8)
+    double* frag_t;        // [nt][K][frag_doubles(N)]
     int K, N, nt;
 };
 
@@ -1186,18 +1183,20 @@ __global__ void heom_field_tables(const FieldParams f)
                 f.hr_t[((size_t)s * f.K + k) * N * (N + 1) + (q / N) * (N + 1) + q % N] = re;
             }
             __syncthreads();
-            if (N <= 8)
-                for (int q = threadIdx.x; q < 256; q += blockDim.x) {
-                    // operand fragments as in the host tables: part q >> 5 (re hb s0, s1 | im hb | re ha | im ha)
-                    const int l = q & 31, part = q >> 5, sl = part & 1, kind = part >> 1;
-                    const int r = l >> 2, c = 4 * sl + (l & 3);
+            {
+                const int fd = frag_doubles(N), nb = frag_blocks(N), ns = frag_slices(N);
+                for (int q = threadIdx.x; q < fd; q += blockDim.x) {
+                    // operand fragments as in the host tables ([kind][block][k-slice][lane], frag_index)
+                    const int l = q & 31, part = q >> 5, sl = part % ns, b = (part / ns) % nb, kind = part / (ns * nb);
+                    const int r = 8 * b + (l >> 2), c = 4 * sl + (l & 3);
                     double v = 0.0;
                     if (r < N && c < N) {
                         const double2 hcr = hs[c * N + r], hrc = hs[r * N + c];
                         v = kind == 0 ? hcr.x : kind == 1 ? hcr.y : kind == 2 ? -hrc.x : -hrc.y;
                     }
-                    f.frag_t[((size_t)s * f.K + k) * 256 + q] = v;
+                    f.frag_t[((size_t)s * f.K + k) * fd + q] = v;
                 }
+            }
             __syncthreads();
         }
     }

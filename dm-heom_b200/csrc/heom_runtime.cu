@@ -282,7 +282,7 @@ struct heom_handle {
     heomk::Pulse pulses[2] = {};
     DevBuf<double2> d_dplus, d_dminus;     // D+ / hbar, D- / hbar
     DevBuf<double2> field_hs;              // [3][K][N*N]
-    DevBuf<double> field_hr, field_frag;   // [3][K][N*(N+1)], [3][K][256]
+    DevBuf<double> field_hr, field_frag;   // [3][K][N*(N+1)], [3][K][frag_doubles(N)]
     DevBuf<double> d_time;                 // time of the propagation state (device, advanced by field steps)
     double time = 0.0;                     // host mirror
 
@@ -351,26 +351,25 @@ int build_neighbours(heom_handle* h)
 
 // device-side forms of one instance's H (interleaved re/im, J): H / hbar
 // row-major (hs), its real part in padded rows (hr) and the MMA operand
-// fragments (frag, N <= 8: lane l = 4r + t, k-slice s: column c = 4s+t;
-// hb = H(c, r), ha = -H(r, c))
+// fragments (frag, heomk::frag_index: lane l = 4g + t, block b, k-slice s,
+// row r = 8b + g, column c = 4s + t; hb = H(c, r), ha = -H(r, c); zero outside N x N)
 void h_tables(const double* hk, int N, double2* hs, double* hr, double* frag)
 {
     for (int q = 0; q < N * N; ++q) {
         hs[q] = make_double2(hk[2 * q] / kHbar, hk[2 * q + 1] / kHbar);
         hr[(q / N) * (N + 1) + q % N] = hk[2 * q] / kHbar;
     }
-    for (int l = 0; l < 32 && N <= 8 && frag; ++l) {
-        const int r = l >> 2, t = l & 3;
-        for (int sl = 0; sl < 2; ++sl) {
-            const int c = 4 * sl + t;
-            if (r >= N || c >= N) continue;
-            const double2 hcr = hs[c * N + r], hrc = hs[r * N + c];
-            frag[32 * (0 + sl) + l] = hcr.x;
-            frag[32 * (2 + sl) + l] = hcr.y;
-            frag[32 * (4 + sl) + l] = -hrc.x;
-            frag[32 * (6 + sl) + l] = -hrc.y;
-        }
-    }
+    for (int b = 0; b < heomk::frag_blocks(N); ++b)
+        for (int sl = 0; sl < heomk::frag_slices(N); ++sl)
+            for (int l = 0; l < 32; ++l) {
+                const int r = 8 * b + (l >> 2), c = 4 * sl + (l & 3);
+                if (r >= N || c >= N) continue;
+                const double2 hcr = hs[c * N + r], hrc = hs[r * N + c];
+                frag[heomk::frag_index(N, 0, b, sl, l)] = hcr.x;
+                frag[heomk::frag_index(N, 1, b, sl, l)] = hcr.y;
+                frag[heomk::frag_index(N, 2, b, sl, l)] = -hrc.x;
+                frag[heomk::frag_index(N, 3, b, sl, l)] = -hrc.y;
+            }
 }
 
 bool real_symmetric(const double* hk, int N)
@@ -409,12 +408,13 @@ int upload_hamiltonian(heom_handle* h)
     const int N = h->N, K = h->n_inst;
     std::vector<double2> hs((size_t)K * N * N);
     std::vector<double> hr((size_t)K * N * (N + 1), 0.0);
-    std::vector<double> frag(N <= 8 ? (size_t)K * 256 : 0, 0.0);
+    const size_t fd = heomk::frag_doubles(N);
+    std::vector<double> frag((size_t)K * fd, 0.0);
     bool real_sym = true;
     for (int k = 0; k < K; ++k) {
         const double* hk = h->ham.data() + (size_t)k * 2 * N * N;
         h_tables(hk, N, hs.data() + (size_t)k * N * N, hr.data() + (size_t)k * N * (N + 1),
-                 N <= 8 ? frag.data() + (size_t)k * 256 : nullptr);
+                 frag.data() + (size_t)k * fd);
         real_sym = real_sym && real_symmetric(hk, N);
     }
     // real symmetric H (every instance) takes the cheaper kernel variants; a
@@ -429,7 +429,7 @@ int upload_hamiltonian(heom_handle* h)
     }
     CUDA_TRY(cudaMemcpy(h->d_hs.p, hs.data(), hs.size() * 16, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(h->d_hr.p, hr.data(), hr.size() * 8, cudaMemcpyHostToDevice));
-    if (!frag.empty()) CUDA_TRY(cudaMemcpy(h->d_hfrag.p, frag.data(), frag.size() * 8, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(h->d_hfrag.p, frag.data(), frag.size() * 8, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(h->d_gamma0.p, g0.data(), g0.size() * 16, cudaMemcpyHostToDevice));
     // the kernel variant may change: rebuild the cached step graph
     if (h->step_graph) {
@@ -569,7 +569,7 @@ int resolve_stage(heom_handle* h, const void** fn_out, int* blocks_out = nullptr
         threads = heomk::kCtaWarps * 32;
     } else {
         fn = (const void*)pick_stage(h->N, h->hkind, h->SLT, adj);
-        smem = heomk::pair_smem_bytes(h->N, h->W, h->NW, h->TWB, h->LS, h->hkind);
+        smem = heomk::pair_smem_bytes(h->N, h->W, h->NW, h->TWB, h->LS);
         threads = cta_threads(h->N);
     }
     if (!fn) return fail(HEOM_E_UNSUPPORTED, "states = %d not supported", h->N);
@@ -711,7 +711,7 @@ AdjTabs field_tabs(const heom_handle* h, int s)
     AdjTabs t;
     t.pss = h->d_pss.p;
     t.gamma0 = h->d_gamma0.p;
-    t.hfrag = h->field_frag.p + (size_t)s * h->n_inst * 256;
+    t.hfrag = h->field_frag.p + (size_t)s * h->n_inst * heomk::frag_doubles(h->N);
     t.hr = h->field_hr.p + (size_t)s * h->n_inst * h->N * (h->N + 1);
     t.hs = h->field_hs.p + (size_t)s * h->n_inst * h->N * h->N;
     t.adjoint = false;
@@ -1372,7 +1372,7 @@ int heom_set_field(heom_handle* h, const double* dipole_plus, const double* dipo
         if (int rc = h->d_dminus.alloc(N * N)) return rc;
         if (int rc = h->field_hs.alloc((size_t)3 * K * N * N)) return rc;
         if (int rc = h->field_hr.alloc((size_t)3 * K * N * (N + 1))) return rc;
-        if (int rc = h->field_frag.alloc((size_t)3 * K * 256)) return rc;
+        if (int rc = h->field_frag.alloc((size_t)3 * K * heomk::frag_doubles(N))) return rc;
         if (int rc = h->d_time.alloc(1)) return rc;
         CUDA_TRY(cudaMemset(h->field_hr.p, 0, (size_t)3 * K * N * (N + 1) * 8));
     }
@@ -1605,7 +1605,7 @@ int heom_set_flow_buffers(heom_handle* h, heom_buffer* flow_from_above, heom_buf
     CUDA_TRY(cudaSetDevice(h->device));
     if ((flow_from_above || flow_from_below) && !h->d_zero.p) {
         const size_t K = h->n_inst, N = h->N;
-        size_t len = std::max<size_t>({K * 256, K * N * (N + 1), 2 * K * N * N, (size_t)6 * h->W * h->LS,
+        size_t len = std::max<size_t>({K * heomk::frag_doubles((int)N), K * N * (N + 1), 2 * K * N * N, (size_t)6 * h->W * h->LS,
                                        (size_t)6 * h->W, (size_t)2 * h->nodes});
         if (int rc = h->d_zero.alloc(len)) return rc;
         CUDA_TRY(cudaMemset(h->d_zero.p, 0, len * 8));
@@ -2413,7 +2413,8 @@ int adj_tables(heom_adjoint* A, const heomhost::system_params& sp)
     std::vector<double2> g0 = gamma0_table(h, h->pf_same);
     for (auto& v : g0) v.y = -v.y;
     std::vector<double2> hs((size_t)K * N * N);
-    std::vector<double> hr((size_t)K * N * (N + 1), 0.0), frag((size_t)K * 256, 0.0), hadj(2 * N * N);
+    const size_t fd = heomk::frag_doubles(N);
+    std::vector<double> hr((size_t)K * N * (N + 1), 0.0), frag((size_t)K * fd, 0.0), hadj(2 * N * N);
     for (int k = 0; k < K; ++k) {
         const double* hk = h->ham.data() + (size_t)k * 2 * N * N;
         for (int i = 0; i < N; ++i)
@@ -2422,7 +2423,7 @@ int adj_tables(heom_adjoint* A, const heomhost::system_params& sp)
                 hadj[2 * (i * N + j) + 1] = hk[2 * (j * N + i) + 1];
             }
         h_tables(hadj.data(), N, hs.data() + (size_t)k * N * N, hr.data() + (size_t)k * N * (N + 1),
-                 N <= 8 ? frag.data() + (size_t)k * 256 : nullptr);
+                 frag.data() + (size_t)k * fd);
     }
     if (int rc = A->pss_adj.alloc(pss.size())) return rc;
     if (int rc = A->g0_adj.alloc(g0.size())) return rc;

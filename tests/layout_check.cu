@@ -27,21 +27,45 @@ int main()
         for (int W = 1; W <= 64; ++W)
             for (int depth = 1; depth <= 40; ++depth) {
                 const int LS = depth + 1, NW = (2 * W + 3) & ~3, TWB = (W + 15) & ~15;
-                for (int hk = 0; hk < 2; ++hk) {
-                    const heomk::PairSmem L = heomk::pair_smem_layout(n, W, NW, TWB, LS, hk);
-                    const int kmin = 0, cplus = 3 * W * LS * 16, end = cplus + W * LS * 8;
-                    if (kmin % 16 || cplus % 16 || end > L.lut) { printf("bad lut n=%d W=%d LS=%d\n", n, W, LS); ++bad; }
-                    if (L.lut % 16 || L.slot % 16 || L.team % 16 || L.tile_off % 16 || L.nbr_off % 16 ||
-                        L.tup_off % 16 || L.pss_off % 16 || L.h_off % 16) { printf("bad slot n=%d W=%d\n", n, W); ++bad; }
-                    const int hbytes = hk == heomk::H_REAL_SYM ? n * (n + 1) * 8 : n * n * 16;
-                    if (hbytes % 16) { printf("bad H bytes n=%d hk=%d\n", n, hk); ++bad; }
-                    if (L.nbr_off - L.tile_off < n * (n + 1) * 16 || L.tup_off - L.nbr_off < NW * 4 ||
-                        L.pss_off - L.tup_off < TWB || L.h_off - L.pss_off < 16 || L.slot - L.h_off < hbytes)
-                        { printf("bad sizes n=%d W=%d\n", n, W); ++bad; }
-                    if (NW % 4 || NW < 2 * W || TWB % 16 || TWB < W) { printf("bad pads W=%d\n", W); ++bad; }
-                    ++checked;
-                }
+                const heomk::PairSmem L = heomk::pair_smem_layout(n, W, NW, TWB, LS);
+                const int kmin = 0, cplus = 3 * W * LS * 16, end = cplus + W * LS * 8;
+                if (kmin % 16 || cplus % 16 || end > L.lut) { printf("bad lut n=%d W=%d LS=%d\n", n, W, LS); ++bad; }
+                if (L.lut % 16 || L.slot % 16 || L.team % 16 || L.tile_off % 16 || L.nbr_off % 16 ||
+                    L.tup_off % 16 || L.pss_off % 16 || L.xch_off % 16) { printf("bad slot n=%d W=%d\n", n, W); ++bad; }
+                if (L.nbr_off - L.tile_off < n * heomk::tile_stride(n) * 16 || L.tup_off - L.nbr_off < NW * 4 ||
+                    L.pss_off - L.tup_off < TWB || L.slot - L.pss_off < 16 || L.xch_off < 2 * L.slot ||
+                    L.team - L.xch_off < heomk::kXchBytes)
+                    { printf("bad sizes n=%d W=%d\n", n, W); ++bad; }
+                if (NW % 4 || NW < 2 * W || TWB % 16 || TWB < W) { printf("bad pads W=%d\n", W); ++bad; }
+                ++checked;
             }
+        // tile positions: inside the row, one per element
+        {
+            int used[16 * 20] = {0};
+            for (int i = 0; i < n; ++i)
+                for (int k = 0; k < n; ++k) {
+                    const int q = heomk::tile_pos(n, i, k);
+                    if (q - i * heomk::tile_stride(n) >= heomk::tile_stride(n) || used[q]++)
+                        { printf("bad tile position n=%d (%d,%d)\n", n, i, k); ++bad; }
+                }
+        }
+        // team kernel: conflict-free quarter-warp operand reads (16-byte bank groups: index mod 8)
+        // and exchange writes; lanes 8q..8q+7 hold g = 2q, 2q+1 and t = 0..3
+        if (n > 8)
+            for (int b = 0; b < 2; ++b)
+                for (int s = 0; s < 4; ++s)
+                    for (int q = 0; q < 4; ++q)
+                        for (int which = 0; which < 3; ++which) {
+                            int used[8] = {0};
+                            for (int g = 2 * q; g <= 2 * q + 1; ++g)
+                                for (int t = 0; t < 4; ++t) {
+                                    int pos;
+                                    if (which == 0) pos = heomk::tile_pos(n, 8 * b + g, 4 * s + t); // A
+                                    else if (which == 1) pos = heomk::tile_pos(n, 4 * s + t, 8 * b + g); // B
+                                    else pos = (8 * b + g) * heomk::kXchStride + 8 * (s & 1) + 2 * t + (s >> 1); // C: J = s & 1, c0/c1 = s >> 1
+                                    if (used[pos % 8]++) { printf("bank conflict n=%d b=%d s=%d q=%d w=%d\n", n, b, s, q, which); ++bad; }
+                                }
+                        }
     }
     // searched sector tables for N <= 8: coverage, and for N = 8 conflict-free
     // operand and exchange reads of the tensor-pipe kernel

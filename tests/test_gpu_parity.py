@@ -40,6 +40,23 @@ def complex_problem():
     return ho.build_problem(mg.complex_system())
 
 
+def complex_hermitian(n, seed, scale=20.0):
+    rng = np.random.default_rng(seed)
+    im = np.zeros((n, n))
+    iu = np.triu_indices(n, 1)
+    im[iu] = rng.normal(0.0, scale, size=len(iu[0]))
+    return ho.synthetic_hamiltonian(n, seed) + 1j * (im - im.T)
+
+
+def ring_shared_problem(n, m, depth, seed):
+    """Every site coupled to its own bath and its neighbour's (two baths per site)."""
+    coupling = np.array([[i, (i + 1) % n] for i in range(n)], np.int32)
+    lam = [35.0 + 2.0 * i for i in range(n)]
+    invnu = [50.0 + 3.0 * i for i in range(n)]
+    return ho.build_problem(ho.make_system(ho.synthetic_hamiltonian(n, seed), lam, invnu, [0.0] * n, m,
+                                           300.0, depth, coupling=coupling))
+
+
 CASES = {
     "cfg1_real_m1": lambda: ho.build_problem(ho.drude_system(7, 4, 1, seed=11)),
     "cfg2_small_m2": lambda: ho.build_problem(ho.drude_system(8, 3, 2, seed=22)),
@@ -48,6 +65,13 @@ CASES = {
     "n12_m1": lambda: ho.build_problem(ho.drude_system(12, 2, 1, seed=5)),
     "n1": lambda: ho.build_problem(ho.drude_system(1, 5, 2, seed=6)),
     "n16_m1": lambda: ho.build_problem(ho.drude_system(16, 1, 1, seed=7)),
+    "n10_m2": lambda: ho.build_problem(ho.drude_system(10, 2, 2, seed=8)),
+    "n13_m1": lambda: ho.build_problem(ho.drude_system(13, 2, 1, seed=9)),
+    "n11_m2_complex": lambda: ho.build_problem(ho.make_system(complex_hermitian(11, 10), [35.0] * 11,
+                                                              [50.0] * 11, [0.0] * 11, 2, 300.0, 2)),
+    "n15_m1_complex": lambda: ho.build_problem(ho.make_system(complex_hermitian(15, 12), [35.0] * 15,
+                                                              [50.0] * 15, [0.0] * 15, 1, 300.0, 2)),
+    "n9_ring_shared_m2": lambda: ring_shared_problem(9, 2, 2, 13),
     "m3_t77": lambda: ho.build_problem(ho.make_system(ho.synthetic_hamiltonian(4, 9), [35] * 4,
                                                       [50] * 4, [0] * 4, 3, 77.0, 3)),
 }
