@@ -89,10 +89,6 @@ struct PairParams {
     const int32_t* __restrict__ nbr; // [nodes][NW]: plus[W], minus[W], padded to NW (multiple of 4)
     const uint8_t* __restrict__ tup; // [nodes][TWB] tuple bytes, padded to TWB (multiple of 16)
     const double2* __restrict__ pss; // [nodes]
-    const double* __restrict__ cplus;  // [W][LS]
-    const double2* __restrict__ kmin;  // [3][W][LS]: kappa_i, kappa_j, kappa_d
-    const double2* __restrict__ hs;    // [n_inst][N*N] H / hbar (complex H, SIMT kernel)
-    const double* __restrict__ hr;     // [n_inst][N*(N+1)] real symmetric H / hbar, padded rows (SIMT kernel)
     const double* __restrict__ hfrag;  // [n_inst][frag_doubles(N)] MMA operand fragments of H / hbar
     const int32_t* __restrict__ inst;  // [nodes] instance of each ADO; NULL when the handle holds one instance
     const double2* __restrict__ gamma0;// [N*N]
@@ -126,9 +122,16 @@ __host__ __device__ constexpr int tile_pos(int n, int i, int k) { return i * til
 constexpr int kXchStride = 17;
 constexpr int kXchBytes = 16 * kXchStride * 16;
 
+// shared look-up tables of both stage kernels: khat 3*W double2, chat W doubles,
+// sqrt LS+1 doubles, pos W int16 (the last read by the team kernel only)
+__host__ __device__ inline int dmma_lut_bytes(int W, int LS)
+{
+    return ((3 * W * 16 + W * 8 + (LS + 1) * 8 + W * 2) + 15) & ~15;
+}
+
 // dynamic shared memory carve-up (bytes); everything 16-B aligned
 struct PairSmem {
-    int lut;     // kmin 3*W*LS double2 + cplus W*LS doubles
+    int lut;     // coefficient tables (dmma_lut_bytes)
     int team;    // per team: 2 slots + the exchange tile
     int slot;    // per slot: tile + nbr + tup + pss
     int tile_off, nbr_off, tup_off, pss_off, xch_off;
@@ -137,8 +140,7 @@ struct PairSmem {
 __host__ __device__ inline PairSmem pair_smem_layout(int n, int W, int NW, int TWB, int LS)
 {
     PairSmem s;
-    const int lut = 3 * W * LS * 16 + W * LS * 8;
-    s.lut = (lut + 15) & ~15;
+    s.lut = dmma_lut_bytes(W, LS);
     const int tile = n * tile_stride(n) * 16;
     s.tile_off = 0;
     s.nbr_off = tile;
@@ -311,11 +313,6 @@ __host__ __device__ inline int dmma_slot_bytes(int P, int NW, int TWB)
 __host__ __device__ inline int dmma_warp_bytes(int P, int NW, int TWB)
 {
     return 2 * dmma_slot_bytes(P, NW, TWB) + 64 * 16 /* exchange tile */ + 16 /* 2 mbarriers */;
-}
-// shared look-up tables of the DMMA kernel: khat 3*W double2, chat W doubles, sqrt LS+1 doubles
-__host__ __device__ inline int dmma_lut_bytes(int W, int LS)
-{
-    return ((3 * W * 16 + W * 8 + (LS + 1) * 8) + 15) & ~15;
 }
 __host__ inline size_t dmma_smem_bytes(int P, int W, int NW, int TWB, int LS)
 {
@@ -592,8 +589,10 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_dmma_stage(const DmmaP
 // fragment hb(J, s); ha(I, s) against B = w(4s+t, 8J+g)).  Warp wt of the
 // team computes blocks [4 wt / TW, 4 (wt+1) / TW) and writes them to the
 // team's exchange tile; after a team barrier every owner reads the two
-// elements of its sector.  The bath terms follow the same formulas as the
-// DMMA kernel, one 32-byte sector load per neighbour.
+// elements of its sector.  (Cutting the work finer, into the real and
+// imaginary parts of each block, balances the warps of a three-warp team but
+// doubles the operand reads and measured slower.)  The bath terms follow the
+// same formulas as the DMMA kernel, one 32-byte sector load per neighbour.
 // ---------------------------------------------------------------------------
 
 // issue the asynchronous copies of ADO u into a team slot
@@ -615,11 +614,12 @@ __device__ __forceinline__ void prefetch_ado(unsigned char* slot, const PairPara
     if (lt == 0) cp_async16(slot + L.pss_off, p.pss + u);
 }
 
-// ADJ: the adjoint operator L^H (see heom_dmma_stage); the coefficient
-// tables are indexed by the tuple entry n: cplus(n) = chat sqrt(n+1) and
-// kappa(n) = khat sqrt(n), so L^H takes cplus(n-1) and conj(kappa(n+1)).
+// ADJ: the adjoint operator L^H (see heom_dmma_stage).  The bath
+// coefficients are the factored tables of heom_dmma_stage (CoefTabs).
+// (three CTAs per SM where at most two slots per state keep the register
+// demand low enough; two otherwise)
 template <int N, int HK, int SLT, bool ADJ>
-__global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_pair_stage(const PairParams p)
+__global__ void __launch_bounds__(kCtaWarps * 32, SLT <= 2 ? 3 : 2) heom_pair_stage(const DmmaParams dp)
 {
     static_assert(N > 8 && N <= 16, "team kernel handles N = 9..16");
     constexpr int P = pairs_of(N);
@@ -629,14 +629,18 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_pair_stage(const PairP
     constexpr int KS = (N + 3) / 4; // k-slices of the padded commutator
     constexpr int FD = frag_doubles(N);
     extern __shared__ __align__(128) unsigned char smem[];
+    const PairParams& p = dp.p;
     const PairSmem L = pair_smem_layout(N, p.W, p.NW, p.TWB, p.LS);
     const int W = p.W, LS = p.LS, SL = p.SL;
 
-    // look-up tables shared by the CTA; 16-byte arrays first (all offsets multiples of 16)
-    double2* s_kmin = reinterpret_cast<double2*>(smem);              // 3 * W * LS
-    double* s_cplus = reinterpret_cast<double*>(s_kmin + 3 * W * LS); // W * LS
-    for (int q = threadIdx.x; q < W * LS; q += blockDim.x) s_cplus[q] = p.cplus[q];
-    for (int q = threadIdx.x; q < 3 * W * LS; q += blockDim.x) s_kmin[q] = p.kmin[q];
+    double2* s_kh = reinterpret_cast<double2*>(smem);      // 3 * W
+    double* s_ch = reinterpret_cast<double*>(s_kh + 3 * W); // W
+    double* s_sq = s_ch + W;                                // LS + 1
+    int16_t* s_pos = reinterpret_cast<int16_t*>(s_sq + LS + 1); // W
+    for (int q = threadIdx.x; q < 3 * W; q += blockDim.x) s_kh[q] = dp.ct.khat[q];
+    for (int q = threadIdx.x; q < W; q += blockDim.x) s_ch[q] = dp.ct.chat[q];
+    for (int q = threadIdx.x; q <= LS; q += blockDim.x) s_sq[q] = dp.ct.sq[q];
+    for (int q = threadIdx.x; q < W; q += blockDim.x) s_pos[q] = dp.ct.pos[q];
 
     const int team = threadIdx.x / TT;
     const int lt = threadIdx.x - team * TT;
@@ -658,10 +662,10 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_pair_stage(const PairP
         slj[q] = (active && q < SL) ? p.slots[j * SL + q] : -1;
     }
     // coefficient tables seen by the two elements of this sector
-    const double2* kap_i1 = s_kmin + (diag ? 2 : 0) * W * LS; // element 1, slots of site i
-    const double2* kap_j1 = s_kmin + 1 * W * LS;              // element 1, slots of site j (off-diagonal)
-    const double2* kap_i2 = s_kmin + 1 * W * LS;              // element 2 = (j,i), slots of site i (its j side)
-    const double2* kap_j2 = s_kmin + (diag ? 2 : 0) * W * LS; // element 2, slots of site j
+    const double2* kap_i1 = s_kh + (diag ? 2 : 0) * W; // element 1, slots of site i
+    const double2* kap_j1 = s_kh + 1 * W;              // element 1, slots of site j (off-diagonal)
+    const double2* kap_i2 = s_kh + 1 * W;              // element 2 = (j,i), slots of site i (its j side)
+    const double2* kap_j2 = s_kh + (diag ? 2 : 0) * W; // element 2, slots of site j
 
     __syncthreads();
     if (team >= TEAMS) return;
@@ -740,18 +744,13 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_pair_stage(const PairP
 #pragma unroll
             for (int sd = 0; sd < 2; ++sd) {
                 double2 xp[SLT][2], xm[SLT][2];
-                int ix[SLT], ik[SLT];
+                int nn[SLT];
 #pragma unroll
                 for (int q = 0; q < SLT; ++q) {
                     const int sl = sd == 0 ? sli[q] : slj[q];
                     const int32_t vp = (sl >= 0 && (ADJ || !diag)) ? nb[sl] : -1;
                     const int32_t vm = (sl >= 0 && (!ADJ || !diag)) ? nb[W + sl] : -1;
-                    ix[q] = sl >= 0 ? (sl * LS + tu[sl]) : 0;
-                    ik[q] = ix[q];
-                    if (ADJ) { // table entries of L^H: cplus at n-1 (minus neighbour), kappa at n+1 (plus neighbour)
-                        ik[q] = vp >= 0 ? ix[q] + 1 : ix[q];
-                        ix[q] = vm >= 0 ? ix[q] - 1 : ix[q];
-                    }
+                    nn[q] = sl >= 0 ? tu[sl] : 0;
                     xp[q][0] = xp[q][1] = xm[q][0] = xm[q][1] = make_double2(0.0, 0.0);
                     if (vp >= 0) ld256(p.in + (int64_t)vp * (2 * P) + 2 * lt, xp[q][0], xp[q][1]);
                     if (vm >= 0) ld256(p.in + (int64_t)vm * (2 * P) + 2 * lt, xm[q][0], xm[q][1]);
@@ -760,13 +759,18 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_pair_stage(const PairP
                 for (int q = 0; q < SLT; ++q) {
                     const int sl = sd == 0 ? sli[q] : slj[q];
                     if (sl < 0) continue;
-                    // L: i-coefficient on the plus neighbour, kappa on the minus one;
-                    // L^H: -i cplus(n-1) on the minus neighbour, conj(kappa(n+1)) on the plus one
-                    const double c = diag ? 0.0 : (ADJ ? -s_cplus[ix[q]] : s_cplus[ix[q]]);
+                    const int ps = s_pos[sl];
+                    const double sq_lo = s_sq[nn[q]], sq_hi = s_sq[nn[q] + 1];
+                    // L: i chat sqrt(n+1) on the plus neighbour, khat sqrt(n) on the minus one;
+                    // L^H: -i chat sqrt(n) on the minus neighbour, conj(khat) sqrt(n+1) on the plus one
+                    const double c = diag ? 0.0 : (ADJ ? -s_ch[ps] * sq_lo : s_ch[ps] * sq_hi);
+                    const double sk = ADJ ? sq_hi : sq_lo;
                     const double2 t1 = ADJ ? xm[q][0] : xp[q][0], t2 = ADJ ? xm[q][1] : xp[q][1];
                     const double2 k1 = ADJ ? xp[q][0] : xm[q][0], k2 = ADJ ? xp[q][1] : xm[q][1];
+                    const double2 m1 = make_double2(k1.x * sk, k1.y * sk);
+                    const double2 m2 = make_double2(k2.x * sk, k2.y * sk);
                     auto kap = [&](const double2* tab) {
-                        const double2 v = tab[ik[q]];
+                        const double2 v = tab[ps];
                         return ADJ ? make_double2(v.x, -v.y) : v;
                     };
                     if (sd == 0) {
@@ -775,16 +779,16 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_pair_stage(const PairP
                         L1.y = fma(c, t1.x, L1.y);
                         L2.x = fma(c, t2.y, L2.x);
                         L2.y = fma(-c, t2.x, L2.y);
-                        cmac(L1, kap(kap_i1), k1);
-                        if (!diag) cmac(L2, kap(kap_i2), k2);
+                        cmac(L1, kap(kap_i1), m1);
+                        if (!diag) cmac(L2, kap(kap_i2), m2);
                     } else {
                         // site j: element 1 j-side (-i c, kappa_j); element 2 i-side (+i c, kappa_i)
                         L1.x = fma(c, t1.y, L1.x);
                         L1.y = fma(-c, t1.x, L1.y);
                         L2.x = fma(-c, t2.y, L2.x);
                         L2.y = fma(c, t2.x, L2.y);
-                        if (!diag) cmac(L1, kap(kap_j1), k1);
-                        cmac(L2, kap(kap_j2), k2);
+                        if (!diag) cmac(L1, kap(kap_j1), m1);
+                        cmac(L2, kap(kap_j2), m2);
                     }
                 }
             }
@@ -1145,7 +1149,6 @@ struct FieldParams {
     double* time;          // step mode: device time of the propagation state (advanced by dt)
     double t0, dt;         // explicit mode: the evaluation time t0 (time == nullptr)
     double2* hs_t;         // [nt][K][N*N]
-    double* hr_t;          // [nt][K][N*(N+1)]
     double* frag_t;        // [nt][K][frag_doubles(N)]
     int K, N, nt;
 };
@@ -1180,7 +1183,6 @@ __global__ void heom_field_tables(const FieldParams f)
                 const double re = h.x - (E.x * dm.x - E.y * dm.y) - (E.x * dp.x + E.y * dp.y);
                 const double im = h.y - (E.x * dm.y + E.y * dm.x) - (E.x * dp.y - E.y * dp.x);
                 hs[q] = make_double2(re, im);
-                f.hr_t[((size_t)s * f.K + k) * N * (N + 1) + (q / N) * (N + 1) + q % N] = re;
             }
             __syncthreads();
             {

@@ -91,8 +91,8 @@ struct DevBuf {
     }
 };
 
-typedef void (*stage_fn_t)(const PairParams);
 typedef void (*dmma_fn_t)(const heomk::DmmaParams);
+typedef dmma_fn_t stage_fn_t;
 
 template <int N, int HK, bool ADJ>
 stage_fn_t pick_slt(int slt)
@@ -172,14 +172,10 @@ struct AdjTabs {
     const double2* pss;    // conj(pf_same_sum)
     const double2* gamma0; // conj(gamma0)
     const double* hfrag;   // fragments of -H^H
-    const double* hr;      // -H (real symmetric H)
-    const double2* hs;     // -H^H
     bool adjoint = true;
     // optional bath-coefficient tables (flow tracking: a zero table switches a term off)
-    const double* chat = nullptr;   // DMMA kernel
+    const double* chat = nullptr;
     const double2* khat = nullptr;
-    const double* cplus = nullptr;  // SIMT kernel
-    const double2* kmin = nullptr;
 };
 
 // stage write modes (runtime parameters of the one stage kernel)
@@ -247,11 +243,10 @@ struct heom_handle {
     // device tables
     DevBuf<int32_t> d_nbr;
     DevBuf<uint8_t> d_tup;
-    DevBuf<double2> d_pss, d_kmin, d_hs, d_gamma0;
-    DevBuf<double> d_hr, d_hfrag;    // per-instance H for the SIMT / DMMA kernels
+    DevBuf<double2> d_pss, d_hs, d_gamma0;
+    DevBuf<double> d_hfrag;          // per-instance MMA fragments of H / hbar
     DevBuf<int32_t> d_inst;          // instance of each internal ADO (n_inst > 1)
     DevBuf<int64_t> d_top;
-    DevBuf<double> d_cplus;
     DevBuf<int16_t> d_slots;
     DevBuf<double> d_chat, d_sq;     // factored coefficients (DMMA kernel)
     DevBuf<double2> d_khat;
@@ -282,7 +277,7 @@ struct heom_handle {
     heomk::Pulse pulses[2] = {};
     DevBuf<double2> d_dplus, d_dminus;     // D+ / hbar, D- / hbar
     DevBuf<double2> field_hs;              // [3][K][N*N]
-    DevBuf<double> field_hr, field_frag;   // [3][K][N*(N+1)], [3][K][frag_doubles(N)]
+    DevBuf<double> field_frag;             // [3][K][frag_doubles(N)]
     DevBuf<double> d_time;                 // time of the propagation state (device, advanced by field steps)
     double time = 0.0;                     // host mirror
 
@@ -350,15 +345,11 @@ int build_neighbours(heom_handle* h)
 }
 
 // device-side forms of one instance's H (interleaved re/im, J): H / hbar
-// row-major (hs), its real part in padded rows (hr) and the MMA operand
-// fragments (frag, heomk::frag_index: lane l = 4g + t, block b, k-slice s,
+// row-major (hs) and the MMA operand fragments (frag, heomk::frag_index: lane l = 4g + t, block b, k-slice s,
 // row r = 8b + g, column c = 4s + t; hb = H(c, r), ha = -H(r, c); zero outside N x N)
-void h_tables(const double* hk, int N, double2* hs, double* hr, double* frag)
+void h_tables(const double* hk, int N, double2* hs, double* frag)
 {
-    for (int q = 0; q < N * N; ++q) {
-        hs[q] = make_double2(hk[2 * q] / kHbar, hk[2 * q + 1] / kHbar);
-        hr[(q / N) * (N + 1) + q % N] = hk[2 * q] / kHbar;
-    }
+    for (int q = 0; q < N * N; ++q) hs[q] = make_double2(hk[2 * q] / kHbar, hk[2 * q + 1] / kHbar);
     for (int b = 0; b < heomk::frag_blocks(N); ++b)
         for (int sl = 0; sl < heomk::frag_slices(N); ++sl)
             for (int l = 0; l < 32; ++l) {
@@ -407,14 +398,12 @@ int upload_hamiltonian(heom_handle* h)
 {
     const int N = h->N, K = h->n_inst;
     std::vector<double2> hs((size_t)K * N * N);
-    std::vector<double> hr((size_t)K * N * (N + 1), 0.0);
     const size_t fd = heomk::frag_doubles(N);
     std::vector<double> frag((size_t)K * fd, 0.0);
     bool real_sym = true;
     for (int k = 0; k < K; ++k) {
         const double* hk = h->ham.data() + (size_t)k * 2 * N * N;
-        h_tables(hk, N, hs.data() + (size_t)k * N * N, hr.data() + (size_t)k * N * (N + 1),
-                 frag.data() + (size_t)k * fd);
+        h_tables(hk, N, hs.data() + (size_t)k * N * N, frag.data() + (size_t)k * fd);
         real_sym = real_sym && real_symmetric(hk, N);
     }
     // real symmetric H (every instance) takes the cheaper kernel variants; a
@@ -423,12 +412,10 @@ int upload_hamiltonian(heom_handle* h)
     const std::vector<double2> g0 = gamma0_table(h, h->pf_same);
     if (!h->d_hs.p) {
         if (int rc = h->d_hs.alloc(hs.size())) return rc;
-        if (int rc = h->d_hr.alloc(hr.size())) return rc;
         if (int rc = h->d_hfrag.alloc(frag.size())) return rc;
         if (int rc = h->d_gamma0.alloc(N * N)) return rc;
     }
     CUDA_TRY(cudaMemcpy(h->d_hs.p, hs.data(), hs.size() * 16, cudaMemcpyHostToDevice));
-    CUDA_TRY(cudaMemcpy(h->d_hr.p, hr.data(), hr.size() * 8, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(h->d_hfrag.p, frag.data(), frag.size() * 8, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(h->d_gamma0.p, g0.data(), g0.size() * 16, cudaMemcpyHostToDevice));
     // the kernel variant may change: rebuild the cached step graph
@@ -442,25 +429,6 @@ int upload_hamiltonian(heom_handle* h)
 int upload_coefficients(heom_handle* h)
 {
     const int W = h->W, LS = h->LS, M = h->M;
-    std::vector<double> cplus((size_t)W * LS, 0.0);
-    std::vector<double2> kmin((size_t)3 * W * LS, make_double2(0.0, 0.0));
-    for (int sl = 0; sl < W; ++sl) {
-        const int b = sl / M;
-        const int m = sl - b * M;
-        const double cr = h->cbk[2 * sl], ci = h->cbk[2 * sl + 1];
-        const double qr = m == 0 ? h->pf_circ[2 * b] : 0.0;
-        const double qi = m == 0 ? h->pf_circ[2 * b + 1] : 0.0;
-        const double habs = std::hypot(cr, ci);
-        for (int n = 0; n < LS; ++n) {
-            cplus[sl * LS + n] = std::sqrt((n + 1.0) * habs / kHbar); // heom_ode.cl:211
-            const double sc = std::sqrt(n / habs * kHbar);             // heom_ode.cl:321
-            const double kir = sc * (-ci / kHbar + qr), kii = sc * (cr / kHbar + qi);
-            const double kjr = sc * (ci / kHbar + qr), kji = sc * (-cr / kHbar + qi);
-            kmin[0 * W * LS + sl * LS + n] = make_double2(kir, kii);
-            kmin[1 * W * LS + sl * LS + n] = make_double2(kjr, kji);
-            kmin[2 * W * LS + sl * LS + n] = make_double2(2.0 * sc * qr, 2.0 * sc * qi);
-        }
-    }
     // slots of each state: b * M + m for every bath b coupled to the state
     std::vector<int16_t> slots((size_t)h->N * h->SL, (int16_t)-1);
     for (int s = 0; s < h->N; ++s) {
@@ -500,11 +468,7 @@ int upload_coefficients(heom_handle* h)
         CUDA_TRY(cudaMemcpy(h->d_sq.p, sq.data(), (LS + 1) * 8, cudaMemcpyHostToDevice));
         CUDA_TRY(cudaMemcpy(h->d_pos.p, pos.data(), W * 2, cudaMemcpyHostToDevice));
     }
-    if (int rc = h->d_cplus.alloc(cplus.size())) return rc;
-    if (int rc = h->d_kmin.alloc(kmin.size())) return rc;
     if (int rc = h->d_slots.alloc(slots.size())) return rc;
-    CUDA_TRY(cudaMemcpy(h->d_cplus.p, cplus.data(), cplus.size() * 8, cudaMemcpyHostToDevice));
-    CUDA_TRY(cudaMemcpy(h->d_kmin.p, kmin.data(), kmin.size() * 16, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(h->d_slots.p, slots.data(), slots.size() * 2, cudaMemcpyHostToDevice));
     return 0;
 }
@@ -515,10 +479,6 @@ PairParams base_params(const heom_handle* h)
     p.nbr = h->d_nbr.p;
     p.tup = h->d_tup.p;
     p.pss = h->d_pss.p;
-    p.cplus = h->d_cplus.p;
-    p.kmin = h->d_kmin.p;
-    p.hs = h->d_hs.p;
-    p.hr = h->d_hr.p;
     p.hfrag = h->d_hfrag.p;
     p.inst = h->n_inst > 1 ? h->d_inst.p : nullptr;
     p.gamma0 = h->d_gamma0.p;
@@ -601,10 +561,6 @@ int launch_stage(heom_handle* h, int epi, const double2* in, const double2* y, d
         p.pss = adj->pss;
         p.gamma0 = adj->gamma0;
         p.hfrag = adj->hfrag;
-        p.hr = adj->hr;
-        p.hs = adj->hs;
-        if (adj->cplus) p.cplus = adj->cplus;
-        if (adj->kmin) p.kmin = adj->kmin;
     }
     p.in = in;
     p.out = out;
@@ -640,19 +596,15 @@ int launch_stage(heom_handle* h, int epi, const double2* in, const double2* y, d
         p.acc_init = acc_init;
         break;
     }
-    if (h->N <= 8) {
-        heomk::DmmaParams dp;
-        dp.p = p;
-        dp.lt = h->lane_tab;
-        dp.ct.chat = adj && adj->chat ? adj->chat : h->d_chat.p;
-        dp.ct.khat = adj && adj->khat ? adj->khat : h->d_khat.p;
-        dp.ct.sq = h->d_sq.p;
-        dp.ct.pos = h->d_pos.p;
-        dp.err = h->d_err.p;
-        ((dmma_fn_t)fn)<<<blocks, heomk::kCtaWarps * 32, h->stage_smem, h->stream>>>(dp);
-    } else {
-        ((stage_fn_t)fn)<<<blocks, cta_threads(h->N), h->stage_smem, h->stream>>>(p);
-    }
+    heomk::DmmaParams dp;
+    dp.p = p;
+    dp.lt = h->lane_tab;
+    dp.ct.chat = adj && adj->chat ? adj->chat : h->d_chat.p;
+    dp.ct.khat = adj && adj->khat ? adj->khat : h->d_khat.p;
+    dp.ct.sq = h->d_sq.p;
+    dp.ct.pos = h->d_pos.p;
+    dp.err = h->d_err.p;
+    ((dmma_fn_t)fn)<<<blocks, h->N <= 8 ? heomk::kCtaWarps * 32 : cta_threads(h->N), h->stage_smem, h->stream>>>(dp);
     h->launches++;
     CUDA_TRY(cudaGetLastError());
     return 0;
@@ -697,7 +649,6 @@ heomk::FieldParams field_params(heom_handle* h, int nt)
     f.pulse[0] = h->pulses[0];
     f.pulse[1] = h->pulses[1];
     f.hs_t = h->field_hs.p;
-    f.hr_t = h->field_hr.p;
     f.frag_t = h->field_frag.p;
     f.K = h->n_inst;
     f.N = h->N;
@@ -712,8 +663,6 @@ AdjTabs field_tabs(const heom_handle* h, int s)
     t.pss = h->d_pss.p;
     t.gamma0 = h->d_gamma0.p;
     t.hfrag = h->field_frag.p + (size_t)s * h->n_inst * heomk::frag_doubles(h->N);
-    t.hr = h->field_hr.p + (size_t)s * h->n_inst * h->N * (h->N + 1);
-    t.hs = h->field_hs.p + (size_t)s * h->n_inst * h->N * h->N;
     t.adjoint = false;
     return t;
 }
@@ -1371,10 +1320,8 @@ int heom_set_field(heom_handle* h, const double* dipole_plus, const double* dipo
         if (int rc = h->d_dplus.alloc(N * N)) return rc;
         if (int rc = h->d_dminus.alloc(N * N)) return rc;
         if (int rc = h->field_hs.alloc((size_t)3 * K * N * N)) return rc;
-        if (int rc = h->field_hr.alloc((size_t)3 * K * N * (N + 1))) return rc;
         if (int rc = h->field_frag.alloc((size_t)3 * K * heomk::frag_doubles(N))) return rc;
         if (int rc = h->d_time.alloc(1)) return rc;
-        CUDA_TRY(cudaMemset(h->field_hr.p, 0, (size_t)3 * K * N * (N + 1) * 8));
     }
     CUDA_TRY(cudaMemcpy(h->d_dplus.p, dp.data(), N * N * 16, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(h->d_dminus.p, dm.data(), N * N * 16, cudaMemcpyHostToDevice));
@@ -1571,20 +1518,14 @@ int heom_solve(heom_handle* h, double time, double step_size, const heom_buffer*
             t.pss = z2;
             t.gamma0 = z2;
             t.hfrag = z1;
-            t.hr = z1;
-            t.hs = z2;
             t.adjoint = false;
             if (part == 0) {
                 t.khat = z2;
-                t.kmin = z2;
             } else {
                 t.chat = z1;
-                t.cplus = z1;
             }
             if (tabs) { // keep the time-dependent H out of the bath terms too
                 t.hfrag = z1;
-                t.hr = z1;
-                t.hs = z2;
             }
             rc = launch_stage(h, EPI_ACC, in->data.p, nullptr, h->flow_scratch.p, dst->data.p,
                               make_double2(acc_coeff, 0.0), 0, &t);
@@ -2362,8 +2303,8 @@ void* heom_ensemble_stream(heom_ensemble* e) { return e ? (void*)e->stream : nul
 struct heom_adjoint {
     heom_handle* h = nullptr;
     AdjTabs tabs{};
-    DevBuf<double2> pss_adj, g0_adj, hs_adj;
-    DevBuf<double> hfrag_adj, hr_adj;
+    DevBuf<double2> pss_adj, g0_adj;
+    DevBuf<double> hfrag_adj;
     DevBuf<double> dpss;       // [nodes] d pf_same_sum / d gamma (internal order)
     DevBuf<double2> dg0;       // [2][N*N]
     DevBuf<double> dchat;      // [2][W]
@@ -2412,9 +2353,9 @@ int adj_tables(heom_adjoint* A, const heomhost::system_params& sp)
         pss[h->int_of_ref[r]] = make_double2(h->pss[2 * r], -h->pss[2 * r + 1]);
     std::vector<double2> g0 = gamma0_table(h, h->pf_same);
     for (auto& v : g0) v.y = -v.y;
-    std::vector<double2> hs((size_t)K * N * N);
+    std::vector<double2> hs((size_t)N * N);
     const size_t fd = heomk::frag_doubles(N);
-    std::vector<double> hr((size_t)K * N * (N + 1), 0.0), frag((size_t)K * fd, 0.0), hadj(2 * N * N);
+    std::vector<double> frag((size_t)K * fd, 0.0), hadj(2 * N * N);
     for (int k = 0; k < K; ++k) {
         const double* hk = h->ham.data() + (size_t)k * 2 * N * N;
         for (int i = 0; i < N; ++i)
@@ -2422,20 +2363,15 @@ int adj_tables(heom_adjoint* A, const heomhost::system_params& sp)
                 hadj[2 * (i * N + j)] = -hk[2 * (j * N + i)];
                 hadj[2 * (i * N + j) + 1] = hk[2 * (j * N + i) + 1];
             }
-        h_tables(hadj.data(), N, hs.data() + (size_t)k * N * N, hr.data() + (size_t)k * N * (N + 1),
-                 frag.data() + (size_t)k * fd);
+        h_tables(hadj.data(), N, hs.data(), frag.data() + (size_t)k * fd);
     }
     if (int rc = A->pss_adj.alloc(pss.size())) return rc;
     if (int rc = A->g0_adj.alloc(g0.size())) return rc;
-    if (int rc = A->hs_adj.alloc(hs.size())) return rc;
-    if (int rc = A->hr_adj.alloc(hr.size())) return rc;
     if (int rc = A->hfrag_adj.alloc(frag.size())) return rc;
     CUDA_TRY(cudaMemcpy(A->pss_adj.p, pss.data(), pss.size() * 16, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(A->g0_adj.p, g0.data(), g0.size() * 16, cudaMemcpyHostToDevice));
-    CUDA_TRY(cudaMemcpy(A->hs_adj.p, hs.data(), hs.size() * 16, cudaMemcpyHostToDevice));
-    CUDA_TRY(cudaMemcpy(A->hr_adj.p, hr.data(), hr.size() * 8, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemcpy(A->hfrag_adj.p, frag.data(), frag.size() * 8, cudaMemcpyHostToDevice));
-    A->tabs = AdjTabs{A->pss_adj.p, A->g0_adj.p, A->hfrag_adj.p, A->hr_adj.p, A->hs_adj.p};
+    A->tabs = AdjTabs{A->pss_adj.p, A->g0_adj.p, A->hfrag_adj.p};
 
     // derivative tables for theta = lambda (0), gamma (1)
     heomhost::bath_derivs bd = heomhost::bath_derivatives(sp);
