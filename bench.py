@@ -509,10 +509,12 @@ def run_adjoint(args, rank, local_rank):
 
 def run_uneven_adjoint(args, rank, local_rank):
     """Gradients of every instance's time-integrated site-0 population w.r.t.
-    its site energies for the uneven batch: one batch adjoint per class
-    (instances sharing states and baths), classes whose checkpoint memory
-    does not fit skipped and counted.  Compared with central differences of
-    the site energies (two forward solves per site), timed on a sample."""
+    its site energies for the uneven batch: one batch adjoint per group of a
+    class (instances sharing states and baths, packed while the group's
+    sqrt(T) checkpoint layout fits); an instance whose layout alone does not
+    fit runs alone, the library then reversing it by recursive checkpointing
+    in the memory there is.  Compared with central differences of the site
+    energies (two forward solves per site), timed on a sample."""
     import torch
     import heom_b200 as hb
     if rank != 0:
@@ -528,12 +530,30 @@ def run_uneven_adjoint(args, rank, local_rank):
     free = torch.cuda.mem_get_info()[0]
     S = max(1, int(np.ceil(np.sqrt(steps))))
     nstates = (steps + S - 1) // S + 4 * S + 3 + 4  # checkpoints, stage inputs, adjoint, product-form stages
-    covered, skipped, t_adj, nodes_done, grads = [], [], 0.0, 0, {}
+    min_states = 7 + 4 + 8  # recursive sweep: stage inputs and adjoint, product-form stages, 8 slots
+    covered, skipped, t_adj, nodes_done, grads, recursive = [], [], 0.0, 0, {}, []
     from math import comb
+
+    def ados(k):
+        return comb(systems[k].sites * systems[k].matsubaras + systems[k].depth, systems[k].depth)
+
+    groups = []
     for (n, m), members in sorted(classes.items()):
         P = n * (n - 1) // 2 + (n + 1) // 2
-        nodes = sum(comb(n * m + systems[k].depth, systems[k].depth) for k in members)
-        if nstates * nodes * P * 32 > 0.85 * free:
+        group = []
+        for k in sorted(members, key=ados):
+            if nstates * (sum(ados(q) for q in group) + ados(k)) * P * 32 <= 0.85 * free:
+                group.append(k)
+                continue
+            if group:
+                groups.append(group)
+            group = [k]
+        groups.append(group)
+    for members in groups:
+        n = systems[members[0]].sites
+        P = n * (n - 1) // 2 + (n + 1) // 2
+        nodes = sum(ados(k) for k in members)
+        if min_states * nodes * P * 32 > 0.85 * free:
             skipped += members
             continue
         rho0 = np.zeros((n, n), complex)
@@ -546,12 +566,16 @@ def run_uneven_adjoint(args, rank, local_rank):
             t0 = time.perf_counter()
             out = A.gradient(rho0, obs, w, dt, steps)
             t_adj += time.perf_counter() - t0
+            if A.recursive_slots():
+                recursive.append({"instances": members, "gb_per_state": nodes * P * 32 / 1e9,
+                                  "slots": A.recursive_slots()})
         for q, k in enumerate(members):
             grads[k] = np.diag(out["h"][q].real).copy()
         covered += members
         nodes_done += nodes
     # central differences for a sample of covered instances (two solves per site energy)
-    sample = covered[:: max(1, len(covered) // 6)][:6]
+    small = [k for k in covered if ados(k) <= 1_000_000]  # FD solves timed on instances of <= 1 M ADOs
+    sample = small[:: max(1, len(small) // 6)][:6]
     t_fd_sample, fd_err, fd_sites = 0.0, 0.0, 0
     for k in sample:
         sysd = systems[k]
@@ -591,9 +615,9 @@ def run_uneven_adjoint(args, rank, local_rank):
             "data": "synthetic (seeded H, Drude-Lorentz baths)",
             "config": {"workload": f"adjoint of the uneven batch ({count} instances, seed {UNEVEN_SEED}): gradient of "
                                    f"each instance's time-integrated site-0 population w.r.t. its site energies, "
-                                   f"{steps} steps of 1 fs, one batch adjoint per class",
+                                   f"{steps} steps of 1 fs, one batch adjoint per group of a class",
                        "instances_covered": len(covered), "instances_skipped_memory": len(skipped),
-                       "classes": len(classes), "parallelism": "single"},
+                       "classes": len(classes), "groups": len(groups), "parallelism": "single"},
             "uneven_adjoint": {"seconds": t_adj, "fd_seconds_estimate": fd_total,
                                "speedup_vs_fd": fd_total / max(t_adj, 1e-12),
                                "fd_note": f"central differences of {fd_sites} site energies on {len(sample)} covered "
@@ -601,8 +625,10 @@ def run_uneven_adjoint(args, rank, local_rank):
                                           f"covered site energy",
                                "max_rel_diff_vs_fd": fd_err,
                                "skipped": skipped,
-                               "memory_note": f"{nstates} states per class ({(steps + S - 1) // S} checkpoints, "
-                                              f"segments of {S} steps); classes above 85 % of free memory skipped"}}
+                               "memory_note": f"{nstates} states per group ({(steps + S - 1) // S} checkpoints, "
+                                              f"segments of {S} steps) within 85 % of free memory; larger instances "
+                                              f"alone by recursive checkpointing",
+                               "recursive": recursive}}
     print(json.dumps(line), flush=True)
 
 

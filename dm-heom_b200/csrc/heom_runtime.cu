@@ -2298,6 +2298,9 @@ void* heom_ensemble_stream(heom_ensemble* e) { return e ? (void*)e->stream : nul
 // the adjoint after F_k^H's successors, w_k the forward stage input).
 // Checkpoints every S = ceil(sqrt(steps)) steps; each segment's stage inputs
 // are recomputed (same kernels, bit-identical) before its backward sweep.
+// When those ceil(steps/S) + 4S + 3 states exceed the memory limit, the sweep
+// reverses the steps by recursive checkpointing in the slots that fit
+// (lean_reverse): same kernels, same backward order, bit-identical results.
 // ---------------------------------------------------------------------------
 
 struct heom_adjoint {
@@ -2316,6 +2319,8 @@ struct heom_adjoint {
     size_t grad_smem = 0;
     DevBuf<double2> cps, seg, scratch, ga, gb, toplog;
     int64_t cap_cps = 0, cap_seg = 0, cap_rows = 0;
+    int64_t mem_limit = 0;     // bytes for the sweep's states (0: free device memory)
+    int64_t rec_slots = 0;     // recursive-checkpointing slots of the last sweep (0: sqrt layout)
     DevBuf<double> d_w;        // loss weights [steps + 1]
     DevBuf<int64_t> d_base;    // step offset of the segment being run (read by the captured kernels)
     int64_t cap_w = 0;
@@ -2550,6 +2555,112 @@ int adj_run(heom_adjoint* A, int which, double dt, int64_t len)
     return 0;
 }
 
+// Splits of the recursive reversal.  To reverse l steps from a stored state
+// with s free slots: advance m steps, store, reverse the last l - m steps with
+// s - 1 slots, then the first m with s.  The forward steps this costs obey
+// cost(l, s) = min_m [m + cost(l - m, s - 1) + cost(m, s)], cost(1, s) = 0,
+// cost(l, 0) = l (l - 1) / 2 (every state recomputed from the stored one);
+// solved exactly while s * l^2 stays small, else by the binomial rule (with
+// r the least integer with C(s + r, s) >= l: m = l - C(s - 1 + r, s - 1)).
+struct RevPlan {
+    int64_t T = 0, S = 0;
+    bool exact = false;
+    std::vector<int32_t> best; // [s][l] optimal m (exact plan)
+
+    void build(int64_t steps, int64_t slots)
+    {
+        T = steps;
+        S = slots;
+        exact = (double)S * T * T <= 1e8;
+        if (!exact) return;
+        std::vector<int64_t> prev(T + 1), cur(T + 1);
+        best.assign((size_t)(S + 1) * (T + 1), 1);
+        for (int64_t l = 1; l <= T; ++l) prev[l] = l * (l - 1) / 2;
+        for (int64_t sl = 1; sl <= S; ++sl) {
+            cur[1] = 0;
+            for (int64_t l = 2; l <= T; ++l) {
+                int64_t bc = INT64_MAX, bm = 1;
+                for (int64_t m = 1; m < l; ++m) {
+                    const int64_t c = m + prev[l - m] + cur[m];
+                    if (c < bc) { bc = c; bm = m; }
+                }
+                cur[l] = bc;
+                best[(size_t)sl * (T + 1) + l] = (int32_t)bm;
+            }
+            std::swap(prev, cur);
+        }
+    }
+    int64_t split(int64_t l, int64_t s) const
+    {
+        if (exact) return best[(size_t)s * (T + 1) + l];
+        auto binom = [](int64_t n, int64_t k) { // C(n, k), saturating
+            long double v = 1.0L;
+            for (int64_t q = 1; q <= k; ++q) v = v * (n - k + q) / q;
+            return v > 9e18L ? INT64_MAX : (int64_t)(v + 0.5L);
+        };
+        int64_t r = 0;
+        while (binom(s + r, s) < l) ++r;
+        return std::max<int64_t>(1, std::min<int64_t>(l - 1, l - binom(s - 1 + r, s - 1)));
+    }
+};
+
+// recursive reversal: device-side step offsets come from `bases` (bases[j] = j)
+struct LeanRun {
+    heom_adjoint* A;
+    double dt;
+    const RevPlan* plan;
+    const int64_t* bases;
+    size_t st;
+
+    int set_base(int64_t j)
+    {
+        CUDA_TRY(cudaMemcpyAsync(A->d_base.p, bases + j, 8, cudaMemcpyHostToDevice, A->h->stream));
+        return 0;
+    }
+    // y <- slot, then `len` steps from step a with their tops recorded
+    int advance(int64_t sl, int64_t a, int64_t len)
+    {
+        heom_handle* h = A->h;
+        CUDA_TRY(cudaMemcpyAsync(h->y.data.p, A->cps.p + sl * st, st * 16, cudaMemcpyDeviceToDevice, h->stream));
+        if (len == 0) return 0;
+        if (int rc = set_base(a)) return rc;
+        return adj_seg_forward(A, dt, len);
+    }
+    // backward through step j from its state src: stage inputs, the top of
+    // state j + 1 (row j + 1), then the four adjoint factors and the weight of step j
+    int step_back(const double2* src, int64_t j)
+    {
+        heom_handle* h = A->h;
+        CUDA_TRY(cudaMemcpyAsync(A->seg.p, src, st * 16, cudaMemcpyDeviceToDevice, h->stream));
+        if (int rc = set_base(j)) return rc;
+        if (int rc = adj_seg_recompute(A, dt, 1)) return rc;
+        heomk::heom_record_top_at<<<h->n_inst, 128, 0, h->stream>>>(A->toplog.p, A->scratch.p, h->d_pair.p,
+                                                                    h->d_top.p, h->N, h->P, A->d_base.p, 1);
+        h->launches++;
+        CUDA_TRY(cudaGetLastError());
+        return adj_seg_backward(A, dt, 1);
+    }
+    // reverse steps [a, b) with state a in slot sl and `free` slots above it unused
+    int reverse(int64_t a, int64_t b, int64_t sl, int64_t free)
+    {
+        const int64_t l = b - a;
+        if (l == 1) return step_back(A->cps.p + sl * st, a);
+        if (free == 0) {
+            for (int64_t j = b - 1; j > a; --j) {
+                if (int rc = advance(sl, a, j - a)) return rc;
+                if (int rc = step_back(A->h->y.data.p, j)) return rc;
+            }
+            return step_back(A->cps.p + sl * st, a);
+        }
+        const int64_t m = a + plan->split(l, free);
+        if (int rc = advance(sl, a, m - a)) return rc;
+        CUDA_TRY(cudaMemcpyAsync(A->cps.p + (sl + 1) * st, A->h->y.data.p, st * 16, cudaMemcpyDeviceToDevice,
+                                 A->h->stream));
+        if (int rc = reverse(m, b, sl + 1, free - 1)) return rc;
+        return reverse(a, m, sl, free);
+    }
+};
+
 } // namespace
 
 extern "C" {
@@ -2624,19 +2735,37 @@ int heom_adjoint_gradient(heom_adjoint* A, const double* rho0, const double* obs
     CUDA_TRY(cudaSetDevice(h->device));
     const int N = h->N, NN = N * N, K = h->n_inst;
     const size_t st = h->state_elems();
-    const int64_t S = std::max<int64_t>(1, (int64_t)std::ceil(std::sqrt((double)steps)));
-    const int64_t ncp = (steps + S - 1) / S;
-    // device memory: checkpoints, stage inputs of one segment, adjoint ping-pong, one scratch state
+    int64_t S = std::max<int64_t>(1, (int64_t)std::ceil(std::sqrt((double)steps)));
+    int64_t ncp = (steps + S - 1) / S;
+    // device memory: the sqrt layout (checkpoints, stage inputs of one segment)
+    // or, when it does not fit, recursive checkpointing in the slots that do;
+    // plus the adjoint ping-pong and one scratch state
+    int64_t slots = 0;
     {
         size_t free_b = 0, total_b = 0;
         CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
-        const int64_t need_states = (ncp > A->cap_cps ? ncp : 0) + (4 * S > A->cap_seg ? 4 * S : 0) + 3;
-        if ((double)need_states * st * 16 > (double)free_b)
-            return fail(HEOM_E_NOMEM, "adjoint needs %.3f GB of device memory (%lld checkpoints, segments of %lld steps)",
-                        need_states * st * 16 / 1e9, (long long)ncp, (long long)S);
+        const double sb = (double)st * 16.0;
+        const double held = (double)(A->cap_cps + A->cap_seg + (A->ga.p ? 3 : 0)) * sb;
+        const double budget = A->mem_limit > 0 ? (double)A->mem_limit : (double)free_b + held;
+        if ((double)(ncp + 4 * S + 3) * sb > budget) {
+            slots = std::min<int64_t>((int64_t)(budget / sb) - 7, steps);
+            if (slots < 1)
+                return fail(HEOM_E_NOMEM, "adjoint needs at least 8 states of %.3f GB; %.3f GB available",
+                            sb / 1e9, budget / 1e9);
+            S = 1;
+            ncp = slots;
+        }
     }
+    A->rec_slots = slots;
     // the captured graphs hold buffer addresses: any reallocation drops them
-    if (ncp > A->cap_cps || 4 * S > A->cap_seg || steps + 1 > A->cap_rows || steps + 1 > A->cap_w) A->drop_graphs();
+    const bool shrink = slots > 0 && (A->cap_cps > ncp || A->cap_seg > 4);
+    if (shrink || ncp > A->cap_cps || 4 * S > A->cap_seg || steps + 1 > A->cap_rows || steps + 1 > A->cap_w)
+        A->drop_graphs();
+    if (shrink) { // release the sqrt layout before the recursive one takes its place
+        A->cps.reset();
+        A->seg.reset();
+        A->cap_cps = A->cap_seg = 0;
+    }
     if (ncp > A->cap_cps) {
         if (int rc = A->cps.alloc(ncp * st)) return rc;
         A->cap_cps = ncp;
@@ -2684,7 +2813,23 @@ int heom_adjoint_gradient(heom_adjoint* A, const double* rho0, const double* obs
     heomk::heom_record_top<<<K, 128, 0, h->stream>>>(A->toplog.p, h->y.data.p, h->d_pair.p, h->d_top.p, N, h->P, 0);
     h->launches++;
     CUDA_TRY(cudaGetLastError());
-    for (int64_t sgm = 0; sgm < ncp; ++sgm) {
+    std::vector<int64_t> bases;
+    if (slots > 0) {
+        // recursive checkpointing: the tops are recorded as the steps are
+        // (re)computed; the adjoint starts with the last step's weight
+        RevPlan plan;
+        plan.build(steps, slots - 1);
+        bases.resize(steps + 1);
+        for (int64_t j = 0; j <= steps; ++j) bases[j] = j;
+        CUDA_TRY(cudaMemcpyAsync(A->cps.p, h->y.data.p, st * 16, cudaMemcpyDeviceToDevice, h->stream));
+        CUDA_TRY(cudaMemsetAsync(A->partial.p, 0, (size_t)A->grid * (NN + 2) * 16, h->stream));
+        CUDA_TRY(cudaMemsetAsync(A->ga.p, 0, st * 16, h->stream));
+        LeanRun run{A, dt, &plan, bases.data(), st};
+        if (int rc = run.set_base(steps)) return rc;
+        if (int rc = adj_add_top(A, A->ga.p, 0)) return rc;
+        if (int rc = run.reverse(0, steps, 0, slots - 1)) return rc;
+    }
+    for (int64_t sgm = 0; sgm < (slots > 0 ? 0 : ncp); ++sgm) {
         const int64_t len = std::min(S, steps - sgm * S);
         CUDA_TRY(cudaMemcpyAsync(A->cps.p + sgm * st, h->y.data.p, st * 16, cudaMemcpyDeviceToDevice, h->stream));
         if (int rc = set_base(sgm)) return rc;
@@ -2706,13 +2851,15 @@ int heom_adjoint_gradient(heom_adjoint* A, const double* rho0, const double* obs
         if (loss) loss[k] = (double)J;
     }
 
-    // ---- backward ----
-    CUDA_TRY(cudaMemsetAsync(A->partial.p, 0, (size_t)A->grid * (NN + 2) * 16, h->stream));
+    // ---- backward (sqrt layout; the recursive sweep has run above) ----
     double2* gcur = A->ga.p;
-    CUDA_TRY(cudaMemsetAsync(gcur, 0, st * 16, h->stream));
-    if (int rc = set_base(ncp)) return rc; // starts[ncp] = ncp * S >= steps
-    if (int rc = adj_add_top(A, gcur, steps - ncp * S)) return rc;
-    for (int64_t sgm = ncp - 1; sgm >= 0; --sgm) {
+    if (slots == 0) {
+        CUDA_TRY(cudaMemsetAsync(A->partial.p, 0, (size_t)A->grid * (NN + 2) * 16, h->stream));
+        CUDA_TRY(cudaMemsetAsync(gcur, 0, st * 16, h->stream));
+        if (int rc = set_base(ncp)) return rc; // starts[ncp] = ncp * S >= steps
+        if (int rc = adj_add_top(A, gcur, steps - ncp * S)) return rc;
+    }
+    for (int64_t sgm = (slots > 0 ? -1 : ncp - 1); sgm >= 0; --sgm) {
         const int64_t len = std::min(S, steps - sgm * S);
         CUDA_TRY(cudaMemcpyAsync(A->seg.p, A->cps.p + sgm * st, st * 16, cudaMemcpyDeviceToDevice, h->stream));
         if (int rc = set_base(sgm)) return rc;
@@ -2746,5 +2893,14 @@ int heom_adjoint_gradient(heom_adjoint* A, const double* rho0, const double* obs
 }
 
 int64_t heom_adjoint_kernel_launches(const heom_adjoint* A) { return A && A->h ? A->h->launches : 0; }
+
+int heom_adjoint_set_memory_limit(heom_adjoint* A, int64_t bytes)
+{
+    if (!A || bytes < 0) return fail(HEOM_E_ARG, "bad argument");
+    A->mem_limit = bytes;
+    return 0;
+}
+
+int64_t heom_adjoint_recursive_slots(const heom_adjoint* A) { return A ? A->rec_slots : -1; }
 
 } // extern "C"

@@ -51,7 +51,7 @@ EXPORTS = [
     "heom_set_flow_buffers", "heom_add_pre_evaluate_action", "heom_clear_pre_evaluate_actions",
     "heom_hierarchy_add", "heom_hierarchy_subtract", "heom_hierarchy_dot_product", "heom_hierarchy_scale",
     "heom_hierarchy_mmult_left", "heom_hierarchy_mmult_right", "heom_instance_write", "heom_instance_read",
-    "heom_tables_state",
+    "heom_tables_state", "heom_adjoint_set_memory_limit", "heom_adjoint_recursive_slots",
 ]
 
 PRE_EVALUATE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_void_p)
@@ -202,6 +202,9 @@ def lib():
         L.heom_adjoint_create_batch.argtypes = [C.POINTER(SystemDesc), i32, C.POINTER(Options), C.POINTER(vp)]
         L.heom_adjoint_instances.restype = i32
         L.heom_adjoint_instances.argtypes = [vp]
+        L.heom_adjoint_set_memory_limit.argtypes = [vp, i64]
+        L.heom_adjoint_recursive_slots.restype = i64
+        L.heom_adjoint_recursive_slots.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -702,6 +705,14 @@ class Adjoint:
 
     def kernel_launches(self):
         return lib().heom_adjoint_kernel_launches(self.h)
+
+    def set_memory_limit(self, nbytes):
+        """Device bytes the sweep may hold for its states (0: free memory)."""
+        _check(lib().heom_adjoint_set_memory_limit(self.h, int(nbytes)))
+
+    def recursive_slots(self):
+        """Slots of the last sweep's recursive checkpointing (0: sqrt layout)."""
+        return lib().heom_adjoint_recursive_slots(self.h)
 
     def close(self):
         if self.h:

@@ -415,7 +415,9 @@ int heom_tables_mask(const heom_tables* t, const char* strategy, int64_t first_l
  * interleaved).  heom_adjoint_gradient returns J and its gradients from one
  * forward and one backward sweep (the transposed derivative L^H run backward
  * through the stages, checkpoints every ceil(sqrt(steps)) steps, each
- * segment recomputed from its checkpoint):
+ * segment recomputed from its checkpoint; when those states exceed the
+ * memory limit, recursive checkpointing in the states that fit, each step
+ * recomputed a few times more -- results are bit-identical either way):
  *   grad_h      [states*states*2]: dJ/dRe H_ij, dJ/dIm H_ij (per cm^-1), every
  *               entry independent (a symmetric coupling perturbation is the
  *               sum of the (i,j) and (j,i) entries)
@@ -441,6 +443,13 @@ int heom_adjoint_gradient(heom_adjoint* a, const double* rho0, const double* obs
                           double dt, int64_t steps, double* loss, double* grad_h, double* grad_lambda,
                           double* grad_gamma, double* grad_rho0);
 int64_t heom_adjoint_kernel_launches(const heom_adjoint* a);
+/* Device memory heom_adjoint_gradient may hold for its states (checkpoints,
+ * stage inputs, adjoint), in bytes; 0 (the default) = the device's free
+ * memory at the call plus what the adjoint already holds.
+ * heom_adjoint_recursive_slots: the step-state slots of the last call's
+ * recursive checkpointing, 0 when it used the sqrt(steps) layout. */
+int heom_adjoint_set_memory_limit(heom_adjoint* a, int64_t bytes);
+int64_t heom_adjoint_recursive_slots(const heom_adjoint* a);
 /* Derivatives of the bath tables (pf_same [baths*2], pf_circ [baths*2],
  * cbk [baths*matsubaras*2], SI units) with respect to theta = 0: lambda of
  * every bath together (per J), theta = 1: gamma = 1/invnu of every bath

@@ -277,3 +277,32 @@ def test_adjoint_graphs_equal_eager_launches_and_survive_regrowth():
     assert a["loss"] == b["loss"]
     assert np.array_equal(a["h"], b["h"]) and np.array_equal(a["rho0"], b["rho0"])
     assert a["lambda"] == b["lambda"] and a["gamma"] == b["gamma"]
+
+
+@pytest.mark.parametrize("limit_states,free_slots", [(8, 0), (11, 3), (20, 12)])
+def test_recursive_checkpointing_is_bit_identical_to_sqrt_layout(limit_states, free_slots):
+    # a memory limit below the sqrt layout's states switches the sweep to
+    # recursive checkpointing: the same kernels in the same backward order
+    n, steps = 5, 47
+    systems = [hb.System(ho.synthetic_hamiltonian(n, 60 + k), [35.0] * n, [50.0] * n, [0.0] * n, 2, 300.0, 2 + k)
+               for k in range(2)]
+    rho0 = np.zeros((n, n), complex)
+    rho0[0, 0] = 1.0
+    obs = np.zeros((2, n, n), complex)
+    obs[0, 1, 1] = obs[1, 2, 2] = 1.0
+    w = hb.trapezoid_weights(steps, 1.0)
+    with hb.Adjoint(systems) as A:
+        ref = A.gradient(rho0, obs, w, 1e-15, steps)
+        assert A.recursive_slots() == 0
+        pairs = n * (n - 1) // 2 + (n + 1) // 2
+        st = sum(int(hb.build_tables(s)["matrices"]) for s in systems) * pairs * 32  # bytes per state
+        A.set_memory_limit(limit_states * st)
+        out = A.gradient(rho0, obs, w, 1e-15, steps)
+        assert A.recursive_slots() == free_slots + 1
+        A.set_memory_limit(0)
+        again = A.gradient(rho0, obs, w, 1e-15, steps)
+        assert A.recursive_slots() == 0
+    for o in (out, again):
+        assert np.array_equal(o["loss"], ref["loss"])
+        assert np.array_equal(o["h"], ref["h"]) and np.array_equal(o["rho0"], ref["rho0"])
+        assert np.array_equal(o["lambda"], ref["lambda"]) and np.array_equal(o["gamma"], ref["gamma"])
