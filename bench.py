@@ -15,7 +15,7 @@ hierarchy; 1 ADO-update = one ADO advanced through one RK4 step.
             the initial hierarchy state from pinned host memory
             (heom_set_state), K steps with the top matrix recorded every 10
             steps and copied back to the host (heom_propagate)
-  roofline  the heom_stage kernel (every launch in the timed region is one):
+  roofline  the stage kernel (every launch in the timed region is one):
             algorithmic bytes per launch = ADOs x 32 N^2 B (read the stage
             input, write the stage output) / average launch duration
   cpu_baseline  the reference's own heom_ode.cl + rk_weighted_add.cl compiled
@@ -60,11 +60,16 @@ def synthetic_h(n, seed):
     return h
 
 
-def workload_config(scheme, depth=DEPTH, ados=735471):
-    return {"workload": f"8 sites, 1 Drude-Lorentz bath/site, 1 Matsubara term (16 modes), depth {depth}, "
-                        f"{ados} ADOs of 8x8, RK4 dt=0.5 fs",
-            "ados": ados, "states": N_SITES, "modes": 16, "depth": depth, "dt_fs": 0.5,
-            "rk4_scheme": scheme, "l2": "inputs larger than L2 (753 MB state), no flush",
+def workload_config(scheme, depth=DEPTH, ados=735471, sites=N_SITES, matsubaras=MATSUBARAS):
+    modes = sites * matsubaras
+    pairs = sites * (sites - 1) // 2 + (sites + 1) // 2
+    mb = ados * pairs * 32 / 1e6
+    return {"workload": f"{sites} sites, 1 Drude-Lorentz bath/site, {matsubaras - 1} Matsubara term(s) "
+                        f"({modes} modes), depth {depth}, {ados} ADOs of {sites}x{sites}, RK4 dt=0.5 fs",
+            "ados": ados, "states": sites, "modes": modes, "depth": depth, "dt_fs": 0.5,
+            "rk4_scheme": scheme,
+            "l2": f"inputs larger than L2 ({mb:.0f} MB state), no flush" if mb > 126 else
+                  f"state of {mb:.0f} MB fits in L2 (no flush)",
             "seed": SEED}
 
 
@@ -137,7 +142,7 @@ def measured_hbm_peak():
 
 
 def profiled_traffic():
-    """Per-launch DRAM bytes of heom_stage from the committed ncu summary."""
+    """Per-launch DRAM bytes of the benchmark stage kernel from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "heom_stage_cfg2.md")
     try:
         for line in open(path):
@@ -203,7 +208,8 @@ def run_e2e(H, y0, args, world, dist, nodes, barrier):
         t = torch.tensor([e2e_secs], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_secs = float(t.item())
-    trace = float(np.sum([tops[-1][(N_SITES + 1) * 2 * i] for i in range(N_SITES)]))
+    n = H.states
+    trace = float(np.sum([tops[-1][(n + 1) * 2 * i] for i in range(n)]))
     return {"value": world * nodes * e2e_steps / e2e_secs, "unit": UNIT,
             "h2d_bytes_per_step": H.state_len * 8 / e2e_steps,
             "d2h_bytes_per_step": tops.size * 8 / e2e_steps,
@@ -643,6 +649,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--depth", type=int, default=DEPTH,
                     help="hierarchy depth (8 = the benchmark workload; smaller for profiling captures)")
+    ap.add_argument("--sites", type=int, default=N_SITES, help="plain workload: states (8 = the benchmark)")
+    ap.add_argument("--matsubaras", type=int, default=MATSUBARAS,
+                    help="plain workload: modes per bath (2 = the benchmark's one Matsubara term)")
     ap.add_argument("--workload", default="plain",
                     choices=["plain", "ensemble", "uneven", "adjoint", "uneven-adjoint"],
                     help="plain: one 735471-ADO hierarchy; ensemble: 256 disorder realisations "
@@ -679,8 +688,10 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    h = synthetic_h(N_SITES, SEED)
-    system = hb.System(h, [35.0] * N_SITES, [50.0] * N_SITES, [0.0] * N_SITES, MATSUBARAS, 300.0, args.depth)
+    ns, nm = args.sites, args.matsubaras
+    benchmark_case = (ns, nm, args.depth) == (N_SITES, MATSUBARAS, DEPTH)
+    h = synthetic_h(ns, SEED)
+    system = hb.System(h, [35.0] * ns, [50.0] * ns, [0.0] * ns, nm, 300.0, args.depth)
     H = hb.from_system(system, device=local_rank, scheme=args.scheme)
     nodes = H.matrices
     y0 = torch.zeros(H.state_len, dtype=torch.float64, pin_memory=True)
@@ -727,12 +738,13 @@ def main():
     peak, peak_kind = measured_hbm_peak()
     roofline = None
     if per_launch_s:
-        alg_bytes = nodes * 32 * N_SITES * N_SITES
+        alg_bytes = nodes * 32 * ns * ns
         achieved = alg_bytes / per_launch_s / 1e9
-        traffic = profiled_traffic()
+        traffic = profiled_traffic() if benchmark_case else None
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "traffic": traffic,
-                    "peak_source": f"{peak_kind} hbm_gbs", "kernel": "heom_stage",
+                    "peak_source": f"{peak_kind} hbm_gbs",
+                    "kernel": "heom_dmma_stage" if ns <= 8 else "heom_pair_stage",
                     "alg_bytes_per_launch": alg_bytes, "avg_launch_us": per_launch_s * 1e6}
 
     if rank == 0:
@@ -740,11 +752,11 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded H, Drude-Lorentz baths)",
-                "config": dict(workload_config(args.scheme, args.depth, nodes),
+                "config": dict(workload_config(args.scheme, args.depth, nodes, ns, nm),
                                parallelism=f"replicas{world}" if world > 1 else "single"),
                 "e2e": e2e,
                 "gpu_launches": int(launches), "roofline": roofline, "clocks": clk}
-        if world == 1 and not args.no_cpu_baseline:
+        if world == 1 and not args.no_cpu_baseline and benchmark_case:
             line["cpu_baseline"] = cpu_reference_sample(steps_cap=3)
         print(json.dumps(line), flush=True)
 

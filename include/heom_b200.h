@@ -209,8 +209,9 @@ int heom_buffer_read(heom_handle* h, const heom_buffer* b, double* host_state);
 size_t heom_buffer_size_byte(const heom_handle* h);
 
 /* One derivative evaluation with the reference's solve() semantics.  time and
- * step_size are accepted for interface parity (the path has no time-dependent
- * terms).  out or acc may be NULL where the mode does not write them. */
+ * step_size go to the pre-evaluate actions and place the field of
+ * heom_set_field (H at time + step_size, as the reference's e_field action).
+ * out or acc may be NULL where the mode does not write them. */
 int heom_solve(heom_handle* h, double time, double step_size, const heom_buffer* in,
                heom_buffer* out, double out_coeff, heom_buffer* acc, double acc_coeff,
                int acc_init, int mode);
