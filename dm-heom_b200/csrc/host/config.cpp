@@ -1,13 +1,16 @@
-// config.cpp -- population_dynamics configuration files.
+// config.cpp -- population_dynamics and linear_absorption configuration files.
 //
 // Reads the reference's INI files (dm-heom/src/heom/config.cpp:37-67,
-// population_dynamics_config.cpp:24-26, config_base.cpp:32): "[section]"
+// population_dynamics_config.cpp:24-26, linear_absorption_config.cpp:17-53,
+// dipole_config_entries.cpp:19-41, config_base.cpp:32): "[section]"
 // headers, "key=value" lines, '#' comments to the end of a line; values are
 // noma/typa literals -- numbers, booleans, braced lists "{a, b}", braced
 // matrices "{{a, b}, {c, d}}", complex numbers "(re, im)" or reals, and pair
 // lists "{(type, file), ...}".  Validation follows config::check
-// (config.cpp:73-175) and population_dynamics_config::check (:32-41); unit
-// conversion follows config::post_process (config.cpp:182-191).
+// (config.cpp:73-175), population_dynamics_config::check (:32-41) and
+// dipole_config_entries::check (:30-37); unit conversion follows
+// config::post_process (config.cpp:182-191) (the dipole strengths stay in
+// Debye: dipole_config_entries.cpp:39-41 leaves them unscaled).
 #include <algorithm>
 #include <cctype>
 #include <cstdlib>
@@ -37,9 +40,23 @@ const std::set<std::string>& known_keys()
         "solver.stepper_type", "solver.step_size", "solver.steps", "solver.track_flows", "solver.flow_filename",
         "system.sites", "system.ado_depth", "system.hamiltonian",
         "baths.number", "baths.max_per_site", "baths.coupling", "baths.lambda", "baths.invnu", "baths.Omega",
-        "baths.matsubaras", "baths.temperature",
-        "population_dynamics.rho_init"};
+        "baths.matsubaras", "baths.temperature"};
     return k;
+}
+
+// the keys each task adds (population_dynamics_config.cpp:24-26, dipole_config_entries.cpp:19-27)
+const std::set<std::string>& task_keys(const std::string& task)
+{
+    static const std::set<std::string> pd = {"population_dynamics.rho_init"};
+    static const std::set<std::string> la = {"dipole.directions", "dipole.strengths", "dipole.centers",
+                                             "dipole.tensor_prefactors", "dipole.tensor_components"};
+    static const std::set<std::string> none;
+    return task == "population_dynamics" ? pd : task == "linear_absorption" ? la : none;
+}
+
+bool any_task_key(const std::string& key)
+{
+    return task_keys("population_dynamics").count(key) || task_keys("linear_absorption").count(key);
 }
 
 const std::set<std::string>& observation_types()
@@ -155,14 +172,18 @@ config::config(const std::string& path)
         const size_t eq = line.find('=');
         if (eq == std::string::npos) throw config_error("expected key=value at line " + std::to_string(lineno));
         const std::string key = (section.empty() ? "" : section + ".") + trim(line.substr(0, eq));
-        if (!known_keys().count(key)) throw config_error("unrecognised option '" + key + "'");
+        if (!known_keys().count(key) && !any_task_key(key)) throw config_error("unrecognised option '" + key + "'");
         if (values_.count(key)) throw config_error("option '" + key + "' cannot be specified more than once");
         values_[key] = trim(line.substr(eq + 1));
     }
 
     // program (config_base.cpp:32, config.cpp:39-40)
     task_ = raw("program.task");
-    if (task_ != "population_dynamics") throw config_error("wrong program_task for this application");
+    if (task_ != "population_dynamics" && task_ != "linear_absorption")
+        throw config_error("program.task '" + task_ + "' is not supported (population_dynamics, linear_absorption)");
+    for (const auto& kv : values_)
+        if (!known_keys().count(kv.first) && !task_keys(task_).count(kv.first))
+            throw config_error("unrecognised option '" + kv.first + "'");
     for (const std::string& it : split_braced(raw("program.observations"))) {
         const std::string s = trim(it);
         if (s.size() < 2 || s.front() != '(' || s.back() != ')') throw config_error("bad observation entry: " + it);
@@ -247,14 +268,39 @@ config::config(const std::string& path)
     sys_.depth = (int32_t)depth;
     validate_system(sys_);
 
-    // population_dynamics.rho_init (population_dynamics_config.cpp:32-41)
-    const auto rrows = parse_matrix_items(raw("population_dynamics.rho_init"));
-    if ((int64_t)rrows.size() != sites)
-        throw config_error("population_dynamics.rho_init must be a system.sites by system.sites matrix");
-    for (const auto& r : rrows) {
-        if ((int64_t)r.size() != sites)
+    if (task_ == "population_dynamics") {
+        // population_dynamics.rho_init (population_dynamics_config.cpp:32-41)
+        const auto rrows = parse_matrix_items(raw("population_dynamics.rho_init"));
+        if ((int64_t)rrows.size() != sites)
             throw config_error("population_dynamics.rho_init must be a system.sites by system.sites matrix");
-        for (const auto& v : r) rho_init_.push_back(parse_complex(v));
+        for (const auto& r : rrows) {
+            if ((int64_t)r.size() != sites)
+                throw config_error("population_dynamics.rho_init must be a system.sites by system.sites matrix");
+            for (const auto& v : r) rho_init_.push_back(parse_complex(v));
+        }
+    } else {
+        // dipole entries (dipole_config_entries.cpp:19-37)
+        auto vectors = [&](const std::string& key) {
+            std::vector<std::vector<double>> out;
+            for (const auto& r : parse_matrix_items(raw(key))) {
+                out.emplace_back();
+                for (const auto& v : r) out.back().push_back(parse_real(v));
+            }
+            return out;
+        };
+        dipole_directions_ = vectors("dipole.directions");
+        dipole_centers_ = vectors("dipole.centers");
+        for (const auto& v : split_braced(raw("dipole.strengths"))) dipole_strengths_.push_back(parse_real(v));
+        for (const auto& v : split_braced(raw("dipole.tensor_prefactors")))
+            dipole_tensor_prefactors_.push_back(parse_real(v));
+        for (const auto& r : parse_matrix_items(raw("dipole.tensor_components"))) {
+            dipole_tensor_components_.emplace_back();
+            for (const auto& v : r) dipole_tensor_components_.back().push_back(parse_int(v));
+        }
+        if (dipole_directions_.size() != dipole_strengths_.size() || dipole_directions_.size() != dipole_centers_.size())
+            throw config_error("dipole.directions, dipole.strengths and dipole.centers must have the same size");
+        if (dipole_tensor_prefactors_.size() != dipole_tensor_components_.size())
+            throw config_error("dipole.tensor_prefactors and dipole.tensor_components must have the same size");
     }
 }
 

@@ -111,7 +111,8 @@ struct observation {
 };
 
 // An INI file with the reference's sections and literals
-// ([program] [filtering] [solver] [system] [baths] [population_dynamics]).
+// ([program] [filtering] [solver] [system] [baths], then [population_dynamics]
+// or [dipole] by program.task).
 class config {
 public:
     explicit config(const std::string& path);
@@ -130,6 +131,12 @@ public:
     const heom_system_desc& system_desc() const { return desc_; }
     const system_params& system() const { return sys_; }   // SI
     const std::vector<complex_t>& rho_init() const { return rho_init_; }
+    // dipole entries (linear_absorption; dipole_config_entries.hpp:41-54)
+    const std::vector<std::vector<double>>& dipole_directions() const { return dipole_directions_; }
+    const std::vector<std::vector<double>>& dipole_centers() const { return dipole_centers_; }
+    const std::vector<double>& dipole_strengths() const { return dipole_strengths_; }
+    const std::vector<double>& dipole_tensor_prefactors() const { return dipole_tensor_prefactors_; }
+    const std::vector<std::vector<int64_t>>& dipole_tensor_components() const { return dipole_tensor_components_; }
     // raw key lookup ("section.key")
     bool has(const std::string& key) const { return values_.count(key) != 0; }
     const std::string& raw(const std::string& key) const;
@@ -150,7 +157,24 @@ private:
     std::vector<int32_t> coupling_;
     system_params sys_;
     std::vector<complex_t> rho_init_;
+    std::vector<std::vector<double>> dipole_directions_, dipole_centers_;
+    std::vector<double> dipole_strengths_, dipole_tensor_prefactors_;
+    std::vector<std::vector<int64_t>> dipole_tensor_components_;
 };
+
+// ------------------------------------------------------------- spectra --
+enum class sites_to_states_mode { identity, with_ground_state };
+// sites_to_states.cpp:16-28 (states), :44-55 (H: ground state row and column
+// zero), :131-142 (coupling: the ground state couples to no bath)
+system_params state_system(const system_params& sites, sites_to_states_mode mode);
+// dipole_matrix.cpp:105-131 (with_ground_state): D(0, i+1) = v_i, every other
+// entry zero; row-major states x states complex, interleaved
+std::vector<double> dipole_matrix(const std::vector<double>& dipole_vector);
+// dipole_matrix.hpp:30-58 for the linear-absorption pseudo pathway
+// (dipole_pseudo_pathway.hpp:22-27: {minus, left}, {plus, left}): v_i =
+// directions[i][component] * strengths[i] with component =
+// tensor_components[tensor][spec]; spec 1 (plus) is the transpose
+std::vector<double> pathway_dipole_matrix(const config& cfg, size_t tensor, size_t spec);
 
 // literal parsing (noma/typa-style values)
 std::vector<std::string> split_braced(const std::string& s); // "{a, {b}, (c, d)}" -> items

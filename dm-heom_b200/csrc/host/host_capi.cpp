@@ -265,6 +265,7 @@ int heom_config_rho_init(const heom_config* c, double* out)
 {
     if (!c || !out) return set_error(HEOM_E_ARG, "NULL argument");
     const auto& r = c->cfg->rho_init();
+    if (r.empty()) return set_error(HEOM_E_ARG, "the configuration has no population_dynamics.rho_init");
     for (size_t q = 0; q < r.size(); ++q) {
         out[2 * q] = r[q].real();
         out[2 * q + 1] = r[q].imag();

@@ -809,7 +809,7 @@ def from_system(system: System, **kw) -> Heom:
 
 
 class Config:
-    """A parsed population_dynamics .cfg file (heom_config_*)."""
+    """A parsed population_dynamics or linear_absorption .cfg file (heom_config_*)."""
 
     def __init__(self, path):
         self.h = C.c_void_p()

@@ -382,12 +382,15 @@ void heom_tables_free(heom_tables* t);
 int heom_create_from_system(const heom_system_desc* sys, const heom_options* opt, heom_handle** out);
 
 typedef struct heom_config heom_config;
-/* Parse and validate a population_dynamics .cfg file. */
+/* Parse and validate a population_dynamics or linear_absorption .cfg file
+ * (program.task selects the task's own section: [population_dynamics] or
+ * [dipole]). */
 int heom_config_load(const char* path, heom_config** out);
 void heom_config_free(heom_config* c);
 /* Borrowed view of the [system]/[baths] values in config units. */
 int heom_config_system(const heom_config* c, heom_system_desc* view);
-/* population_dynamics.rho_init as sites*sites*2 interleaved doubles. */
+/* population_dynamics.rho_init as sites*sites*2 interleaved doubles
+ * (HEOM_E_ARG for a configuration of another task). */
 int heom_config_rho_init(const heom_config* c, double* out);
 /* Raw text of "section.key" copied into buf (NUL-terminated). */
 int heom_config_get(const heom_config* c, const char* key, char* buf, size_t len);

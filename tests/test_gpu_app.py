@@ -1,5 +1,6 @@
-"""GPU: the population-dynamics application end to end (reference command
-line and config files, all five observer types) and the hierarchy norm."""
+"""GPU: the population-dynamics and linear-absorption applications end to end
+(reference command line and config files, all five population observers, the
+dipole pseudo pathway) and the hierarchy norm."""
 import os
 import subprocess
 
@@ -8,11 +9,12 @@ import pytest
 
 import heom_b200 as hb
 import heom_oracle as ho
-from test_host import FMO_CFG
+from test_host import FMO_CFG, LA_CFG
 
 pytestmark = pytest.mark.gpu
 
 APP = os.path.join(os.path.dirname(hb.__file__), "bin", "heom_population_dynamics")
+LA_APP = os.path.join(os.path.dirname(hb.__file__), "bin", "heom_linear_absorption")
 
 
 def read_dat(path):
@@ -73,3 +75,44 @@ def test_hierarchy_norm_and_threshold_filter():
         want = mask.copy()
         want[(norms <= thr) & (mask != 2)] = 0
         assert np.array_equal(got, want)
+
+
+def test_linear_absorption_app_matches_oracle(tmp_path):
+    """tr(D- rho_top(t)) after D+ |g><g|, averaged over the three tensor
+    components, against the oracle propagating the ground-state system."""
+    (tmp_path / "heom.cfg").write_text(LA_CFG)
+    (tmp_path / "rt.cfg").write_text("[cuda]\ndevice_index=0\nrk4_scheme=product\n")
+    r = subprocess.run([LA_APP, "rt.cfg", "heom.cfg"], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    hdr, got = read_dat(tmp_path / "la.dat")
+    assert hdr == ["time", "trace_real", "trace_imag"]
+    assert np.allclose(got[:, 0], np.arange(5) * 5e-15, rtol=1e-15, atol=0)
+    # the state system: ground state 0 with zero H row/column and no bath, sites 1..3
+    h = np.array([[12410.0, -87.7, 5.5], [-87.7, 12530.0, 30.8], [5.5, 30.8, 12210.0]])
+    hs = np.zeros((4, 4))
+    hs[1:, 1:] = h
+    coupling = np.array([[-1], [0], [1], [2]], np.int32)
+    prob = ho.build_problem(ho.make_system(hs, [35] * 3, [50] * 3, [0] * 3, 2, 77.0, 3, coupling=coupling))
+    dirs = np.array([[-0.741, -0.561, -0.370], [-0.857, 0.504, -0.107], [-0.197, 0.957, -0.211]])
+    strengths = np.array([4, 3.5, 4.2])
+    want = np.zeros(5, complex)
+    for comp in range(3):  # tensor_components {{0, 0}, {1, 1}, {2, 2}}, prefactors 1
+        v = dirs[:, comp] * strengths
+        dm = np.zeros((4, 4))
+        dm[0, 1:] = v
+        dp = dm.T
+        top = np.zeros((4, 4))
+        top[:, 0] = dp[:, 0]
+        y = np.zeros(prob.state_len)
+        y[0:32:2] = top.reshape(-1)
+        for row in range(5):
+            if row:
+                y, _ = ho.propagate(prob, 1e-15, 5, 5, y=y)
+            rho = (y[0:32:2] + 1j * y[1:32:2]).reshape(4, 4)
+            want[row] += np.trace(dm @ rho)
+    want /= 3
+    scale = np.max(np.abs(want))
+    assert np.max(np.abs(got[:, 1] - want.real)) <= 1e-10 * scale
+    assert np.max(np.abs(got[:, 2] - want.imag)) <= 1e-10 * scale
+    # at t = 0 the trace is the mean squared dipole length over the components
+    assert abs(want[0] - sum(np.sum((dirs[:, c] * strengths) ** 2) for c in range(3)) / 3) <= 1e-12 * scale

@@ -3,6 +3,7 @@ the C ABI library itself (exports, admission checks that need no GPU)."""
 import ctypes as C
 import os
 import re
+import subprocess
 
 import numpy as np
 import pytest
@@ -103,7 +104,8 @@ def test_config_parses_reference_style_file(tmp_path):
     (("first_layer=-1", "first_layer=0"), "first_layer"),
     (("{-87.7, 12530.0, 30.8}", "{-87.0, 12530.0, 30.8}"), "hermitian"),
     (("sites=3", "sites=4"), "matrix"),
-    (("task=population_dynamics", "task=linear_absorption"), "program_task"),
+    (("task=population_dynamics", "task=thermal_state_search"), "program.task"),
+    (("task=population_dynamics", "task=linear_absorption"), "population_dynamics.rho_init"),
     (("stepper_type=rk_rk4", "stepper_type=rk_euler"), "rk_rk4"),
     (("lambda={35, 35, 35}", "lambda={35, 35}"), "lambda"),
     (("invnu={50, 50, 50}", "invnu={50, 0, 50}"), "invnu"),
@@ -117,6 +119,53 @@ def test_config_rejects_invalid(tmp_path, edit, msg):
     with pytest.raises(hb.HeomError) as e:
         hb.Config(p)
     assert msg in str(e.value)
+
+
+LA_CFG = FMO_CFG.replace("task=population_dynamics", "task=linear_absorption").replace(
+    "observations={(matrix_complete, m.dat), (matrix_diagonal, d.dat), (matrix_trace_id, t.dat)}",
+    "observations={(matrix_trace_linear_absorption, la.dat)}").split("[population_dynamics]")[0] + """[dipole]
+directions={{-0.741, -0.561, -0.370}, {-0.857, 0.504, -0.107}, {-0.197, 0.957, -0.211}}
+centers={{2.651, 0.260, -1.135}, {1.561, -0.152, -1.725}, {0.339, -1.361, -1.385}}
+strengths={4, 3.5, 4.2}
+tensor_prefactors={1, 1, 1}
+tensor_components={{0, 0}, {1, 1}, {2, 2}}
+"""
+
+
+def test_linear_absorption_config(tmp_path):
+    p = tmp_path / "la.cfg"
+    p.write_text(LA_CFG)
+    c = hb.Config(p)
+    assert c.get("program.task") == "linear_absorption"
+    assert c.get("dipole.strengths") == "{4, 3.5, 4.2}"
+    with pytest.raises(hb.HeomError):
+        c.rho_init()  # a population_dynamics entry
+    # dipole entries belong to the linear_absorption task only, and must agree in size
+    p.write_text(FMO_CFG + LA_CFG.split("[baths]")[1].split("temperature=77 # K")[1])
+    with pytest.raises(hb.HeomError) as e:
+        hb.Config(p)
+    assert "unrecognised option 'dipole." in str(e.value)
+    p.write_text(LA_CFG.replace("strengths={4, 3.5, 4.2}", "strengths={4, 3.5}"))
+    with pytest.raises(hb.HeomError) as e:
+        hb.Config(p)
+    assert "same size" in str(e.value)
+    p.write_text(LA_CFG.replace("tensor_prefactors={1, 1, 1}", "tensor_prefactors={1, 1}"))
+    with pytest.raises(hb.HeomError) as e:
+        hb.Config(p)
+    assert "same size" in str(e.value)
+
+
+def test_linear_absorption_app_reports_config_errors_before_the_device(tmp_path, root):
+    app = os.path.join(root, "dm-heom_b200", "bin", "heom_linear_absorption")
+    (tmp_path / "rt.cfg").write_text("[cuda]\ndevice_index=0\n")
+    (tmp_path / "pd.cfg").write_text(FMO_CFG)
+    r = subprocess.run([app, "rt.cfg", "pd.cfg"], cwd=tmp_path, capture_output=True, text=True, timeout=60)
+    assert r.returncode != 0 and "population_dynamics.rho_init" not in r.stderr
+    assert "wrong program_task" in r.stderr
+    (tmp_path / "la.cfg").write_text(LA_CFG.replace("tensor_components={{0, 0}, {1, 1}, {2, 2}}",
+                                                    "tensor_components={{0, 0}, {1, 1}, {2, 5}}"))
+    r = subprocess.run([app, "rt.cfg", "la.cfg"], cwd=tmp_path, capture_output=True, text=True, timeout=60)
+    assert r.returncode != 0 and "out of range" in r.stderr
 
 
 def test_config_missing_file():
