@@ -567,10 +567,10 @@ def run_uneven_adjoint(args, rank, local_rank):
         obs = np.zeros((n, n), complex)
         obs[0, 0] = 1.0
         with hb.Adjoint([systems[k] for k in members], device=local_rank) as A:
-            A.gradient(rho0, obs, hb.trapezoid_weights(2, 1.0), dt, 2)  # set-up outside the timing
+            A.gradient(rho0, obs, hb.trapezoid_weights(2, 1.0), dt, 2, outputs=("h",))  # set-up outside the timing
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            out = A.gradient(rho0, obs, w, dt, steps)
+            out = A.gradient(rho0, obs, w, dt, steps, outputs=("h",))  # site energies: the diagonal of dJ/dH
             t_adj += time.perf_counter() - t0
             if A.recursive_slots():
                 recursive.append({"instances": members, "gb_per_state": nodes * P * 32 / 1e9,

@@ -956,6 +956,8 @@ struct GradParams {
     const int64_t* inst_base;          // [instances + 1] first ADO of every instance
     int blocks_per_inst;               // blocks [k*bpi, (k+1)*bpi) sweep instance k only
     int N, P, W, NW, TWB, SL;
+    int want_h;                        // accumulate Z (the H gradient)
+    int want_bath;                     // accumulate <a, L_theta' w> (the lambda and gamma gradients)
 };
 
 __host__ __device__ inline int grad_warp_bytes(int n) { return 2 * n * (n + 1) * 16; }
@@ -972,10 +974,18 @@ __global__ void __launch_bounds__(kCtaWarps * 32) heom_adjoint_grad(const GradPa
     double2* At = reinterpret_cast<double2*>(smem + warp * grad_warp_bytes(N)); // [N][N+1]
     double2* Wt = At + N * (N + 1);
     double2* red = reinterpret_cast<double2*>(smem + kCtaWarps * grad_warp_bytes(N)); // [warps][NN+2]
-    double2 zac[8];
+    // Z on the FP64 tensor pipe: blocks (I, J) of 8 x 8 of the zero-padded Z (one block for
+    // N <= 8, 2 x 2 for N <= 16), accumulated over the warp's ADOs in the MMA fragments:
+    // lane 4g + t holds Z(8I+g, 8J+2t) and Z(8I+g, 8J+2t+1), real and imaginary parts
+    const int gq = lane >> 2, t4 = lane & 3;
+    const int nblk = N <= 8 ? 1 : 4, ks = (N + 3) / 4;
+    double zr[4][2], zi[4][2];
 #pragma unroll
-    for (int r = 0; r < 8; ++r) zac[r] = make_double2(0.0, 0.0);
+    for (int b = 0; b < 4; ++b) zr[b][0] = zr[b][1] = zi[b][0] = zi[b][1] = 0.0;
     double2 dl = make_double2(0.0, 0.0), dgm = dl;
+    auto el = [&](const double2* T, int r, int c) {
+        return (r < N && c < N) ? T[r * (N + 1) + c] : make_double2(0.0, 0.0);
+    };
 
     const int inst = blockIdx.x / g.blocks_per_inst, jb = blockIdx.x - inst * g.blocks_per_inst;
     const int64_t stride = (int64_t)g.blocks_per_inst * kCtaWarps, end = g.inst_base[inst + 1];
@@ -994,6 +1004,7 @@ __global__ void __launch_bounds__(kCtaWarps * 32) heom_adjoint_grad(const GradPa
             Wt[i2 * (N + 1) + j2] = w2;
             const bool diag = i1 == j1;
             const bool twin = e2 == e1; // padding half of an odd diagonal pair
+            if (!g.want_bath) continue;
             // derivative of the operator applied to w, for theta = lambda (0), gamma (1)
             double2 D1[2], D2[2];
             for (int th = 0; th < 2; ++th) {
@@ -1053,32 +1064,45 @@ __global__ void __launch_bounds__(kCtaWarps * 32) heom_adjoint_grad(const GradPa
             }
         }
         __syncwarp();
-        // Z(k,l) = sum_i w(i,k) conj(a(i,l)) - sum_j conj(a(k,j)) w(l,j)
+        // Z(k,l) = sum_i w(i,k) conj(a(i,l)) - sum_j conj(a(k,j)) w(l,j):
+        //   Re Z = Wr^T Ar + Wi^T Ai - Ar Wr^T - Ai Wi^T, Im Z = Wi^T Ar - Wr^T Ai - Ar Wi^T + Ai Wr^T
+        if (g.want_h) {
 #pragma unroll
-        for (int r = 0; r < 8; ++r) {
-            const int q = lane + 32 * r;
-            if (q >= NN) break;
-            const int k = q / N, l = q - k * N;
-            double zr = 0.0, zi = 0.0;
-            for (int i = 0; i < N; ++i) {
-                const double2 wv = Wt[i * (N + 1) + k], av = At[i * (N + 1) + l];
-                zr += wv.x * av.x + wv.y * av.y;
-                zi += wv.y * av.x - wv.x * av.y;
-                const double2 ak = At[k * (N + 1) + i], wl = Wt[l * (N + 1) + i];
-                zr -= ak.x * wl.x + ak.y * wl.y;
-                zi -= ak.x * wl.y - ak.y * wl.x;
+            for (int b = 0; b < 4; ++b) {
+                if (b >= nblk) continue;
+                const int I = b >> 1, J = b & 1;
+#pragma unroll
+                for (int s = 0; s < 4; ++s) {
+                    if (s >= ks) continue;
+                    const int k0 = 4 * s + t4;
+                    const double2 wT = el(Wt, k0, 8 * I + gq); // A operand of W^T A: W(4s+t, 8I+g)
+                    const double2 aB = el(At, k0, 8 * J + gq); // B operand of W^T A: A(4s+t, 8J+g)
+                    const double2 aA = el(At, 8 * I + gq, k0); // A operand of A W^T: A(8I+g, 4s+t)
+                    const double2 wB = el(Wt, 8 * J + gq, k0); // B operand of A W^T: W(8J+g, 4s+t)
+                    dmma(zr[b][0], zr[b][1], wT.x, aB.x);
+                    dmma(zr[b][0], zr[b][1], wT.y, aB.y);
+                    dmma(zr[b][0], zr[b][1], -aA.x, wB.x);
+                    dmma(zr[b][0], zr[b][1], -aA.y, wB.y);
+                    dmma(zi[b][0], zi[b][1], wT.y, aB.x);
+                    dmma(zi[b][0], zi[b][1], -wT.x, aB.y);
+                    dmma(zi[b][0], zi[b][1], -aA.x, wB.y);
+                    dmma(zi[b][0], zi[b][1], aA.y, wB.x);
+                }
             }
-            zac[r].x += zr;
-            zac[r].y += zi;
         }
         __syncwarp();
     }
     // block sum in a fixed order, then weight * sum into this block's row
     double2* mine = red + warp * (NN + 2);
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-        const int q = lane + 32 * r;
-        if (q < NN) mine[q] = zac[r];
+    for (int b = 0; b < 4; ++b) {
+        if (b >= nblk) continue;
+        const int r = 8 * (b >> 1) + gq;
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+            const int c = 8 * (b & 1) + 2 * t4 + e;
+            if (r < N && c < N) mine[r * N + c] = make_double2(zr[b][e], zi[b][e]);
+        }
     }
     for (int off = 16; off > 0; off >>= 1) {
         dl.x += __shfl_down_sync(0xffffffffu, dl.x, off);

@@ -2321,6 +2321,7 @@ struct heom_adjoint {
     int64_t cap_cps = 0, cap_seg = 0, cap_rows = 0;
     int64_t mem_limit = 0;     // bytes for the sweep's states (0: free device memory)
     int64_t rec_slots = 0;     // recursive-checkpointing slots of the last sweep (0: sqrt layout)
+    int want_h = 1, want_bath = 1; // gradients the sweep accumulates (from the output pointers)
     DevBuf<double> d_w;        // loss weights [steps + 1]
     DevBuf<int64_t> d_base;    // step offset of the segment being run (read by the captured kernels)
     int64_t cap_w = 0;
@@ -2443,6 +2444,8 @@ int adj_grad(heom_adjoint* A, const double2* a, const double2* w, double2 weight
     g.NW = h->NW;
     g.TWB = h->TWB;
     g.SL = h->SL;
+    g.want_h = A->want_h;
+    g.want_bath = A->want_bath;
     heomk::heom_adjoint_grad<<<A->grid, heomk::kCtaWarps * 32, A->grad_smem, h->stream>>>(g);
     h->launches++;
     CUDA_TRY(cudaGetLastError());
@@ -2757,6 +2760,13 @@ int heom_adjoint_gradient(heom_adjoint* A, const double* rho0, const double* obs
         }
     }
     A->rec_slots = slots;
+    // the gradients to accumulate (NULL outputs are skipped); the captured graphs hold them
+    const int want_h = grad_h ? 1 : 0, want_bath = (grad_lambda || grad_gamma) ? 1 : 0;
+    if (want_h != A->want_h || want_bath != A->want_bath) {
+        A->drop_graphs();
+        A->want_h = want_h;
+        A->want_bath = want_bath;
+    }
     // the captured graphs hold buffer addresses: any reallocation drops them
     const bool shrink = slots > 0 && (A->cap_cps > ncp || A->cap_seg > 4);
     if (shrink || ncp > A->cap_cps || 4 * S > A->cap_seg || steps + 1 > A->cap_rows || steps + 1 > A->cap_w)

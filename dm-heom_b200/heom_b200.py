@@ -679,7 +679,9 @@ class Adjoint:
         self.states = systems[0].sites
         self.instances = len(systems)
 
-    def gradient(self, rho0, observable, weights, dt, steps):
+    def gradient(self, rho0, observable, weights, dt, steps, outputs=("h", "lambda", "gamma", "rho0")):
+        """Loss and gradients; `outputs` names the gradients to compute (the
+        others are skipped by the sweep and returned as None)."""
         n, K = self.states, self.instances
 
         def per_instance(a):
@@ -695,12 +697,16 @@ class Adjoint:
         loss, gl, gg = np.zeros(K), np.zeros(K), np.zeros(K)
         gh = np.zeros(2 * K * n * n)
         gr = np.zeros(2 * K * n * n)
+        def opt(name, a):
+            return _ptr(a) if name in outputs else None
         _check(lib().heom_adjoint_gradient(self.h, _ptr(rho0), _ptr(obs), _ptr(w), dt, steps, _ptr(loss),
-                                           _ptr(gh), _ptr(gl), _ptr(gg), _ptr(gr)))
+                                           opt("h", gh), opt("lambda", gl), opt("gamma", gg), opt("rho0", gr)))
         out = {"loss": loss, "h": gh.view(np.complex128).reshape(K, n, n),  # dJ/dRe H + i dJ/dIm H, per cm^-1
                "lambda": gl, "gamma": gg, "rho0": gr.view(np.complex128).reshape(K, n, n)}
+        out = {k: (v if k == "loss" or k in outputs else None) for k, v in out.items()}
         if not self.batch:
-            out = {k: (v[0] if k != "loss" and k not in ("lambda", "gamma") else float(v[0])) for k, v in out.items()}
+            out = {k: (None if v is None else v[0] if k not in ("loss", "lambda", "gamma") else float(v[0]))
+                   for k, v in out.items()}
         return out
 
     def kernel_launches(self):

@@ -306,3 +306,21 @@ def test_recursive_checkpointing_is_bit_identical_to_sqrt_layout(limit_states, f
         assert np.array_equal(o["loss"], ref["loss"])
         assert np.array_equal(o["h"], ref["h"]) and np.array_equal(o["rho0"], ref["rho0"])
         assert np.array_equal(o["lambda"], ref["lambda"]) and np.array_equal(o["gamma"], ref["gamma"])
+
+
+def test_gradient_subset_skips_work_and_keeps_bits():
+    # NULL outputs skip their accumulation; the others are bit-identical
+    n, steps = 9, 30
+    system = hb.System(ho.synthetic_hamiltonian(n, 17), [35.0] * n, [50.0] * n, [0.0] * n, 2, 300.0, 2)
+    rho0 = np.zeros((n, n), complex)
+    rho0[0, 0] = 1.0
+    obs = np.zeros((n, n), complex)
+    obs[2, 2] = 1.0
+    w = hb.trapezoid_weights(steps, 1.0)
+    with hb.Adjoint(system) as A:
+        full = A.gradient(rho0, obs, w, 1e-15, steps)
+        only_h = A.gradient(rho0, obs, w, 1e-15, steps, outputs=("h",))
+        only_bath = A.gradient(rho0, obs, w, 1e-15, steps, outputs=("lambda", "gamma"))
+    assert only_h["lambda"] is None and only_h["rho0"] is None and only_bath["h"] is None
+    assert np.array_equal(only_h["h"], full["h"]) and only_h["loss"] == full["loss"]
+    assert only_bath["lambda"] == full["lambda"] and only_bath["gamma"] == full["gamma"]
