@@ -173,7 +173,20 @@ def cpu_reference_sample(steps_cap=1, scheme_note="reference"):
     return {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
             "sample": f"{steps_cap} RK4 step(s) of the full 735471-ADO hierarchy "
                       f"({'heom_ode.cl + rk_weighted_add.cl compiled for the host' if kind == 'reference' else 'oracle C port'}, "
-                      f"OpenMP over {threads} threads), {secs:.2f} s"}
+                      f"OpenMP over {threads} threads), {secs:.2f} s",
+            "opencl_cpu": opencl_cpu_note()}
+
+
+def opencl_cpu_note():
+    """Whether this box offers a CPU OpenCL device (an installable client
+    driver other than the GPU vendor's); the reference's own OpenCL path is
+    timed only through its kernels compiled for the host."""
+    import glob
+    icds = sorted(os.path.basename(p) for p in glob.glob("/etc/OpenCL/vendors/*.icd"))
+    cpu = [i for i in icds if "nvidia" not in i.lower()]
+    if not cpu:
+        return "OpenCL CPU device unavailable on this box" + (f" (ICDs: {', '.join(icds)})" if icds else " (no ICD)")
+    return f"CPU OpenCL ICDs present but not timed: {', '.join(cpu)}"
 
 
 def run_reference_arm(args, rank):
@@ -755,7 +768,8 @@ def main():
                 "config": dict(workload_config(args.scheme, args.depth, nodes, ns, nm),
                                parallelism=f"replicas{world}" if world > 1 else "single"),
                 "e2e": e2e,
-                "gpu_launches": int(launches), "roofline": roofline, "clocks": clk}
+                "gpu_launches": int(launches), "roofline": roofline, "clocks": clk,
+                "derivative_evals_per_s": 4 * value}
         if world == 1 and not args.no_cpu_baseline and benchmark_case:
             line["cpu_baseline"] = cpu_reference_sample(steps_cap=3)
         print(json.dumps(line), flush=True)
