@@ -722,18 +722,19 @@ __global__ void __launch_bounds__(kCtaWarps * 32, SLT <= 2 ? 3 : 2) heom_pair_st
             xr[0] = make_double2(cr0, ci0);
             xr[1] = make_double2(cr1, ci1);
         }
-        team_sync<TW>(team);
 
+        // the bath terms first: they need only the staged tile and the
+        // neighbours, so a warp that finished its commutator blocks goes on
+        // while the others complete theirs; the exchange tile is read after
+        // the team barrier
+        const int i1 = e1 / N, j1 = e1 - i1 * N, i2 = e2 / N, j2 = e2 - i2 * N;
+        double2 L1 = make_double2(0.0, 0.0), L2 = L1, s1 = L1, s2 = L1;
         if (active) {
             const int32_t* nb = reinterpret_cast<const int32_t*>(slot + L.nbr_off);
             const unsigned char* tu = slot + L.tup_off;
             const double2 pss = *reinterpret_cast<const double2*>(slot + L.pss_off);
-            const int i1 = e1 / N, j1 = e1 - i1 * N, i2 = e2 / N, j2 = e2 - i2 * N;
-            const double2 s1 = t[tile_pos(N, i1, j1)];
-            const double2 s2 = t[tile_pos(N, i2, j2)];
-            const double2 c1 = xch[i1 * kXchStride + j1], c2 = xch[i2 * kXchStride + j2];
-            double2 L1 = make_double2(-c1.y, c1.x); // i * (w H - H w) / hbar
-            double2 L2 = make_double2(-c2.y, c2.x);
+            s1 = t[tile_pos(N, i1, j1)];
+            s2 = t[tile_pos(N, i2, j2)];
 
             // ---- same term ----
             cmac(L1, make_double2(pss.x + g1.x, pss.y + g1.y), s1);
@@ -792,6 +793,17 @@ __global__ void __launch_bounds__(kCtaWarps * 32, SLT <= 2 ? 3 : 2) heom_pair_st
                     }
                 }
             }
+
+        }
+        team_sync<TW>(team);
+
+        if (active) {
+            // ---- commutator: i * (w H - H w) / hbar from the exchange tile ----
+            const double2 c1 = xch[i1 * kXchStride + j1], c2 = xch[i2 * kXchStride + j2];
+            L1.x -= c1.y;
+            L1.y += c1.x;
+            L2.x -= c2.y;
+            L2.y += c2.x;
 
             // ---- stage write ----
             const int64_t off = u * (2 * P) + 2 * lt;
