@@ -5,7 +5,7 @@ combine the per-neighbour coefficients on the host, so results differ from
 the reference's operation order by rounding only):
   * one derivative evaluation: max |gpu - ref| <= 1e-13 * max |ref|
   * propagated populations:   max |gpu - ref| <= 1e-10 (relative to the
-    total population 1)
+    total population 1), the accuracy the path must keep
 """
 import numpy as np
 import pytest
