@@ -1926,7 +1926,9 @@ int ens_autotune(heom_ensemble* e, double* best_us)
         if (int rc = resolve_stage(h, &fn, &blocks)) return rc;
         full[c] = h->per_sm[0][h->hkind] * h->sm_count;
         groups[c] = blocks;
-        work[c] = (double)h->nodes * h->P;
+        // a stage costs about one warp pass per ADO (N <= 8) or per team member
+        // (N > 8), whatever the sectors an ADO fills
+        work[c] = (double)h->n_active * (h->N <= 8 ? 1 : heomk::team_warps(h->N));
         total += work[c];
     }
     const std::string sig = ens_signature(e);
