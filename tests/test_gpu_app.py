@@ -77,11 +77,17 @@ def test_hierarchy_norm_and_threshold_filter():
         assert np.array_equal(got, want)
 
 
-def test_linear_absorption_app_matches_oracle(tmp_path):
+@pytest.mark.parametrize("scheme,filtering", [("product", None), ("reference", None),
+                                              ("product", ("single_excitation", 1))])
+def test_linear_absorption_app_matches_oracle(tmp_path, scheme, filtering):
     """tr(D- rho_top(t)) after D+ |g><g|, averaged over the three tensor
     components, against the oracle propagating the ground-state system."""
-    (tmp_path / "heom.cfg").write_text(LA_CFG)
-    (tmp_path / "rt.cfg").write_text("[cuda]\ndevice_index=0\nrk4_scheme=product\n")
+    cfg = LA_CFG
+    if filtering:
+        cfg = cfg.replace("strategy=none", f"strategy={filtering[0]}").replace(
+            "first_layer=-1", f"first_layer={filtering[1]}")
+    (tmp_path / "heom.cfg").write_text(cfg)
+    (tmp_path / "rt.cfg").write_text(f"[cuda]\ndevice_index=0\nrk4_scheme={scheme}\n")
     r = subprocess.run([LA_APP, "rt.cfg", "heom.cfg"], cwd=tmp_path, capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     hdr, got = read_dat(tmp_path / "la.dat")
@@ -92,7 +98,12 @@ def test_linear_absorption_app_matches_oracle(tmp_path):
     hs = np.zeros((4, 4))
     hs[1:, 1:] = h
     coupling = np.array([[-1], [0], [1], [2]], np.int32)
-    prob = ho.build_problem(ho.make_system(hs, [35] * 3, [50] * 3, [0] * 3, 2, 77.0, 3, coupling=coupling))
+    sysd = ho.make_system(hs, [35] * 3, [50] * 3, [0] * 3, 2, 77.0, 3, coupling=coupling)
+    mask = None
+    if filtering:
+        import make_golden as mg
+        mask = mg.single_excitation_mask(ho.build_graph(6, 3), 2, filtering[1])
+    prob = ho.build_problem(sysd, mask=mask)
     dirs = np.array([[-0.741, -0.561, -0.370], [-0.857, 0.504, -0.107], [-0.197, 0.957, -0.211]])
     strengths = np.array([4, 3.5, 4.2])
     want = np.zeros(5, complex)
