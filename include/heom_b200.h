@@ -428,7 +428,9 @@ int heom_tables_mask(const heom_tables* t, const char* strategy, int64_t first_l
  *   grad_lambda dJ/dlambda with lambda of every bath moved together (per cm^-1)
  *   grad_gamma  dJ/dgamma with gamma = 1/invnu of every bath moved together (per fs^-1)
  *   grad_rho0   [states*states*2]: dJ/dRe rho0_ij, dJ/dIm rho0_ij
- * Any output pointer may be NULL.  Masks are not supported. */
+ * Any output pointer may be NULL: the sweep then skips that gradient's
+ * accumulation (grad_h: the Z reduction; grad_lambda and grad_gamma both
+ * NULL: the bath-derivative terms).  Masks are not supported. */
 typedef struct heom_adjoint heom_adjoint;
 int heom_adjoint_create(const heom_system_desc* sys, const heom_options* opt, heom_adjoint** out);
 /* A batch of K systems that share states, baths and bath parameters (they
