@@ -1,7 +1,12 @@
-// app_linear_absorption.cpp -- linear absorption on one B200.
+// app_linear_absorption.cpp -- linear absorption (and, built with
+// HEOM_CIRCULAR_DICHROISM, circular dichroism) on one B200.
 //
 // Same command line and flow as dm-heom/src/app_linear_absorption.cpp:39-183:
 //   heom_linear_absorption <runtime_config> <heom_config>
+// and dm-heom/src/app_circular_dichroism.cpp:36-174:
+//   heom_circular_dichroism <runtime_config> <heom_config>
+// which differs in D-: the magnetic dipole (center x direction,
+// dipole_matrix.hpp:43-48, 60-64), and applies no filtering mask.
 // For every dipole tensor component t (dipole.tensor_prefactors /
 // dipole.tensor_components): the state system with a ground state
 // (sites_to_states with_ground_state), the top |g><g| with every other ADO
@@ -32,6 +37,14 @@
 using namespace heomhost;
 
 namespace {
+
+#ifdef HEOM_CIRCULAR_DICHROISM
+constexpr bool kCircular = true;
+const char* const kTask = "circular_dichroism";
+#else
+constexpr bool kCircular = false;
+const char* const kTask = "linear_absorption";
+#endif
 
 void check(int rc)
 {
@@ -115,7 +128,7 @@ int main(int argc, char* argv[])
         heom_options opt = read_runtime_options(argv[1]);
         std::cout << "Parsing HEOM configuration from file: " << argv[2] << std::endl;
         heomhost::config cfg(argv[2]);
-        if (cfg.task() != "linear_absorption") throw config_error("wrong program_task for this application");
+        if (cfg.task() != kTask) throw config_error("wrong program_task for this application");
         const std::string& out_name = cfg.observations().front().filename;
         std::ofstream out(out_name);
         if (out.fail()) throw std::runtime_error("Error: could not open output file: " + out_name);
@@ -138,7 +151,7 @@ int main(int argc, char* argv[])
                 tops0[k][2 * (i * m)] = dplus[2 * (i * m)];
                 tops0[k][2 * (i * m) + 1] = dplus[2 * (i * m) + 1];
             }
-            dminus[k] = pathway_dipole_matrix(cfg, k, 0);
+            dminus[k] = pathway_dipole_matrix(cfg, k, 0, kCircular);
             const double pf = cfg.dipole_tensor_prefactors()[k]; // pathway sign plus
             for (double& v : dminus[k]) v *= pf;
         }
@@ -148,12 +161,14 @@ int main(int argc, char* argv[])
         check(heom_create_batch(descs.data(), (int32_t)K, &opt, &h));
         std::unique_ptr<heom_handle, int (*)(heom_handle*)> guard(h, heom_destroy);
 
-        hierarchy_graph g(inst.width, sys.depth);
-        const std::vector<uint8_t> mask1 =
-            make_mask(cfg.filtering_strategy(), g, sys.matsubaras, cfg.filtering_first_layer());
-        std::vector<uint8_t> mask;
-        for (size_t k = 0; k < K; ++k) mask.insert(mask.end(), mask1.begin(), mask1.end());
-        check(heom_set_mask(h, mask.data()));
+        if (!kCircular) { // the circular-dichroism application sets no mask
+            hierarchy_graph g(inst.width, sys.depth);
+            const std::vector<uint8_t> mask1 =
+                make_mask(cfg.filtering_strategy(), g, sys.matsubaras, cfg.filtering_first_layer());
+            std::vector<uint8_t> mask;
+            for (size_t k = 0; k < K; ++k) mask.insert(mask.end(), mask1.begin(), mask1.end());
+            check(heom_set_mask(h, mask.data()));
+        }
 
         for (size_t k = 0; k < K; ++k) check(heom_set_instance_top(h, (int32_t)k, tops0[k].data()));
 

@@ -1,7 +1,9 @@
-// config.cpp -- population_dynamics and linear_absorption configuration files.
+// config.cpp -- population_dynamics, linear_absorption and circular_dichroism
+// configuration files.
 //
 // Reads the reference's INI files (dm-heom/src/heom/config.cpp:37-67,
 // population_dynamics_config.cpp:24-26, linear_absorption_config.cpp:17-53,
+// circular_dichroism_config.cpp:17-53,
 // dipole_config_entries.cpp:19-41, config_base.cpp:32): "[section]"
 // headers, "key=value" lines, '#' comments to the end of a line; values are
 // noma/typa literals -- numbers, booleans, braced lists "{a, b}", braced
@@ -51,7 +53,7 @@ const std::set<std::string>& task_keys(const std::string& task)
     static const std::set<std::string> la = {"dipole.directions", "dipole.strengths", "dipole.centers",
                                              "dipole.tensor_prefactors", "dipole.tensor_components"};
     static const std::set<std::string> none;
-    return task == "population_dynamics" ? pd : task == "linear_absorption" ? la : none;
+    return task == "population_dynamics" ? pd : (task == "linear_absorption" || task == "circular_dichroism") ? la : none;
 }
 
 bool any_task_key(const std::string& key)
@@ -179,8 +181,9 @@ config::config(const std::string& path)
 
     // program (config_base.cpp:32, config.cpp:39-40)
     task_ = raw("program.task");
-    if (task_ != "population_dynamics" && task_ != "linear_absorption")
-        throw config_error("program.task '" + task_ + "' is not supported (population_dynamics, linear_absorption)");
+    if (task_ != "population_dynamics" && task_ != "linear_absorption" && task_ != "circular_dichroism")
+        throw config_error("program.task '" + task_ +
+                           "' is not supported (population_dynamics, linear_absorption, circular_dichroism)");
     for (const auto& kv : values_)
         if (!known_keys().count(kv.first) && !task_keys(task_).count(kv.first))
             throw config_error("unrecognised option '" + kv.first + "'");

@@ -170,11 +170,13 @@ system_params state_system(const system_params& sites, sites_to_states_mode mode
 // dipole_matrix.cpp:105-131 (with_ground_state): D(0, i+1) = v_i, every other
 // entry zero; row-major states x states complex, interleaved
 std::vector<double> dipole_matrix(const std::vector<double>& dipole_vector);
-// dipole_matrix.hpp:30-58 for the linear-absorption pseudo pathway
-// (dipole_pseudo_pathway.hpp:22-27: {minus, left}, {plus, left}): v_i =
-// directions[i][component] * strengths[i] with component =
-// tensor_components[tensor][spec]; spec 1 (plus) is the transpose
-std::vector<double> pathway_dipole_matrix(const config& cfg, size_t tensor, size_t spec);
+// dipole_matrix.hpp:30-58 for the pseudo pathway of linear absorption and
+// circular dichroism (dipole_pseudo_pathway.hpp:22-27: {minus, left},
+// {plus, left}): v_i = directions[i][component] * strengths[i] with component
+// = tensor_components[tensor][spec], or for the magnetic dipole (circular)
+// v_i = (centers[i] x directions[i])[component] * strengths[i]
+// (dipole_matrix.hpp:43-48); spec 1 (plus) is the transpose
+std::vector<double> pathway_dipole_matrix(const config& cfg, size_t tensor, size_t spec, bool circular = false);
 
 // literal parsing (noma/typa-style values)
 std::vector<std::string> split_braced(const std::string& s); // "{a, {b}, (c, d)}" -> items

@@ -1,5 +1,5 @@
 // spectra.cpp -- state systems with a ground state and dipole matrices for
-// the spectroscopy applications (linear absorption).
+// the spectroscopy applications (linear absorption, circular dichroism).
 //
 // The sites -> states map follows dm-heom/src/heom/sites_to_states.cpp:16-28,
 // 44-55, 131-142; the dipole matrices follow dipole_matrix.cpp:105-131 and
@@ -37,19 +37,29 @@ std::vector<double> dipole_matrix(const std::vector<double>& v)
     return d;
 }
 
-std::vector<double> pathway_dipole_matrix(const config& cfg, size_t tensor, size_t spec)
+std::vector<double> pathway_dipole_matrix(const config& cfg, size_t tensor, size_t spec, bool circular)
 {
     const auto& comps = cfg.dipole_tensor_components();
     if (tensor >= comps.size() || spec >= comps[tensor].size())
         throw config_error("dipole.tensor_components has no entry for this pathway");
     const int64_t c = comps[tensor][spec];
     const auto& dirs = cfg.dipole_directions();
+    const auto& ctrs = cfg.dipole_centers();
     const int sites = cfg.system().states;
     if ((int64_t)dirs.size() < sites) throw config_error("dipole.directions needs one direction per site");
     std::vector<double> v(sites);
     for (int i = 0; i < sites; ++i) {
         if (c < 0 || c >= (int64_t)dirs[i].size()) throw config_error("dipole.tensor_components out of range");
-        v[i] = dirs[i][c] * cfg.dipole_strengths()[i];
+        double d = dirs[i][c];
+        if (circular) { // (center x direction)[c], dipole_matrix.cpp:14-25
+            if (dirs[i].size() != 3 || ctrs[i].size() != 3 || c > 2)
+                throw config_error("circular dichroism needs 3-vectors in dipole.centers and dipole.directions");
+            const std::vector<double>& a = ctrs[i];
+            const std::vector<double>& b = dirs[i];
+            const double cx[3] = {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+            d = cx[c];
+        }
+        v[i] = d * cfg.dipole_strengths()[i];
     }
     std::vector<double> d = dipole_matrix(v);
     if (spec == 1) { // the plus dipole of the pathway: the transpose

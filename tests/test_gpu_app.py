@@ -15,6 +15,7 @@ pytestmark = pytest.mark.gpu
 
 APP = os.path.join(os.path.dirname(hb.__file__), "bin", "heom_population_dynamics")
 LA_APP = os.path.join(os.path.dirname(hb.__file__), "bin", "heom_linear_absorption")
+CD_APP = os.path.join(os.path.dirname(hb.__file__), "bin", "heom_circular_dichroism")
 
 
 def read_dat(path):
@@ -127,3 +128,42 @@ def test_linear_absorption_app_matches_oracle(tmp_path, scheme, filtering):
     assert np.max(np.abs(got[:, 2] - want.imag)) <= 1e-10 * scale
     # at t = 0 the trace is the mean squared dipole length over the components
     assert abs(want[0] - sum(np.sum((dirs[:, c] * strengths) ** 2) for c in range(3)) / 3) <= 1e-12 * scale
+
+
+def test_circular_dichroism_app_matches_oracle(tmp_path):
+    """As linear absorption with the magnetic dipole (center x direction) in
+    D- and no filtering mask (the configured filter is not applied)."""
+    cfg = LA_CFG.replace("task=linear_absorption", "task=circular_dichroism").replace(
+        "strategy=none", "strategy=single_excitation").replace("first_layer=-1", "first_layer=1")
+    (tmp_path / "heom.cfg").write_text(cfg)
+    (tmp_path / "rt.cfg").write_text("[cuda]\ndevice_index=0\n")
+    r = subprocess.run([CD_APP, "rt.cfg", "heom.cfg"], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    hdr, got = read_dat(tmp_path / "la.dat")
+    assert hdr == ["time", "trace_real", "trace_imag"]
+    h = np.array([[12410.0, -87.7, 5.5], [-87.7, 12530.0, 30.8], [5.5, 30.8, 12210.0]])
+    hs = np.zeros((4, 4))
+    hs[1:, 1:] = h
+    coupling = np.array([[-1], [0], [1], [2]], np.int32)
+    prob = ho.build_problem(ho.make_system(hs, [35] * 3, [50] * 3, [0] * 3, 2, 77.0, 3, coupling=coupling))
+    dirs = np.array([[-0.741, -0.561, -0.370], [-0.857, 0.504, -0.107], [-0.197, 0.957, -0.211]])
+    ctrs = np.array([[2.651, 0.260, -1.135], [1.561, -0.152, -1.725], [0.339, -1.361, -1.385]])
+    strengths = np.array([4, 3.5, 4.2])
+    mag = np.cross(ctrs, dirs)
+    want = np.zeros(5, complex)
+    for comp in range(3):
+        dm = np.zeros((4, 4))
+        dm[0, 1:] = mag[:, comp] * strengths
+        dp = np.zeros((4, 4))
+        dp[1:, 0] = dirs[:, comp] * strengths
+        y = np.zeros(prob.state_len)
+        y[0:32:2] = (dp @ np.diag([1.0, 0, 0, 0])).reshape(-1)
+        for row in range(5):
+            if row:
+                y, _ = ho.propagate(prob, 1e-15, 5, 5, y=y)
+            rho = (y[0:32:2] + 1j * y[1:32:2]).reshape(4, 4)
+            want[row] += np.trace(dm @ rho)
+    want /= 3
+    scale = np.max(np.abs(want))
+    assert np.max(np.abs(got[:, 1] - want.real)) <= 1e-10 * scale
+    assert np.max(np.abs(got[:, 2] - want.imag)) <= 1e-10 * scale

@@ -168,6 +168,19 @@ def test_linear_absorption_app_reports_config_errors_before_the_device(tmp_path,
     assert r.returncode != 0 and "out of range" in r.stderr
 
 
+def test_circular_dichroism_config_and_app_tasks(tmp_path, root):
+    cd = LA_CFG.replace("task=linear_absorption", "task=circular_dichroism")
+    (tmp_path / "cd.cfg").write_text(cd)
+    assert hb.Config(tmp_path / "cd.cfg").get("program.task") == "circular_dichroism"
+    (tmp_path / "la.cfg").write_text(LA_CFG)
+    (tmp_path / "rt.cfg").write_text("[cuda]\ndevice_index=0\n")
+    bins = os.path.join(root, "dm-heom_b200", "bin")
+    for app, cfg in (("heom_circular_dichroism", "la.cfg"), ("heom_linear_absorption", "cd.cfg")):
+        r = subprocess.run([os.path.join(bins, app), "rt.cfg", cfg], cwd=tmp_path, capture_output=True,
+                           text=True, timeout=60)
+        assert r.returncode != 0 and "wrong program_task" in r.stderr
+
+
 def test_config_missing_file():
     with pytest.raises(hb.HeomError):
         hb.Config("/nonexistent/file.cfg")
