@@ -29,9 +29,12 @@ def alone(prob, steps, every, **kw):
         return H.propagate(DT, steps, every)
 
 
-def disorder_problems(count, n, depths, m, seed):
+def disorder_problems(count, n, depths, m, seed, complex_h=False):
     rng = np.random.default_rng(seed)
     base = ho.synthetic_hamiltonian(n, seed)
+    if complex_h:  # Hermitian with an imaginary antisymmetric part
+        im = np.triu(rng.normal(0.0, 20.0, size=(n, n)), 1)
+        base = base + 1j * (im - im.T)
     out = []
     for k in range(count):
         h = base.copy()
@@ -42,10 +45,12 @@ def disorder_problems(count, n, depths, m, seed):
     return out
 
 
-@pytest.mark.parametrize("n,m,depths", [(7, 1, [3, 4]), (5, 2, [2, 3]), (10, 1, [2, 3])])
+@pytest.mark.parametrize("n,m,depths,complex_h", [(7, 1, [3, 4], False), (5, 2, [2, 3], False),
+                                                 (10, 1, [2, 3], False), (6, 2, [2, 3], True),
+                                                 (9, 2, [1, 2], True), (13, 1, [1, 2], False)])
 @pytest.mark.parametrize("scheme", ["product", "reference"])
-def test_batch_bitwise_equal_to_single_instances(n, m, depths, scheme):
-    probs = disorder_problems(3, n, depths, m, seed=40 + n)
+def test_batch_bitwise_equal_to_single_instances(n, m, depths, complex_h, scheme):
+    probs = disorder_problems(3, n, depths, m, seed=40 + n, complex_h=complex_h)
     with hb.Heom.batch([hb.Heom.tables_of(p) for p in probs], scheme=scheme) as H:
         assert H.instances == 3
         for k, p in enumerate(probs):
