@@ -86,7 +86,7 @@ struct PairParams {
     double2 acc_beta;                // acc = (acc_init ? in : acc) + acc_beta * L
     int acc_init;
     int use_acc;
-    const int32_t* __restrict__ nbr; // [nodes][NW]: plus[W], minus[W], padded to NW (multiple of 4)
+    const int32_t* __restrict__ nbr; // [nodes][NW]: (plus, minus) of every slot, padded to NW (multiple of 4)
     const uint8_t* __restrict__ tup; // [nodes][TWB] tuple bytes, padded to TWB (multiple of 16)
     const double2* __restrict__ pss; // [nodes]
     const double* __restrict__ hfrag;  // [n_inst][frag_doubles(N)] MMA operand fragments of H / hbar
@@ -122,11 +122,12 @@ __host__ __device__ constexpr int tile_pos(int n, int i, int k) { return i * til
 constexpr int kXchStride = 17;
 constexpr int kXchBytes = 16 * kXchStride * 16;
 
-// shared look-up tables of both stage kernels: khat 3*W double2, chat W doubles,
-// sqrt LS+1 doubles, pos W int16 (the last read by the team kernel only)
+// shared look-up tables of both stage kernels: khat 3*W double2, (sqrt(n),
+// sqrt(n+1)) LS+1 double2, chat W doubles, pos W int16 (the last read by the
+// team kernel only)
 __host__ __device__ inline int dmma_lut_bytes(int W, int LS)
 {
-    return ((3 * W * 16 + W * 8 + (LS + 1) * 8 + W * 2) + 15) & ~15;
+    return ((3 * W * 16 + (LS + 1) * 16 + W * 8 + W * 2) + 15) & ~15;
 }
 
 // dynamic shared memory carve-up (bytes); everything 16-B aligned
@@ -335,11 +336,12 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_dmma_stage(const DmmaP
     const int W = p.W, LS = p.LS, SL = p.SL;
 
     double2* s_kh = reinterpret_cast<double2*>(smem);            // 3 * W
-    double* s_ch = reinterpret_cast<double*>(s_kh + 3 * W);       // W
-    double* s_sq = s_ch + W;                                      // LS + 1
+    double2* s_sq = s_kh + 3 * W;                                 // LS + 1: (sqrt(n), sqrt(n+1))
+    double* s_ch = reinterpret_cast<double*>(s_sq + LS + 1);      // W
     for (int q = threadIdx.x; q < 3 * W; q += blockDim.x) s_kh[q] = dp.ct.khat[q];
     for (int q = threadIdx.x; q < W; q += blockDim.x) s_ch[q] = dp.ct.chat[q];
-    for (int q = threadIdx.x; q <= LS; q += blockDim.x) s_sq[q] = dp.ct.sq[q];
+    for (int q = threadIdx.x; q <= LS; q += blockDim.x)
+        s_sq[q] = make_double2(dp.ct.sq[q], q < LS ? dp.ct.sq[q + 1] : 0.0);
     const int lut = dmma_lut_bytes(W, LS);
 
     const int warp = threadIdx.x >> 5;
@@ -494,8 +496,9 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_dmma_stage(const DmmaP
                 for (int q = 0; q < SLT; ++q) {
                     const int sl = sd == 0 ? sli[q] : slj[q];
                     // diagonal elements: the plus terms of L cancel (the minus terms of L^H)
-                    const int32_t vp = (sl >= 0 && (ADJ || !diag)) ? nb[sl] : -1;
-                    const int32_t vm = (sl >= 0 && (!ADJ || !diag)) ? nb[W + sl] : -1;
+                    const int2 pm = sl >= 0 ? reinterpret_cast<const int2*>(nb)[sl] : make_int2(-1, -1);
+                    const int32_t vp = (ADJ || !diag) ? pm.x : -1;
+                    const int32_t vm = (!ADJ || !diag) ? pm.y : -1;
                     nn[q] = sl >= 0 ? tu[sl] : 0;
                     xp[q][0] = xp[q][1] = xm[q][0] = xm[q][1] = make_double2(0.0, 0.0);
                     if (vp >= 0) ld256(p.in + (int64_t)vp * (2 * P) + 2 * lane, xp[q][0], xp[q][1]);
@@ -506,7 +509,8 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_dmma_stage(const DmmaP
                     const int sl = sd == 0 ? sli[q] : slj[q];
                     if (sl < 0) continue;
                     const int ps = sd == 0 ? pi[q] : pj[q];
-                    const double sq_lo = s_sq[nn[q]], sq_hi = s_sq[nn[q] + 1];
+                    const double2 sqp = s_sq[nn[q]];
+                    const double sq_lo = sqp.x, sq_hi = sqp.y;
                     // L:   i-coefficient term on the plus neighbour (chat sqrt(n+1)),
                     //      complex term on the minus neighbour (khat sqrt(n))
                     // L^H: i-coefficient term on the minus neighbour (-chat sqrt(n)),
@@ -634,12 +638,13 @@ __global__ void __launch_bounds__(kCtaWarps * 32, SLT <= 2 ? 3 : 2) heom_pair_st
     const int W = p.W, LS = p.LS, SL = p.SL;
 
     double2* s_kh = reinterpret_cast<double2*>(smem);      // 3 * W
-    double* s_ch = reinterpret_cast<double*>(s_kh + 3 * W); // W
-    double* s_sq = s_ch + W;                                // LS + 1
-    int16_t* s_pos = reinterpret_cast<int16_t*>(s_sq + LS + 1); // W
+    double2* s_sq = s_kh + 3 * W;                           // LS + 1: (sqrt(n), sqrt(n+1))
+    double* s_ch = reinterpret_cast<double*>(s_sq + LS + 1); // W
+    int16_t* s_pos = reinterpret_cast<int16_t*>(s_ch + W);   // W
     for (int q = threadIdx.x; q < 3 * W; q += blockDim.x) s_kh[q] = dp.ct.khat[q];
     for (int q = threadIdx.x; q < W; q += blockDim.x) s_ch[q] = dp.ct.chat[q];
-    for (int q = threadIdx.x; q <= LS; q += blockDim.x) s_sq[q] = dp.ct.sq[q];
+    for (int q = threadIdx.x; q <= LS; q += blockDim.x)
+        s_sq[q] = make_double2(dp.ct.sq[q], q < LS ? dp.ct.sq[q + 1] : 0.0);
     for (int q = threadIdx.x; q < W; q += blockDim.x) s_pos[q] = dp.ct.pos[q];
 
     const int team = threadIdx.x / TT;
@@ -749,8 +754,9 @@ __global__ void __launch_bounds__(kCtaWarps * 32, SLT <= 2 ? 3 : 2) heom_pair_st
 #pragma unroll
                 for (int q = 0; q < SLT; ++q) {
                     const int sl = sd == 0 ? sli[q] : slj[q];
-                    const int32_t vp = (sl >= 0 && (ADJ || !diag)) ? nb[sl] : -1;
-                    const int32_t vm = (sl >= 0 && (!ADJ || !diag)) ? nb[W + sl] : -1;
+                    const int2 pm = sl >= 0 ? reinterpret_cast<const int2*>(nb)[sl] : make_int2(-1, -1);
+                    const int32_t vp = (ADJ || !diag) ? pm.x : -1;
+                    const int32_t vm = (!ADJ || !diag) ? pm.y : -1;
                     nn[q] = sl >= 0 ? tu[sl] : 0;
                     xp[q][0] = xp[q][1] = xm[q][0] = xm[q][1] = make_double2(0.0, 0.0);
                     if (vp >= 0) ld256(p.in + (int64_t)vp * (2 * P) + 2 * lt, xp[q][0], xp[q][1]);
@@ -761,7 +767,8 @@ __global__ void __launch_bounds__(kCtaWarps * 32, SLT <= 2 ? 3 : 2) heom_pair_st
                     const int sl = sd == 0 ? sli[q] : slj[q];
                     if (sl < 0) continue;
                     const int ps = s_pos[sl];
-                    const double sq_lo = s_sq[nn[q]], sq_hi = s_sq[nn[q] + 1];
+                    const double2 sqp = s_sq[nn[q]];
+                    const double sq_lo = sqp.x, sq_hi = sqp.y;
                     // L: i chat sqrt(n+1) on the plus neighbour, khat sqrt(n) on the minus one;
                     // L^H: -i chat sqrt(n) on the minus neighbour, conj(khat) sqrt(n+1) on the plus one
                     const double c = diag ? 0.0 : (ADJ ? -s_ch[ps] * sq_lo : s_ch[ps] * sq_hi);
@@ -954,7 +961,7 @@ __global__ void heom_write_top(double2* __restrict__ y, const double2* __restric
 struct GradParams {
     const double2* __restrict__ a;     // adjoint (pair layout, internal order)
     const double2* __restrict__ w;     // forward stage input
-    const int32_t* __restrict__ nbr;   // [nodes][NW] plus[W], minus[W]
+    const int32_t* __restrict__ nbr;   // [nodes][NW] (plus, minus) of every slot
     const uint8_t* __restrict__ tup;   // [nodes][TWB]
     const int16_t* __restrict__ pe;    // [2P] element indices of the sector halves
     const int16_t* __restrict__ slots; // [N][SL] slot ids of each state, -1 padded
@@ -1033,8 +1040,9 @@ __global__ void __launch_bounds__(kCtaWarps * 32) heom_adjoint_grad(const GradPa
                     const int sl = g.slots[site * SL + q];
                     if (sl < 0) continue;
                     const int n = tu[sl];
-                    const int32_t vp = diag ? -1 : nb[sl];
-                    const int32_t vm = nb[W + sl];
+                    const int2 pm = reinterpret_cast<const int2*>(nb)[sl];
+                    const int32_t vp = diag ? -1 : pm.x;
+                    const int32_t vm = pm.y;
                     double2 p1 = make_double2(0.0, 0.0), p2 = p1, m1 = p1, m2 = p1;
                     if (vp >= 0) { p1 = g.w[((int64_t)vp * P + p) * 2]; p2 = g.w[((int64_t)vp * P + p) * 2 + 1]; }
                     if (vm >= 0) { m1 = g.w[((int64_t)vm * P + p) * 2]; m2 = g.w[((int64_t)vm * P + p) * 2 + 1]; }

@@ -323,8 +323,8 @@ int build_neighbours(heom_handle* h)
                 if (has_plus && pr >= 0 && h->mask[pr]) pv = (int32_t)h->int_of_ref[pr];
                 const int32_t mr = h->minus[r * W + m];
                 if (t > 0 && mr >= 0 && h->mask[mr]) mv = (int32_t)h->int_of_ref[mr];
-                nbr[u * NW + m] = pv;
-                nbr[u * NW + W + m] = mv;
+                nbr[u * NW + 2 * m] = pv;
+                nbr[u * NW + 2 * m + 1] = mv;
             }
             pss[u] = make_double2(h->pss[2 * r], h->pss[2 * r + 1]);
             if (h->n_inst > 1) inst[u] = k;

@@ -28,8 +28,8 @@ int main()
             for (int depth = 1; depth <= 40; ++depth) {
                 const int LS = depth + 1, NW = (2 * W + 3) & ~3, TWB = (W + 15) & ~15;
                 const heomk::PairSmem L = heomk::pair_smem_layout(n, W, NW, TWB, LS);
-                // khat 3W double2, chat W doubles, sqrt(n) for n = 0..LS
-                if (3 * W * 16 + W * 8 + (LS + 1) * 8 > L.lut) { printf("bad lut n=%d W=%d LS=%d\n", n, W, LS); ++bad; }
+                // khat 3W double2, (sqrt(n), sqrt(n+1)) for n = 0..LS, chat W doubles, pos W int16
+                if (3 * W * 16 + (LS + 1) * 16 + W * 8 + W * 2 > L.lut) { printf("bad lut n=%d W=%d LS=%d\n", n, W, LS); ++bad; }
                 if (L.lut % 16 || L.slot % 16 || L.team % 16 || L.tile_off % 16 || L.nbr_off % 16 ||
                     L.tup_off % 16 || L.pss_off % 16 || L.xch_off % 16) { printf("bad slot n=%d W=%d\n", n, W); ++bad; }
                 if (L.nbr_off - L.tile_off < n * heomk::tile_stride(n) * 16 || L.tup_off - L.nbr_off < NW * 4 ||
