@@ -416,6 +416,9 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_dmma_stage(const DmmaP
     unsigned ph0 = 0u, ph1 = 0u; // mbarrier phase parity of slot 0 / slot 1
     // instance of the current ADO (warp-uniform); its fragments are in hb_* / ha_*
     int ci = (MI && u < nodes) ? __ldg(p.inst + u) : 0;
+    // the next ADO's instance, read one iteration ahead of its use so that the
+    // instance compare never waits on the load
+    int ni_ahead = (MI && u + stride < nodes) ? __ldg(p.inst + u + stride) : ci;
     load_frag(ci, hb_r, hb_i, ha_r, ha_i);
 
     auto issue = [&](int64_t v, int sl) {
@@ -437,8 +440,9 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_dmma_stage(const DmmaP
         int ni = ci;
         double nb_r[2], nb_i[2], na_r[2], na_i[2];
         if (MI && un < nodes) {
-            ni = __ldg(p.inst + un);
+            ni = ni_ahead;
             if (ni != ci) load_frag(ni, nb_r, nb_i, na_r, na_i);
+            ni_ahead = un + stride < nodes ? __ldg(p.inst + un + stride) : ni;
         }
         if (!mbar_wait(&bars[cur], cur ? ph1 : ph0)) {
             failed = true;
