@@ -112,7 +112,7 @@ __host__ __device__ constexpr int frag_index(int n, int kind, int b, int s, int 
     return ((kind * frag_blocks(n) + b) * frag_slices(n) + s) * 32 + lane;
 }
 
-// SIMT-team kernel (N = 9..16): the staged ADO is row-major with row stride
+// Team kernel (N = 9..16): the staged ADO is row-major with row stride
 // TS = 4 (mod 8) double2 and the columns of rows with bit 1 set swapped in
 // pairs (k ^ 2), so that the quarter-warp reads of both MMA operands,
 // A = w(8I+g, 4s+t) and B = w(4s+t, 8J+g), hit eight distinct 16-byte bank groups.

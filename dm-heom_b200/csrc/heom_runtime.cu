@@ -114,7 +114,7 @@ stage_fn_t pick_n(int hk, int slt, bool adj)
                                    : pick_slt<N, heomk::H_GENERIC, false>(slt);
 }
 
-// SIMT pair kernel: N = 9..16
+// team kernel (tensor-pipe commutator, a team of warps per ADO): N = 9..16
 stage_fn_t pick_stage(int n, int hk, int slt, bool adj)
 {
     switch (n) {
@@ -248,7 +248,7 @@ struct heom_handle {
     DevBuf<int32_t> d_inst;          // instance of each internal ADO (n_inst > 1)
     DevBuf<int64_t> d_top;
     DevBuf<int16_t> d_slots;
-    DevBuf<double> d_chat, d_sq;     // factored coefficients (DMMA kernel)
+    DevBuf<double> d_chat, d_sq;     // factored bath coefficients (both stage kernels)
     DevBuf<double2> d_khat;
     DevBuf<int16_t> d_pos;
     DevBuf<int64_t> d_int_of_ref, d_ref_of_int;
