@@ -1019,8 +1019,9 @@ __global__ void __launch_bounds__(kCtaWarps * 32) heom_adjoint_grad(const GradPa
         for (int p = lane; p < P; p += 32) {
             const int e1 = g.pe[2 * p], e2 = g.pe[2 * p + 1];
             const int i1 = e1 / N, j1 = e1 - i1 * N, i2 = e2 / N, j2 = e2 - i2 * N;
-            const double2 a1 = g.a[(u * P + p) * 2], a2 = g.a[(u * P + p) * 2 + 1];
-            const double2 w1 = g.w[(u * P + p) * 2], w2 = g.w[(u * P + p) * 2 + 1];
+            double2 a1, a2, w1, w2;
+            ld256(g.a + (u * P + p) * 2, a1, a2);
+            ld256(g.w + (u * P + p) * 2, w1, w2);
             At[i1 * (N + 1) + j1] = a1;
             At[i2 * (N + 1) + j2] = a2;
             Wt[i1 * (N + 1) + j1] = w1;
@@ -1048,8 +1049,8 @@ __global__ void __launch_bounds__(kCtaWarps * 32) heom_adjoint_grad(const GradPa
                     const int32_t vp = diag ? -1 : pm.x;
                     const int32_t vm = pm.y;
                     double2 p1 = make_double2(0.0, 0.0), p2 = p1, m1 = p1, m2 = p1;
-                    if (vp >= 0) { p1 = g.w[((int64_t)vp * P + p) * 2]; p2 = g.w[((int64_t)vp * P + p) * 2 + 1]; }
-                    if (vm >= 0) { m1 = g.w[((int64_t)vm * P + p) * 2]; m2 = g.w[((int64_t)vm * P + p) * 2 + 1]; }
+                    if (vp >= 0) ld256(g.w + ((int64_t)vp * P + p) * 2, p1, p2);
+                    if (vm >= 0) ld256(g.w + ((int64_t)vm * P + p) * 2, m1, m2);
                     const double shi = g.sq[n + 1], slo = g.sq[n];
                     for (int th = 0; th < 2; ++th) {
                         const double c = g.dchat[th * W + sl] * shi;
