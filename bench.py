@@ -1,5 +1,5 @@
 #!/usr/bin/env python3
-"""Benchmark: HEOM ADO-updates/s in FP64 on B200.
+"""Benchmark: HEOM ADO-updates/s in FP64 on B200; batched & adjoint vs plain.
 
 Workload (one GPU): 8 sites, one Drude-Lorentz bath per site (lambda = 35
 cm^-1, invnu = 50 fs, T = 300 K) with one Matsubara term (16 modes), depth 8:
@@ -19,8 +19,18 @@ hierarchy; 1 ADO-update = one ADO advanced through one RK4 step.
             algorithmic bytes per launch = ADOs x 32 N^2 B (read the stage
             input, write the stage output) / average launch duration
   cpu_baseline  the reference's own heom_ode.cl + rk_weighted_add.cl compiled
-            for the host (oracle/_ref) with OpenMP over all host cores, one
-            RK4 step of the same workload
+            for the host (oracle/_ref) with OpenMP over all host cores, RK4
+            steps of the same workload
+  parity    the GPU state after the same RK4 steps from the same initial
+            state against that reference run: the error per result
+  batched   256 static-disorder realisations of a 7-site system, depth 6, in
+            one ensemble (one graph launch per RK4 step) against the same
+            realisations solved one after another; populations of a sample
+            of realisations against the oracle
+  adjoint   gradients of the time-integrated site-3 population of a 7-site,
+            depth-8 system (2000 steps) w.r.t. 7 site energies, 21 couplings,
+            lambda and gamma by one adjoint sweep, against central finite
+            differences of 60 + 4 forward solves
 
 --impl reference times that CPU implementation as the reference arm.
 Multi-GPU (torchrun): every rank propagates its own replica of the hierarchy
@@ -30,6 +40,7 @@ sum of ADO-updates over ranks / the max over ranks of the device time.
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
 import subprocess
@@ -42,11 +53,12 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "dm-heom_b200"))
 
-METRIC = "HEOM ADO-updates/s FP64 on 1 B200; batched & adjoint vs plain at \u22641e-10 error"
+METRIC = "HEOM ADO-updates/s FP64 on 1 B200; batched & adjoint vs plain at ≤1e-10 error"
 UNIT = "ADO-updates/s"
 N_SITES, DEPTH, MATSUBARAS, SEED, DT = 8, 8, 2, 22, 0.5e-15
 OBSERVE_EVERY = 10
 FALLBACK_HBM = 6650.0
+POP_FLOOR = 1e-3  # relative population errors: |dp| / max(|p_ref|, POP_FLOOR)
 
 
 def synthetic_h(n, seed):
@@ -58,6 +70,11 @@ def synthetic_h(n, seed):
     h = h + h.T
     h[np.diag_indices(n)] = diag
     return h
+
+
+def rel_pop_err(got, ref):
+    got, ref = np.asarray(got, np.float64), np.asarray(ref, np.float64)
+    return float(np.max(np.abs(got - ref) / np.maximum(np.abs(ref), POP_FLOOR)))
 
 
 def workload_config(scheme, depth=DEPTH, ados=735471, sites=N_SITES, matsubaras=MATSUBARAS):
@@ -80,8 +97,9 @@ class ClockSampler:
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
               "clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index):
+    def __init__(self, index, period_ms=100):
         self.index = index
+        self.period_ms = period_ms
         self.proc = None
         self.lines = []
         self.thread = None
@@ -90,7 +108,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", str(self.period_ms)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
@@ -141,28 +159,47 @@ def measured_hbm_peak():
         return FALLBACK_HBM, "fallback"
 
 
+def kernel_source_hash():
+    """Hash of the stage kernel's sources (the kernel header and its sector tables)."""
+    h = hashlib.sha256()
+    for rel in ("dm-heom_b200/csrc/heom_kernels.cuh", "dm-heom_b200/csrc/pair_tables.inc"):
+        with open(os.path.join(ROOT, rel), "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()[:16]
+
+
 def profiled_traffic():
-    """Per-launch DRAM bytes of the benchmark stage kernel from the committed ncu summary."""
+    """Per-launch DRAM bytes of the benchmark stage kernel from the committed ncu
+    summary, used only when the summary was taken on this build of the kernel
+    (its kernel_source_hash line matches); otherwise None."""
     path = os.path.join(ROOT, "profiles", "heom_stage_cfg2.md")
+    traffic, src = None, None
     try:
         for line in open(path):
-            if line.strip().startswith("traffic_bytes_per_launch"):
-                return float(line.split("=")[1].strip().split()[0])
+            ln = line.strip()
+            if ln.startswith("traffic_bytes_per_launch"):
+                traffic = float(ln.split("=")[1].strip().split()[0])
+            if ln.startswith("kernel_source_hash"):
+                src = ln.split("=")[1].strip().split()[0]
     except Exception:
-        pass
-    return None
+        return None, "no profile summary"
+    if traffic is None or src != kernel_source_hash():
+        return None, "profile summary taken on another build of the kernel"
+    return traffic, "ncu dram__bytes_read.sum + dram__bytes_write.sum of this build (profiles/heom_stage_cfg2.md)"
 
 
-def cpu_reference_sample(steps_cap=1, scheme_note="reference"):
+def cpu_reference_sample(steps_cap=1):
     """Time the reference's own kernels (compiled for the host) on the bench
-    workload: RK4 steps of the full hierarchy with all host threads."""
+    workload: RK4 steps of the full hierarchy with all host threads.  Returns
+    the baseline record and the state after 1 + steps_cap steps from the
+    initial state (one untimed warm-up step, then the timed ones)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import heom_oracle as ho
     prob = ho.build_problem(ho.drude_system(N_SITES, DEPTH, MATSUBARAS, seed=SEED))
     y = prob.initial_state()
     threads = os.cpu_count() or 1
-    kind = "reference" if ho.ref_lib() is not None else "port"
-    step = (lambda v: ho.ref_rk4_step(prob, DT, v, threads)) if kind == "reference" else \
+    kind = "reference" if ho.ref_lib(fast=True) is not None else "port"
+    step = (lambda v: ho.ref_rk4_step(prob, DT, v, threads, fast=True)) if kind == "reference" else \
         (lambda v: ho.rk4_step(prob, DT, v, threads))
     y = step(y)  # warm-up (page in, thread pool)
     t0 = time.perf_counter()
@@ -170,11 +207,12 @@ def cpu_reference_sample(steps_cap=1, scheme_note="reference"):
         y = step(y)
     secs = time.perf_counter() - t0
     value = prob.graph.nodes * steps_cap / secs
-    return {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"{steps_cap} RK4 step(s) of the full 735471-ADO hierarchy "
-                      f"({'heom_ode.cl + rk_weighted_add.cl compiled for the host' if kind == 'reference' else 'oracle C port'}, "
-                      f"OpenMP over {threads} threads), {secs:.2f} s",
-            "opencl_cpu": opencl_cpu_note()}
+    rec = {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+           "sample": f"{steps_cap} RK4 step(s) of the full 735471-ADO hierarchy "
+                     f"({'heom_ode.cl + rk_weighted_add.cl compiled for the host with -O3 -march=native' if kind == 'reference' else 'oracle C port'}, "
+                     f"OpenMP over {threads} threads), {secs:.2f} s",
+           "opencl_cpu": opencl_cpu_note()}
+    return rec, y, 1 + steps_cap
 
 
 def opencl_cpu_note():
@@ -195,7 +233,7 @@ def run_reference_arm(args, rank):
     # each step is one full-hierarchy RK4 step of the reference kernels on the
     # host; the number of timed steps is capped so the run ends in minutes
     per_step_cap = max(1, min(args.steps, 6))
-    base = cpu_reference_sample(steps_cap=per_step_cap)
+    base, _, _ = cpu_reference_sample(steps_cap=per_step_cap)
     line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT,
             "n_gpus": args.gpus, "steps": per_step_cap, "warmup": 1,
             "ms_per_step": 735471 / base["value"] * 1e3, "higher_is_better": True,
@@ -228,6 +266,21 @@ def run_e2e(H, y0, args, world, dist, nodes, barrier):
             "d2h_bytes_per_step": tops.size * 8 / e2e_steps,
             "note": f"{e2e_steps} steps: full state upload from pinned host memory + top matrix "
                     f"every {OBSERVE_EVERY} steps copied back; final trace {trace:.15f}"}
+
+
+def plain_parity(H, y0, ref_state, ref_steps):
+    """The GPU state after ref_steps RK4 steps from y0 against the reference
+    kernels' state after the same steps (FP64 both)."""
+    n = H.states
+    H.set_state(y0)
+    H.rk4_steps(DT, ref_steps)
+    got = H.get_state()
+    idx = [(n + 1) * 2 * i for i in range(n)]
+    return {"steps": ref_steps,
+            "against": "the reference kernels (heom_ode.cl + rk_weighted_add.cl, FP64) from the same initial state",
+            "max_rel_pop_err": rel_pop_err(got[idx], ref_state[idx]),
+            "max_rel_state_err": float(np.max(np.abs(got - ref_state)) / np.max(np.abs(ref_state))),
+            "pop_floor": POP_FLOOR}
 
 
 # --------------------------------------------------------------------------
@@ -268,62 +321,46 @@ def uneven_systems(count):
     return out
 
 
-def shard(sizes, world, rank):
-    """Instances of this rank: greedy by bytes, largest first."""
-    load = [0] * world
-    mine = []
-    for k in sorted(range(len(sizes)), key=lambda q: -sizes[q]):
-        r = min(range(world), key=lambda q: load[q])
-        load[r] += sizes[k]
-        if r == rank:
-            mine.append(k)
-    return sorted(mine)
+def oracle_populations(system, steps, dt):
+    """Site populations after `steps` RK4 steps from rho0 = |0><0| by the oracle."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import heom_oracle as ho
+    n = system.sites
+    h = (system.h[0::2] + 1j * system.h[1::2]).reshape(n, n)
+    prob = ho.build_problem(ho.make_system(h.real if not np.any(h.imag) else h, [35.0] * n, [50.0] * n,
+                                           [0.0] * n, system.matsubaras, 300.0, system.depth))
+    _, pops = ho.propagate(prob, dt, steps, steps)
+    return pops[-1]
 
 
-def reduce_throughput(dist, ados_steps, secs, device):
-    """Whole-job ADO-updates and the slowest rank's time: one sum and one max
-    all-reduce (the only collectives of a sharded ensemble)."""
-    import torch
-    a = torch.tensor([float(ados_steps)], dtype=torch.float64, device=device)
-    t = torch.tensor([float(secs)], dtype=torch.float64, device=device)
-    if dist is not None:
-        dist.all_reduce(a)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(a.item()), float(t.item())
-
-
-def run_batched(args, world, rank, local_rank):
+def batched_measure(workload, count, steps, warmup, seq_steps, seq_sample, parity_sample, parity_steps,
+                    world=1, rank=0, local_rank=0, dist=None):
+    """Ensemble throughput (one graph launch per RK4 step over all classes),
+    the same instances solved one after another, the e2e path and the
+    populations of a sample of instances against the oracle."""
     import torch
     import heom_b200 as hb
-    torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-
-    count = args.instances or (ENS_COUNT if args.workload == "ensemble" else UNEVEN_COUNT)
-    systems = ensemble_systems(count) if args.workload == "ensemble" else uneven_systems(count)
-    t_setup = time.perf_counter()
-    tables_all = [None] * count
-    sizes = []
     from math import comb
-    for s in systems:
-        P = s.sites * (s.sites - 1) // 2 + (s.sites + 1) // 2
-        sizes.append(comb(s.sites * s.matsubaras + s.depth, s.depth) * P * 32)
-    mine = shard(sizes, world, rank)
-    for k in mine:
-        tables_all[k] = hb.build_tables(systems[k])
-    tables = [tables_all[k] for k in mine]
+    systems = ensemble_systems(count) if workload == "ensemble" else uneven_systems(count)
+    t_setup = time.perf_counter()
+    sizes = [comb(s.sites * s.matsubaras + s.depth, s.depth) * (s.sites * (s.sites - 1) // 2 + (s.sites + 1) // 2) * 32
+             for s in systems]
+    mine = hb.shard_instances(sizes, world, rank)
+    tables = [hb.build_tables(systems[k]) for k in mine]
     footprint = hb.Ensemble.footprint(tables)
     E = hb.Ensemble(tables, device=local_rank)
     nodes = [int(t["matrices"]) for t in tables]
     states = [int(t["states"]) for t in tables]
     total_nodes = sum(nodes)
-    for q, n in enumerate(states):
-        top = np.zeros(n * n * 2)
-        top[0] = 1.0
-        E.set_top(q, top)
+
+    def seed_tops():
+        E.clear()
+        for q, n in enumerate(states):
+            top = np.zeros(n * n * 2)
+            top[0] = 1.0
+            E.set_top(q, top)
+
+    seed_tops()
     stage_us = E.autotune()
     setup_s = time.perf_counter() - t_setup
     stream = torch.cuda.ExternalStream(E.stream(), device=local_rank)
@@ -333,7 +370,7 @@ def run_batched(args, world, rank, local_rank):
             dist.barrier()
         torch.cuda.synchronize()
 
-    E.rk4_steps(ENS_DT, max(args.warmup, 0))
+    E.rk4_steps(ENS_DT, max(warmup, 3))
     start = torch.cuda.Event(enable_timing=True)
     stop = torch.cuda.Event(enable_timing=True)
     clocks = ClockSampler(local_rank)
@@ -341,44 +378,50 @@ def run_batched(args, world, rank, local_rank):
     launches0 = E.kernel_launches()
     clocks.start()
     start.record(stream)
-    E.rk4_steps(ENS_DT, args.steps)
+    E.rk4_steps(ENS_DT, steps)
     stop.record(stream)
     stop.synchronize()
     clk = clocks.stop()
     launches = E.kernel_launches() - launches0
-    ms = start.elapsed_time(stop)
-    secs_local = ms / 1e3
-    job_ados, job_secs = reduce_throughput(dist, total_nodes * args.steps, secs_local, "cuda")
+    secs_local = start.elapsed_time(stop) / 1e3
+    job_ados, job_secs = hb.reduce_throughput(dist, total_nodes * steps, secs_local, "cuda")
     value = job_ados / job_secs
 
     # e2e through the C ABI: initial tops from the host, propagate with every
-    # observation copied back, ensemble mean of the site populations
-    e2e_steps = args.steps - args.steps % OBSERVE_EVERY or OBSERVE_EVERY
+    # observation copied back
+    e2e_steps = steps - steps % OBSERVE_EVERY or OBSERVE_EVERY
     barrier()
     t0 = time.perf_counter()
-    for q, n in enumerate(states):
-        top = np.zeros(n * n * 2)
-        top[0] = 1.0
-        E.set_top(q, top)
+    seed_tops()
     tops = E.propagate(ENS_DT, e2e_steps, OBSERVE_EVERY)
     e2e_secs = time.perf_counter() - t0
-    pops_final = [E.populations(tops[q], q)[-1] for q in range(len(tables))]
-    traces = [float(np.sum(p)) for p in pops_final]
+    traces = [float(np.sum(E.populations(tops[q], q)[-1])) for q in range(len(tables))]
     e2e = {"value": total_nodes * e2e_steps / e2e_secs, "unit": UNIT,
            "h2d_bytes_per_step": sum(n * n * 16 for n in states) / e2e_steps,
            "d2h_bytes_per_step": sum(t.size for t in tops) * 8 / e2e_steps,
-           "note": f"{e2e_steps} steps: every instance's initial top from the host (heom_ensemble_set_top), "
-                   f"heom_ensemble_propagate with all tops copied back every {OBSERVE_EVERY} steps; "
-                   f"trace of every instance within {max(abs(t - 1.0) for t in traces):.1e} of 1"}
+           "note": f"{e2e_steps} steps: every hierarchy cleared and its initial top from the host "
+                   f"(heom_ensemble_clear + heom_ensemble_set_top), heom_ensemble_propagate with all tops "
+                   f"copied back every {OBSERVE_EVERY} steps; trace of every instance within "
+                   f"{max(abs(t - 1.0) for t in traces):.1e} of 1"}
 
-    # sequential plain solves of the same instances (one handle each, graphs),
-    # timed per instance on a sample of steps
-    seq_steps = min(args.steps, args.seq_steps)
-    sample = mine if args.workload == "uneven" else mine[:args.seq_sample]
-    seq_ms = []
+    # populations of a sample of instances against the oracle
+    seed_tops()
+    ptops = E.propagate(ENS_DT, parity_steps, parity_steps)
+    sample = mine[:: max(1, len(mine) // parity_sample)][:parity_sample]
+    perr = 0.0
     for k in sample:
-        with hb.Heom(**tables_all[k], device=local_rank) as H:
-            top = np.zeros(int(tables_all[k]["states"]) ** 2 * 2)
+        q = mine.index(k)
+        perr = max(perr, rel_pop_err(E.populations(ptops[q], q)[-1], oracle_populations(systems[k], parity_steps,
+                                                                                          ENS_DT)))
+    mean_pops = np.mean([E.populations(ptops[q], q)[-1][:3] for q in range(len(mine))
+                         if states[q] == states[0]], axis=0)
+
+    # sequential plain solves of the same instances (one handle each, graphs)
+    seq_sample_k = mine if workload == "uneven" else mine[:seq_sample]
+    seq_ms = []
+    for k in seq_sample_k:
+        with hb.Heom(**tables[mine.index(k)], device=local_rank) as H:
+            top = np.zeros(int(tables[mine.index(k)]["states"]) ** 2 * 2)
             top[0] = 1.0
             H.set_top(top)
             H.rk4_steps(ENS_DT, 3)
@@ -390,38 +433,59 @@ def run_batched(args, world, rank, local_rank):
             b.record(st)
             H.synchronize()
             seq_ms.append(a.elapsed_time(b) / seq_steps)
-    seq_step_ms = (float(np.mean(seq_ms)) * len(mine) if args.workload == "ensemble" else float(np.sum(seq_ms)))
+    seq_step_ms = (float(np.mean(seq_ms)) * len(mine) if workload == "ensemble" else float(np.sum(seq_ms)))
     seq_value = total_nodes / (seq_step_ms / 1e3)
-
-    if args.workload == "ensemble":
-        workload = (f"{count} static-disorder realisations of 7 sites (site energies + N(0,100 cm^-1)), "
-                    f"1 Drude-Lorentz bath/site, no Matsubara term, depth 6 (1716 ADOs each), RK4 dt=1 fs")
-    else:
-        workload = (f"{count} instances, sites U{{4..12}}, depth U{{4..8}}, 0 or 1 Matsubara term, "
-                    f"RK4 dt=1 fs (seed {UNEVEN_SEED})")
     classes = E.classes()
+    E.close()
+    if workload == "ensemble":
+        desc = (f"{count} static-disorder realisations of 7 sites (site energies + N(0,100 cm^-1)), "
+                f"1 Drude-Lorentz bath/site, no Matsubara term, depth 6 (1716 ADOs each), RK4 dt=1 fs")
+    else:
+        desc = (f"{count} instances, sites U{{4..12}}, depth U{{4..8}}, 0 or 1 Matsubara term, "
+                f"RK4 dt=1 fs (seed {UNEVEN_SEED})")
+    return {"workload": desc, "instances": count, "ados": total_nodes * world, "classes": classes,
+            "device_footprint_gb": footprint / 1e9, "steps": steps, "value": value, "unit": UNIT,
+            "ms_per_step": job_secs * 1e3 / steps, "gpu_launches": int(launches), "clocks": clk,
+            "l2": "state larger than L2 (no flush)" if total_nodes * 800 > 126e6 else
+                  "state fits in L2 (no flush; L2-resident by design)",
+            "autotuned_stage_us": stage_us, "setup_s": setup_s,
+            "sequential_value": seq_value,
+            "sequential_note": (f"each instance alone through heom_rk4_steps (graph-captured), "
+                                f"{seq_steps} steps timed per instance on {len(seq_sample_k)} of {len(mine)} "
+                                f"instances{', scaled to all' if len(seq_sample_k) < len(mine) else ''}"),
+            "speedup_vs_sequential": value / seq_value / world,
+            "e2e": e2e,
+            "parity": {"instances_checked": len(sample), "steps": parity_steps,
+                       "against": "the oracle (C restatement of heom_ode.cl, FP64), each instance alone",
+                       "max_rel_pop_err": perr, "pop_floor": POP_FLOOR},
+            "ensemble_mean_populations": [float(v) for v in mean_pops]}
+
+
+def run_batched(args, world, rank, local_rank):
+    import torch
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    count = args.instances or (ENS_COUNT if args.workload == "ensemble" else UNEVEN_COUNT)
+    r = batched_measure(args.workload, count, args.steps, args.warmup, args.seq_steps, args.seq_sample,
+                        args.parity_sample, args.parity_steps, world, rank, local_rank, dist)
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": job_secs * 1e3 / args.steps,
+        line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
                 "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded H, Drude-Lorentz baths)",
-                "config": {"workload": workload, "instances": count, "ados": total_nodes * world,
-                           "classes": classes, "device_footprint_gb": footprint / 1e9,
-                           "l2": "state larger than L2 (no flush)" if total_nodes * 800 > 126e6 else
-                                 "state fits in L2 (no flush; L2-resident by design)",
+                "config": {"workload": r["workload"], "instances": count, "ados": r["ados"],
+                           "classes": r["classes"], "device_footprint_gb": r["device_footprint_gb"],
+                           "l2": r["l2"],
                            "parallelism": f"instances sharded over {world} ranks" if world > 1 else "single"},
-                "e2e": e2e, "gpu_launches": int(launches), "clocks": clk,
-                "batched": {"autotuned_stage_us": stage_us, "setup_s": setup_s,
-                            "sequential_value": seq_value,
-                            "sequential_note": (f"each instance alone through heom_rk4_steps (graph-captured), "
-                                                f"{seq_steps} steps timed per instance on "
-                                                f"{len(sample)} of {len(mine)} instances"
-                                                f"{', scaled to all' if len(sample) < len(mine) else ''}"),
-                            "speedup_vs_sequential": value / seq_value / world,
-                            "ensemble_mean_final_populations": [float(v) for v in np.mean(
-                                [p[:3] for p in pops_final], axis=0)]}}
+                "e2e": r["e2e"], "gpu_launches": r["gpu_launches"], "clocks": r["clocks"],
+                "batched": {k: r[k] for k in ("autotuned_stage_us", "setup_s", "sequential_value",
+                                              "sequential_note", "speedup_vs_sequential", "parity",
+                                              "ensemble_mean_populations")}}
         print(json.dumps(line), flush=True)
-    E.close()
     if dist is not None:
         dist.destroy_process_group()
 
@@ -429,18 +493,14 @@ def run_batched(args, world, rank, local_rank):
 ADJ_SITES, ADJ_DEPTH, ADJ_SEED, ADJ_DT_FS, ADJ_STEPS = 7, 8, 44, 1.0, 2000
 
 
-def run_adjoint(args, rank, local_rank):
+def adjoint_measure(steps, warmup, local_rank):
     """Gradients of the time-integrated site-3 population (trapezoid rule)
     w.r.t. 7 site energies, 21 couplings, lambda and gamma: one adjoint sweep
     against central finite differences (h = 1e-4 cm^-1; gamma relative 1e-5)
-    of the same forward solver, both timed on the device's stream."""
+    of the same forward solver, both timed on the host around blocking calls."""
     import torch
     import heom_b200 as hb
-    if rank != 0:
-        return
-    torch.cuda.set_device(local_rank)
     n = ADJ_SITES
-    steps = args.steps
     h = synthetic_h(n, ADJ_SEED)
     lam, inv = 35.0, 50.0
     system = hb.System(h, [lam] * n, [inv] * n, [0.0] * n, 1, 300.0, ADJ_DEPTH)
@@ -451,8 +511,7 @@ def run_adjoint(args, rank, local_rank):
     w = hb.trapezoid_weights(steps, ADJ_DT_FS)
     dt = ADJ_DT_FS * 1e-15
     A = hb.Adjoint(system, device=local_rank)
-    nodes = 6435
-    for _ in range(max(args.warmup, 1)):  # also sizes the checkpoint buffers outside the timed call
+    for _ in range(max(warmup, 1)):  # also sizes the checkpoint buffers outside the timed call
         A.gradient(rho0, obs, w, dt, steps)
     clocks = ClockSampler(local_rank)
     clocks.start()
@@ -505,37 +564,47 @@ def run_adjoint(args, rank, local_rank):
     ad.append(out["gamma"])
     fd, ad = np.array(fd), np.array(ad)
     rel = np.abs(ad - fd) / np.maximum(np.abs(fd), 1e-3 * np.max(np.abs(fd[:-2])))
-    value = nodes * steps / t_adj
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": steps,
-            "warmup": args.warmup, "ms_per_step": t_adj * 1e3 / steps, "higher_is_better": True,
+    return {"workload": f"adjoint: 7 sites, 1 Drude-Lorentz bath/site, no Matsubara term, depth 8 "
+                        f"(6435 ADOs), RK4 dt=1 fs, {steps} steps, loss = trapezoid integral of the "
+                        f"site-3 population; gradients w.r.t. 7 site energies, 21 couplings, lambda, gamma",
+            "ados": 6435, "steps": steps, "seconds": t_adj, "value": 6435 * steps / t_adj, "unit": UNIT,
+            "value_note": "ADOs x steps / seconds of one heom_adjoint_gradient call "
+                          "(forward sweep + checkpointed backward sweep, host I/O included)",
+            "loss": out["loss"], "gpu_launches": int(launches), "clocks": clk,
+            "fd_seconds": t_fd, "fd_solves": 2 * len(params) + 4, "speedup_vs_fd": t_fd / t_adj,
+            "max_rel_diff_vs_fd": float(np.max(rel)),
+            "fd_note": "central differences carry an O(h^2) truncation error; the FP64 reference "
+                       "gradient check (oracle tangents) is in tests/test_gpu_adjoint.py",
+            "grad_site_energies": ad[:n].tolist(), "grad_lambda": out["lambda"], "grad_gamma": out["gamma"]}
+
+
+def run_adjoint(args, rank, local_rank):
+    import torch
+    if rank != 0:
+        return
+    torch.cuda.set_device(local_rank)
+    r = adjoint_measure(args.steps, args.warmup, local_rank)
+    line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": 1, "steps": r["steps"],
+            "warmup": args.warmup, "ms_per_step": r["seconds"] * 1e3 / r["steps"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded H, Drude-Lorentz baths)",
-            "config": {"workload": f"adjoint: 7 sites, 1 Drude-Lorentz bath/site, no Matsubara term, depth 8 "
-                                   f"(6435 ADOs), RK4 dt=1 fs, {steps} steps, loss = trapezoid integral of the "
-                                   f"site-3 population; gradients w.r.t. 7 site energies, 21 couplings, lambda, gamma",
-                       "ados": nodes, "seed": ADJ_SEED, "parallelism": "single"},
-            "gpu_launches": int(launches), "clocks": clk,
-            "adjoint": {"seconds": t_adj, "loss": out["loss"],
-                        "value_note": "value = ADOs x steps / seconds of one heom_adjoint_gradient call "
-                                      "(forward sweep + checkpointed backward sweep, host I/O included)",
-                        "fd_seconds": t_fd, "fd_solves": 2 * len(params) + 4,
-                        "speedup_vs_fd": t_fd / t_adj,
-                        "max_rel_diff_vs_fd": float(np.max(rel)),
-                        "grad_site_energies": ad[:n].tolist(), "grad_lambda": out["lambda"],
-                        "grad_gamma": out["gamma"]}}
+            "config": {"workload": r["workload"], "ados": r["ados"], "seed": ADJ_SEED, "parallelism": "single"},
+            "gpu_launches": r["gpu_launches"], "clocks": r["clocks"],
+            "adjoint": {k: r[k] for k in ("seconds", "loss", "value_note", "fd_seconds", "fd_solves",
+                                          "speedup_vs_fd", "max_rel_diff_vs_fd", "grad_site_energies",
+                                          "grad_lambda", "grad_gamma")}}
     print(json.dumps(line), flush=True)
 
 
 def run_uneven_adjoint(args, rank, local_rank):
     """Gradients of every instance's time-integrated site-0 population w.r.t.
-    its site energies for the uneven batch: one batch adjoint per group of a
-    class (instances sharing states and baths, packed while the group's
-    sqrt(T) checkpoint layout fits); an instance whose layout alone does not
-    fit runs alone, the library then reversing it by recursive checkpointing
-    in the memory there is.  Compared with central differences of the site
-    energies (two forward solves per site), timed on a sample."""
+    its site energies for the uneven batch, by the library's ensemble adjoint
+    (heom_ensemble_adjoint_*: class grouping, packing within the memory
+    budget and recursive checkpointing of instances that do not fit), against
+    central differences of the site energies on a sample of instances."""
     import torch
     import heom_b200 as hb
+    from math import comb
     if rank != 0:
         return
     torch.cuda.set_device(local_rank)
@@ -543,57 +612,26 @@ def run_uneven_adjoint(args, rank, local_rank):
     systems = uneven_systems(count)
     steps, dt = args.steps, 1e-15
     w = hb.trapezoid_weights(steps, 1.0)
-    classes = {}
-    for k, sysd in enumerate(systems):
-        classes.setdefault((sysd.sites, sysd.matsubaras), []).append(k)
-    free = torch.cuda.mem_get_info()[0]
-    S = max(1, int(np.ceil(np.sqrt(steps))))
-    nstates = (steps + S - 1) // S + 4 * S + 3 + 4  # checkpoints, stage inputs, adjoint, product-form stages
-    min_states = 7 + 4 + 8  # recursive sweep: stage inputs and adjoint, product-form stages, 8 slots
-    covered, skipped, t_adj, nodes_done, grads, recursive = [], [], 0.0, 0, {}, []
-    from math import comb
+    rho0, obs = [], []
+    for s in systems:
+        r = np.zeros((s.sites, s.sites), complex)
+        r[0, 0] = 1.0
+        rho0.append(r)
+        obs.append(r)
+    E = hb.EnsembleAdjoint(systems, device=local_rank)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    out = E.gradient(rho0, obs, w, dt, steps, outputs=("h",))  # site energies: the diagonal of dJ/dH
+    t_adj = time.perf_counter() - t0
+    groups = E.groups()
+    launches = E.kernel_launches()
+    E.close()
+    grads = [np.diag(g.real).copy() for g in out["h"]]
 
     def ados(k):
         return comb(systems[k].sites * systems[k].matsubaras + systems[k].depth, systems[k].depth)
 
-    groups = []
-    for (n, m), members in sorted(classes.items()):
-        P = n * (n - 1) // 2 + (n + 1) // 2
-        group = []
-        for k in sorted(members, key=ados):
-            if nstates * (sum(ados(q) for q in group) + ados(k)) * P * 32 <= 0.85 * free:
-                group.append(k)
-                continue
-            if group:
-                groups.append(group)
-            group = [k]
-        groups.append(group)
-    for members in groups:
-        n = systems[members[0]].sites
-        P = n * (n - 1) // 2 + (n + 1) // 2
-        nodes = sum(ados(k) for k in members)
-        if min_states * nodes * P * 32 > 0.85 * free:
-            skipped += members
-            continue
-        rho0 = np.zeros((n, n), complex)
-        rho0[0, 0] = 1.0
-        obs = np.zeros((n, n), complex)
-        obs[0, 0] = 1.0
-        with hb.Adjoint([systems[k] for k in members], device=local_rank) as A:
-            A.gradient(rho0, obs, hb.trapezoid_weights(2, 1.0), dt, 2, outputs=("h",))  # set-up outside the timing
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            out = A.gradient(rho0, obs, w, dt, steps, outputs=("h",))  # site energies: the diagonal of dJ/dH
-            t_adj += time.perf_counter() - t0
-            if A.recursive_slots():
-                recursive.append({"instances": members, "gb_per_state": nodes * P * 32 / 1e9,
-                                  "slots": A.recursive_slots()})
-        for q, k in enumerate(members):
-            grads[k] = np.diag(out["h"][q].real).copy()
-        covered += members
-        nodes_done += nodes
-    # central differences for a sample of covered instances (two solves per site energy)
-    small = [k for k in covered if ados(k) <= 1_000_000]  # FD solves timed on instances of <= 1 M ADOs
+    small = [k for k in range(count) if ados(k) <= 1_000_000]
     sample = small[:: max(1, len(small) // 6)][:6]
     t_fd_sample, fd_err, fd_sites = 0.0, 0.0, 0
     for k in sample:
@@ -622,32 +660,27 @@ def run_uneven_adjoint(args, rank, local_rank):
             fd = (fp - fm) / 2e-4
             fd_err = max(fd_err, abs(grads[k][a] - fd) / max(abs(fd), 1e-12))
             fd_sites += 1
-    # FD cost of every covered site energy, from the sampled per-solve times per ADO
-    sample_nodes = sum(comb(systems[k].sites * systems[k].matsubaras + systems[k].depth, systems[k].depth)
-                       for k in sample) * 2  # two sites each
+    sample_nodes = sum(ados(k) for k in sample) * 2  # two sites each
     per_node_s = t_fd_sample / max(1, sample_nodes)
-    fd_total = sum(per_node_s * comb(systems[k].sites * systems[k].matsubaras + systems[k].depth, systems[k].depth)
-                   * systems[k].sites for k in covered)
-    line = {"metric": METRIC, "value": nodes_done * steps / max(t_adj, 1e-12), "unit": UNIT, "n_gpus": 1,
-            "steps": steps, "warmup": 1, "ms_per_step": t_adj * 1e3 / steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+    fd_total = sum(per_node_s * ados(k) * systems[k].sites for k in range(count))
+    n_groups = len(set(g for g, _ in groups))
+    line = {"metric": METRIC, "value": sum(ados(k) for k in range(count)) * steps / max(t_adj, 1e-12),
+            "unit": UNIT, "n_gpus": 1, "steps": steps, "warmup": 0, "ms_per_step": t_adj * 1e3 / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded H, Drude-Lorentz baths)",
             "config": {"workload": f"adjoint of the uneven batch ({count} instances, seed {UNEVEN_SEED}): gradient of "
                                    f"each instance's time-integrated site-0 population w.r.t. its site energies, "
-                                   f"{steps} steps of 1 fs, one batch adjoint per group of a class",
-                       "instances_covered": len(covered), "instances_skipped_memory": len(skipped),
-                       "classes": len(classes), "groups": len(groups), "parallelism": "single"},
+                                   f"{steps} steps of 1 fs, heom_ensemble_adjoint_gradient",
+                       "instances": count, "groups": n_groups, "parallelism": "single"},
+            "gpu_launches": int(launches),
             "uneven_adjoint": {"seconds": t_adj, "fd_seconds_estimate": fd_total,
                                "speedup_vs_fd": fd_total / max(t_adj, 1e-12),
-                               "fd_note": f"central differences of {fd_sites} site energies on {len(sample)} covered "
+                               "fd_note": f"central differences of {fd_sites} site energies on {len(sample)} "
                                           f"instances timed ({t_fd_sample:.2f} s) and scaled by ADOs to every "
-                                          f"covered site energy",
+                                          f"site energy of the batch",
                                "max_rel_diff_vs_fd": fd_err,
-                               "skipped": skipped,
-                               "memory_note": f"{nstates} states per group ({(steps + S - 1) // S} checkpoints, "
-                                              f"segments of {S} steps) within 85 % of free memory; larger instances "
-                                              f"alone by recursive checkpointing",
-                               "recursive": recursive}}
+                               "recursive": [{"instance": k, "slots": sl} for k, (g, sl) in enumerate(groups) if sl],
+                               "value_note": "includes the creation of every group's batch adjoint"}}
     print(json.dumps(line), flush=True)
 
 
@@ -660,6 +693,8 @@ def main():
     ap.add_argument("--scheme", default="product", choices=["product", "horner", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="plain workload: skip the batched sub-object")
+    ap.add_argument("--no-adjoint", action="store_true", help="plain workload: skip the adjoint sub-object")
     ap.add_argument("--depth", type=int, default=DEPTH,
                     help="hierarchy depth (8 = the benchmark workload; smaller for profiling captures)")
     ap.add_argument("--sites", type=int, default=N_SITES, help="plain workload: states (8 = the benchmark)")
@@ -667,11 +702,16 @@ def main():
                     help="plain workload: modes per bath (2 = the benchmark's one Matsubara term)")
     ap.add_argument("--workload", default="plain",
                     choices=["plain", "ensemble", "uneven", "adjoint", "uneven-adjoint"],
-                    help="plain: one 735471-ADO hierarchy; ensemble: 256 disorder realisations "
-                         "(7 sites, depth 6); uneven: 64 instances of uneven sizes")
+                    help="plain: one 735471-ADO hierarchy (with the batched and adjoint sub-objects); "
+                         "ensemble: 256 disorder realisations (7 sites, depth 6); uneven: 64 instances of "
+                         "uneven sizes; adjoint, uneven-adjoint: gradients")
     ap.add_argument("--instances", type=int, default=0, help="instance count of a batched workload")
     ap.add_argument("--seq-steps", type=int, default=100, help="steps per instance of the sequential timing")
     ap.add_argument("--seq-sample", type=int, default=16, help="instances timed alone (ensemble workload)")
+    ap.add_argument("--parity-sample", type=int, default=8, help="instances checked against the oracle")
+    ap.add_argument("--parity-steps", type=int, default=200, help="steps of the batched parity check")
+    ap.add_argument("--batched-steps", type=int, default=500, help="timed steps of the batched sub-object")
+    ap.add_argument("--adjoint-steps", type=int, default=ADJ_STEPS, help="steps of the adjoint sub-object")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -753,13 +793,15 @@ def main():
     if per_launch_s:
         alg_bytes = nodes * 32 * ns * ns
         achieved = alg_bytes / per_launch_s / 1e9
-        traffic = profiled_traffic() if benchmark_case else None
+        traffic, traffic_src = profiled_traffic() if benchmark_case else (None, "not the benchmark workload")
         roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                    "frac": achieved / peak, "traffic": traffic,
+                    "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_src,
                     "peak_source": f"{peak_kind} hbm_gbs",
                     "kernel": "heom_dmma_stage" if ns <= 8 else "heom_pair_stage",
+                    "kernel_source_hash": kernel_source_hash(),
                     "alg_bytes_per_launch": alg_bytes, "avg_launch_us": per_launch_s * 1e6}
 
+    line = None
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -771,10 +813,20 @@ def main():
                 "gpu_launches": int(launches), "roofline": roofline, "clocks": clk,
                 "derivative_evals_per_s": 4 * value}
         if world == 1 and not args.no_cpu_baseline and benchmark_case:
-            line["cpu_baseline"] = cpu_reference_sample(steps_cap=3)
-        print(json.dumps(line), flush=True)
-
+            base, ref_state, ref_steps = cpu_reference_sample(steps_cap=3)
+            line["cpu_baseline"] = base
+            line["parity"] = plain_parity(H, y0.numpy(), ref_state, ref_steps)
     H.close()
+
+    if rank == 0 and world == 1:
+        if not args.no_batched:
+            b = batched_measure("ensemble", ENS_COUNT, args.batched_steps, args.warmup, args.seq_steps,
+                                args.seq_sample, args.parity_sample, args.parity_steps, local_rank=local_rank)
+            line["batched"] = b
+        if not args.no_adjoint:
+            line["adjoint"] = adjoint_measure(args.adjoint_steps, 1, local_rank)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
 

@@ -288,6 +288,8 @@ struct heom_handle {
     heom_buffer* flow_above = nullptr;
     heom_buffer* flow_below = nullptr;
     DevBuf<double2> flow_scratch;
+    // buffers created on this handle and not yet destroyed (orphaned by heom_destroy)
+    std::vector<heom_buffer*> live_buffers;
     DevBuf<double> d_zero;                 // zeros, as long as the longest table they replace
 
     // cached graph of one RK4 step
@@ -1239,6 +1241,12 @@ int heom_destroy(heom_handle* h)
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->step_graph) cudaGraphExecDestroy(h->step_graph);
+    // buffers that outlive their handle keep no device memory and no owner;
+    // heom_buffer_destroy then only frees the struct
+    for (heom_buffer* b : h->live_buffers) {
+        b->data.reset();
+        b->owner = nullptr;
+    }
     cudaStream_t s = h->stream;
     delete h;
     if (s) cudaStreamDestroy(s);
@@ -1435,6 +1443,7 @@ int heom_buffer_create(heom_handle* h, heom_buffer** out)
     b->owner = h;
     if (int rc = b->data.alloc(h->state_elems())) return rc;
     CUDA_TRY(cudaMemset(b->data.p, 0, h->state_elems() * sizeof(double2)));
+    h->live_buffers.push_back(b.get());
     *out = b.release();
     return 0;
 }
@@ -1443,9 +1452,13 @@ int heom_buffer_destroy(heom_buffer* b)
 {
     if (!b) return 0;
     if (b->borrowed) return fail(HEOM_E_ARG, "cannot destroy a borrowed buffer view");
-    cudaSetDevice(b->owner->device);
-    if (b->owner->flow_above == b) b->owner->flow_above = nullptr;
-    if (b->owner->flow_below == b) b->owner->flow_below = nullptr;
+    if (heom_handle* h = b->owner) {
+        cudaSetDevice(h->device);
+        if (h->flow_above == b) h->flow_above = nullptr;
+        if (h->flow_below == b) h->flow_below = nullptr;
+        auto& v = h->live_buffers;
+        v.erase(std::remove(v.begin(), v.end(), b), v.end());
+    }
     delete b;
     return 0;
 }
@@ -1712,6 +1725,17 @@ int heom_rk4_steps_noalloc(heom_handle* h, double* d_state, double dt, int64_t s
 {
     if (!h || !d_state || steps < 0 || !(dt > 0.0)) return fail(HEOM_E_ARG, "bad argument");
     if (reinterpret_cast<uintptr_t>(d_state) % 16 != 0) return fail(HEOM_E_ARG, "d_state must be 16-byte aligned");
+    // the static scratch holds the three buffers of the time-independent
+    // product form and nothing else: refuse handle state that step cannot honour
+    if (!h->actions.empty())
+        return fail(HEOM_E_UNSUPPORTED, "host pre-evaluate actions run with heom_solve only; the stepping calls take "
+                                        "a device-side time dependence (heom_set_field)");
+    if (h->field_on)
+        return fail(HEOM_E_UNSUPPORTED, "heom_rk4_steps_noalloc: a time-dependent field needs the classical RK4 "
+                                        "buffers (use heom_rk4_steps)");
+    if (h->flow_above || h->flow_below)
+        return fail(HEOM_E_UNSUPPORTED, "heom_rk4_steps_noalloc: flow tracking needs buffers the static scratch "
+                                        "does not hold (use heom_rk4_steps)");
     const size_t need = h->state_elems() * sizeof(double2);
     if (need > kNoAllocBufferBytes)
         return fail(HEOM_E_UNSUPPORTED,
@@ -2174,6 +2198,18 @@ int heom_ensemble_set_hamiltonian(heom_ensemble* e, int32_t inst, const double* 
     if (int rc = heom_set_instance_hamiltonian(h, idx, ham)) return rc;
     ens_drop_graph(e);
     if (h->hkind != old_kind) e->tuned = false; // another kernel variant: shapes are re-timed
+    return 0;
+}
+
+int heom_ensemble_clear(heom_ensemble* e)
+{
+    if (!e) return fail(HEOM_E_ARG, "NULL argument");
+    CUDA_TRY(cudaSetDevice(e->device));
+    CUDA_TRY(cudaStreamSynchronize(e->stream));
+    for (heom_handle* h : e->cls) {
+        CUDA_TRY(cudaMemsetAsync(h->y.data.p, 0, h->state_elems() * sizeof(double2), h->stream));
+        CUDA_TRY(cudaStreamSynchronize(h->stream));
+    }
     return 0;
 }
 
@@ -2914,5 +2950,219 @@ int heom_adjoint_set_memory_limit(heom_adjoint* A, int64_t bytes)
 }
 
 int64_t heom_adjoint_recursive_slots(const heom_adjoint* A) { return A ? A->rec_slots : -1; }
+
+} // extern "C"
+
+// ---------------------------------------------------------------------------
+// Adjoint gradients of an ensemble of systems of any sizes: the systems are
+// grouped into classes that share states, baths and bath parameters (what a
+// batch adjoint needs); within a class, instances are packed, smallest first,
+// into groups whose sqrt(steps) checkpoint layout fits in the memory budget,
+// and every group is swept by one batch adjoint.  An instance whose layout
+// alone does not fit is swept alone; its adjoint falls back to recursive
+// checkpointing in the memory there is.  Groups run one after another, each
+// adjoint created for its sweep and destroyed after it, so the device holds
+// one group's states at a time.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct ens_system {
+    heom_system_desc d{};
+    std::vector<double> ham, lam, inv, om;
+    std::vector<int32_t> coup;
+    int64_t nodes = 0; // hierarchy ADOs
+    int32_t P = 0;     // sectors per ADO
+};
+
+bool same_adjoint_class(const heom_system_desc& a, const heom_system_desc& b)
+{
+    if (a.sites != b.sites || a.baths != b.baths || a.baths_max_per_site != b.baths_max_per_site ||
+        a.matsubaras != b.matsubaras || a.temperature != b.temperature)
+        return false;
+    auto eq = [](const void* x, const void* y, size_t n) { return std::memcmp(x, y, n) == 0; };
+    return eq(a.baths_coupling, b.baths_coupling, sizeof(int32_t) * a.sites * a.baths_max_per_site) &&
+           eq(a.lambda, b.lambda, sizeof(double) * a.baths) && eq(a.invnu, b.invnu, sizeof(double) * a.baths) &&
+           eq(a.omega, b.omega, sizeof(double) * a.baths);
+}
+
+} // namespace
+
+struct heom_ensemble_adjoint {
+    std::vector<ens_system> sys;
+    heom_options opt{};
+    int64_t mem_limit = 0;
+    std::vector<std::vector<int32_t>> groups; // of the last gradient call
+    std::vector<int64_t> group_slots;         // recursive-checkpointing slots per group (0: sqrt layout)
+    std::vector<int32_t> group_of;            // per instance
+    std::vector<int64_t> mat_off;             // per instance: offset of its states^2 matrix (complex elements)
+    int64_t launches = 0;
+};
+
+extern "C" {
+
+int heom_ensemble_adjoint_create(const heom_system_desc* systems, int32_t count, const heom_options* opt,
+                                 heom_ensemble_adjoint** out)
+{
+    if (!systems || !out || count < 1) return fail(HEOM_E_ARG, "NULL argument or count < 1");
+    *out = nullptr;
+    std::unique_ptr<heom_ensemble_adjoint> e(new heom_ensemble_adjoint());
+    heom_default_options(&e->opt);
+    if (opt) e->opt = *opt;
+    e->sys.resize(count);
+    e->mat_off.resize(count + 1, 0);
+    for (int k = 0; k < count; ++k) {
+        const heom_system_desc& d = systems[k];
+        if (d.sites < 1 || d.sites > kMaxStates || d.baths < 1 || d.baths_max_per_site < 1 || d.matsubaras < 1 ||
+            d.ado_depth < 0 || !d.hamiltonian || !d.baths_coupling || !d.lambda || !d.invnu || !d.omega)
+            return fail(HEOM_E_ARG, "system %d: bad descriptor", k);
+        ens_system& x = e->sys[k];
+        x.ham.assign(d.hamiltonian, d.hamiltonian + 2 * d.sites * d.sites);
+        x.lam.assign(d.lambda, d.lambda + d.baths);
+        x.inv.assign(d.invnu, d.invnu + d.baths);
+        x.om.assign(d.omega, d.omega + d.baths);
+        x.coup.assign(d.baths_coupling, d.baths_coupling + d.sites * d.baths_max_per_site);
+        x.d = d;
+        x.d.hamiltonian = x.ham.data();
+        x.d.lambda = x.lam.data();
+        x.d.invnu = x.inv.data();
+        x.d.omega = x.om.data();
+        x.d.baths_coupling = x.coup.data();
+        // ADOs = C(W + D, D), W = baths x matsubaras
+        const int64_t W = (int64_t)d.baths * d.matsubaras;
+        long double c = 1.0L;
+        for (int64_t i = 1; i <= d.ado_depth; ++i) c = c * (long double)(W + i) / (long double)i;
+        x.nodes = (int64_t)std::llround((double)c);
+        x.P = heomk::pairs_of(d.sites);
+        e->mat_off[k + 1] = e->mat_off[k] + (int64_t)d.sites * d.sites;
+    }
+    *out = e.release();
+    return 0;
+}
+
+int heom_ensemble_adjoint_destroy(heom_ensemble_adjoint* e)
+{
+    delete e;
+    return 0;
+}
+
+int heom_ensemble_adjoint_set_memory_limit(heom_ensemble_adjoint* e, int64_t bytes)
+{
+    if (!e || bytes < 0) return fail(HEOM_E_ARG, "bad argument");
+    e->mem_limit = bytes;
+    return 0;
+}
+
+int heom_ensemble_adjoint_gradient(heom_ensemble_adjoint* e, const double* rho0, const double* observable,
+                                   const double* weights, double dt, int64_t steps, double* loss, double* grad_h,
+                                   double* grad_lambda, double* grad_gamma, double* grad_rho0)
+{
+    if (!e || !rho0 || !observable || !weights || steps < 1 || !(dt > 0.0)) return fail(HEOM_E_ARG, "bad argument");
+    CUDA_TRY(cudaSetDevice(e->opt.device));
+    const int count = (int)e->sys.size();
+    // memory budget of one group's states: the limit, or 85 % of the free memory
+    int64_t budget = e->mem_limit;
+    if (budget <= 0) {
+        size_t free_b = 0, total_b = 0;
+        CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+        budget = (int64_t)(0.85 * (double)free_b);
+    }
+    const int64_t S = std::max<int64_t>(1, (int64_t)std::ceil(std::sqrt((double)steps)));
+    const int64_t ncp = (steps + S - 1) / S;
+    // sqrt layout of a batch adjoint: checkpoints, the stage inputs of one
+    // segment, the adjoint ping-pong and a scratch state, plus the forward
+    // handle's state and its two product-form stage buffers
+    const int64_t states_needed = ncp + 4 * S + 3 + 3;
+    auto bytes_of = [&](int k) { return e->sys[k].nodes * (int64_t)e->sys[k].P * 32; };
+    // classes (first fit on the descriptor), then groups per class
+    std::vector<std::vector<int32_t>> classes;
+    for (int k = 0; k < count; ++k) {
+        bool placed = false;
+        for (auto& c : classes)
+            if (same_adjoint_class(e->sys[c[0]].d, e->sys[k].d)) {
+                c.push_back(k);
+                placed = true;
+                break;
+            }
+        if (!placed) classes.push_back({k});
+    }
+    e->groups.clear();
+    for (auto& c : classes) {
+        std::vector<int32_t> m = c;
+        std::stable_sort(m.begin(), m.end(), [&](int a, int b) { return e->sys[a].nodes < e->sys[b].nodes; });
+        std::vector<int32_t> g;
+        int64_t held = 0;
+        for (int k : m) {
+            if (!g.empty() && states_needed * (held + bytes_of(k)) > budget) {
+                e->groups.push_back(g);
+                g.clear();
+                held = 0;
+            }
+            g.push_back(k);
+            held += bytes_of(k);
+        }
+        if (!g.empty()) e->groups.push_back(g);
+    }
+    e->group_of.assign(count, -1);
+    e->group_slots.assign(e->groups.size(), 0);
+    for (size_t gi = 0; gi < e->groups.size(); ++gi) {
+        const std::vector<int32_t>& g = e->groups[gi];
+        const int K = (int)g.size();
+        const int N = e->sys[g[0]].d.sites, NN = N * N;
+        std::vector<heom_system_desc> d(K);
+        for (int q = 0; q < K; ++q) d[q] = e->sys[g[q]].d;
+        heom_adjoint* A = nullptr;
+        if (int rc = heom_adjoint_create_batch(d.data(), K, &e->opt, &A)) return rc;
+        std::unique_ptr<heom_adjoint, int (*)(heom_adjoint*)> hold(A, heom_adjoint_destroy);
+        if (e->mem_limit > 0) heom_adjoint_set_memory_limit(A, e->mem_limit);
+        // gather the group's per-instance arrays
+        std::vector<double> r0(2 * (size_t)K * NN), ob(2 * (size_t)K * NN), gl(K), gg(K), ls(K);
+        std::vector<double> gh(grad_h ? 2 * (size_t)K * NN : 0), gr(grad_rho0 ? 2 * (size_t)K * NN : 0);
+        for (int q = 0; q < K; ++q) {
+            const size_t src = 2 * (size_t)e->mat_off[g[q]];
+            std::copy(rho0 + src, rho0 + src + 2 * NN, r0.begin() + 2 * (size_t)q * NN);
+            std::copy(observable + src, observable + src + 2 * NN, ob.begin() + 2 * (size_t)q * NN);
+        }
+        const int64_t before = heom_adjoint_kernel_launches(A);
+        if (int rc = heom_adjoint_gradient(A, r0.data(), ob.data(), weights, dt, steps, ls.data(),
+                                           grad_h ? gh.data() : nullptr, grad_lambda ? gl.data() : nullptr,
+                                           grad_gamma ? gg.data() : nullptr, grad_rho0 ? gr.data() : nullptr))
+            return rc;
+        e->launches += heom_adjoint_kernel_launches(A) - before;
+        e->group_slots[gi] = heom_adjoint_recursive_slots(A);
+        for (int q = 0; q < K; ++q) {
+            const int k = g[q];
+            const size_t dst = 2 * (size_t)e->mat_off[k];
+            e->group_of[k] = (int32_t)gi;
+            if (loss) loss[k] = ls[q];
+            if (grad_lambda) grad_lambda[k] = gl[q];
+            if (grad_gamma) grad_gamma[k] = gg[q];
+            if (grad_h) std::copy(gh.begin() + 2 * (size_t)q * NN, gh.begin() + 2 * (size_t)(q + 1) * NN, grad_h + dst);
+            if (grad_rho0)
+                std::copy(gr.begin() + 2 * (size_t)q * NN, gr.begin() + 2 * (size_t)(q + 1) * NN, grad_rho0 + dst);
+        }
+    }
+    return 0;
+}
+
+int32_t heom_ensemble_adjoint_groups(const heom_ensemble_adjoint* e) { return e ? (int32_t)e->groups.size() : 0; }
+
+int heom_ensemble_adjoint_group_of(const heom_ensemble_adjoint* e, int32_t inst, int32_t* group,
+                                   int64_t* recursive_slots)
+{
+    if (!e || inst < 0 || inst >= (int32_t)e->sys.size()) return fail(HEOM_E_ARG, "bad argument");
+    if (e->group_of.empty()) return fail(HEOM_E_ARG, "no gradient has been computed yet");
+    const int32_t g = e->group_of[inst];
+    if (group) *group = g;
+    if (recursive_slots) *recursive_slots = g >= 0 ? e->group_slots[g] : 0;
+    return 0;
+}
+
+int64_t heom_ensemble_adjoint_offset(const heom_ensemble_adjoint* e, int32_t inst)
+{
+    if (!e || inst < 0 || inst > (int32_t)e->sys.size()) return -1;
+    return e->mat_off[inst];
+}
+
+int64_t heom_ensemble_adjoint_kernel_launches(const heom_ensemble_adjoint* e) { return e ? e->launches : 0; }
 
 } // extern "C"

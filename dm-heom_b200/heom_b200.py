@@ -43,7 +43,7 @@ EXPORTS = [
     "heom_ensemble_class", "heom_ensemble_set_hamiltonian", "heom_ensemble_set_top",
     "heom_ensemble_get_top", "heom_ensemble_autotune", "heom_ensemble_rk4_steps",
     "heom_ensemble_propagate", "heom_ensemble_top_row_len", "heom_ensemble_top_offset",
-    "heom_ensemble_kernel_launches", "heom_ensemble_stream",
+    "heom_ensemble_kernel_launches", "heom_ensemble_stream", "heom_ensemble_clear",
     "heom_adjoint_create", "heom_adjoint_destroy", "heom_adjoint_handle", "heom_adjoint_gradient",
     "heom_adjoint_kernel_launches", "heom_bath_derivatives", "heom_adjoint_create_batch",
     "heom_adjoint_instances", "heom_set_mask_compact", "heom_active_matrices", "heom_get_mask",
@@ -52,6 +52,9 @@ EXPORTS = [
     "heom_hierarchy_add", "heom_hierarchy_subtract", "heom_hierarchy_dot_product", "heom_hierarchy_scale",
     "heom_hierarchy_mmult_left", "heom_hierarchy_mmult_right", "heom_instance_write", "heom_instance_read",
     "heom_tables_state", "heom_adjoint_set_memory_limit", "heom_adjoint_recursive_slots",
+    "heom_ensemble_adjoint_create", "heom_ensemble_adjoint_destroy", "heom_ensemble_adjoint_set_memory_limit",
+    "heom_ensemble_adjoint_gradient", "heom_ensemble_adjoint_groups", "heom_ensemble_adjoint_group_of",
+    "heom_ensemble_adjoint_offset", "heom_ensemble_adjoint_kernel_launches",
 ]
 
 PRE_EVALUATE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_void_p)
@@ -191,6 +194,7 @@ def lib():
         L.heom_ensemble_kernel_launches.argtypes = [vp]
         L.heom_ensemble_stream.restype = vp
         L.heom_ensemble_stream.argtypes = [vp]
+        L.heom_ensemble_clear.argtypes = [vp]
         L.heom_adjoint_create.argtypes = [C.POINTER(SystemDesc), C.POINTER(Options), C.POINTER(vp)]
         L.heom_adjoint_destroy.argtypes = [vp]
         L.heom_adjoint_handle.restype = vp
@@ -205,6 +209,17 @@ def lib():
         L.heom_adjoint_set_memory_limit.argtypes = [vp, i64]
         L.heom_adjoint_recursive_slots.restype = i64
         L.heom_adjoint_recursive_slots.argtypes = [vp]
+        L.heom_ensemble_adjoint_create.argtypes = [C.POINTER(SystemDesc), i32, C.POINTER(Options), C.POINTER(vp)]
+        L.heom_ensemble_adjoint_destroy.argtypes = [vp]
+        L.heom_ensemble_adjoint_set_memory_limit.argtypes = [vp, i64]
+        L.heom_ensemble_adjoint_gradient.argtypes = [vp, vp, vp, vp, dbl, i64, vp, vp, vp, vp, vp]
+        L.heom_ensemble_adjoint_groups.restype = i32
+        L.heom_ensemble_adjoint_groups.argtypes = [vp]
+        L.heom_ensemble_adjoint_group_of.argtypes = [vp, i32, vp, vp]
+        L.heom_ensemble_adjoint_offset.restype = i64
+        L.heom_ensemble_adjoint_offset.argtypes = [vp, i32]
+        L.heom_ensemble_adjoint_kernel_launches.restype = i64
+        L.heom_ensemble_adjoint_kernel_launches.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -547,6 +562,10 @@ class Ensemble:
         _check(lib().heom_ensemble_locate(self.h, k, C.byref(c), C.byref(i)))
         return c.value, i.value
 
+    def clear(self):
+        """Zero every instance's hierarchy state (set the tops afterwards)."""
+        _check(lib().heom_ensemble_clear(self.h))
+
     def set_top(self, k, top):
         top = np.ascontiguousarray(top, dtype=np.float64)
         assert top.size == self.states[k] ** 2 * 2
@@ -736,6 +755,115 @@ class Adjoint:
 
     def __exit__(self, *a):
         self.close()
+
+
+class EnsembleAdjoint:
+    """Adjoint gradients for systems of any sizes (heom_ensemble_adjoint_*):
+    the library groups them into batch adjoints by class and memory and
+    sweeps the groups one after another.  rho0 / observable: one (n, n)
+    matrix for all instances or a list of per-instance matrices; results are
+    per-instance lists (matrices) and arrays (loss, lambda, gamma)."""
+
+    def __init__(self, systems, device=0, graphs=True):
+        self.systems = list(systems)
+        ds = (SystemDesc * len(self.systems))(*[x.desc() for x in self.systems])
+        o = make_options(device, "lex", "product", graphs)
+        self.h = C.c_void_p()
+        _check(lib().heom_ensemble_adjoint_create(ds, len(self.systems), C.byref(o), C.byref(self.h)))
+        self.instances = len(self.systems)
+        self.offsets = [lib().heom_ensemble_adjoint_offset(self.h, k) for k in range(self.instances + 1)]
+
+    def set_memory_limit(self, nbytes):
+        _check(lib().heom_ensemble_adjoint_set_memory_limit(self.h, int(nbytes)))
+
+    def _pack(self, mats):
+        out = np.zeros(2 * self.offsets[-1])
+        for k, sysd in enumerate(self.systems):
+            n = sysd.sites
+            m = mats[k] if isinstance(mats, (list, tuple)) else mats
+            m = np.asarray(m, np.complex128).reshape(n, n)
+            out[2 * self.offsets[k]:2 * self.offsets[k + 1]] = m.reshape(-1).view(np.float64)
+        return out
+
+    def _unpack(self, flat):
+        res = []
+        for k, sysd in enumerate(self.systems):
+            n = sysd.sites
+            res.append(flat[2 * self.offsets[k]:2 * self.offsets[k + 1]].view(np.complex128).reshape(n, n).copy())
+        return res
+
+    def gradient(self, rho0, observable, weights, dt, steps, outputs=("h", "lambda", "gamma", "rho0")):
+        K = self.instances
+        r0, ob = self._pack(rho0), self._pack(observable)
+        w = np.ascontiguousarray(np.asarray(weights, np.float64))
+        assert w.size == steps + 1
+        loss, gl, gg = np.zeros(K), np.zeros(K), np.zeros(K)
+        gh, gr = np.zeros(2 * self.offsets[-1]), np.zeros(2 * self.offsets[-1])
+
+        def opt(name, a):
+            return _ptr(a) if name in outputs else None
+        _check(lib().heom_ensemble_adjoint_gradient(self.h, _ptr(r0), _ptr(ob), _ptr(w), dt, steps, _ptr(loss),
+                                                    opt("h", gh), opt("lambda", gl), opt("gamma", gg),
+                                                    opt("rho0", gr)))
+        return {"loss": loss,
+                "h": self._unpack(gh) if "h" in outputs else None,
+                "lambda": gl if "lambda" in outputs else None,
+                "gamma": gg if "gamma" in outputs else None,
+                "rho0": self._unpack(gr) if "rho0" in outputs else None}
+
+    def groups(self):
+        """(group, recursive-checkpointing slots) of every instance in the last call."""
+        out = []
+        for k in range(self.instances):
+            g, sl = C.c_int32(), C.c_int64()
+            _check(lib().heom_ensemble_adjoint_group_of(self.h, k, C.byref(g), C.byref(sl)))
+            out.append((g.value, sl.value))
+        return out
+
+    def kernel_launches(self):
+        return lib().heom_ensemble_adjoint_kernel_launches(self.h)
+
+    def close(self):
+        if self.h:
+            lib().heom_ensemble_adjoint_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def shard_instances(sizes, world, rank):
+    """Instances of rank `rank` when independent instances are spread over
+    `world` GPUs: greedy by bytes, largest first (no data exchange)."""
+    load = [0] * world
+    mine = []
+    for k in sorted(range(len(sizes)), key=lambda q: -sizes[q]):
+        r = min(range(world), key=lambda q: load[q])
+        load[r] += sizes[k]
+        if r == rank:
+            mine.append(k)
+    return sorted(mine)
+
+
+def reduce_throughput(dist, ados_steps, secs, device):
+    """Whole-job ADO-updates and the slowest rank's time of a sharded run: one
+    sum and one max all-reduce (the only collectives of a sharded ensemble)."""
+    import torch
+    a = torch.tensor([float(ados_steps)], dtype=torch.float64, device=device)
+    t = torch.tensor([float(secs)], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(a)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(a.item()), float(t.item())
 
 
 def trapezoid_weights(steps, dt_fs):

@@ -203,6 +203,9 @@ int heom_get_mask(const heom_handle* h, uint8_t* mask);
 int heom_hierarchy_norm(heom_handle* h, double threshold, double* norms);
 
 int heom_buffer_create(heom_handle* h, heom_buffer** out);
+/* Buffers may outlive their handle: heom_destroy frees their device memory
+ * and detaches them (every later call but heom_buffer_destroy then fails with
+ * HEOM_E_ARG); heom_buffer_destroy frees what is left. */
 int heom_buffer_destroy(heom_buffer* b);
 int heom_buffer_write(heom_handle* h, heom_buffer* b, const double* host_state);
 int heom_buffer_read(heom_handle* h, const heom_buffer* b, double* host_state);
@@ -257,7 +260,12 @@ int heom_synchronize(heom_handle* h);
  *            complex doubles in the reference layout (uid order, row-major,
  *            interleaved re/im); read and overwritten with the result.
  * The handle's tables are used (create the handle beforehand); the stages use
- * the product-form RK4 whatever the handle's scheme.  Scratch comes from a
+ * the product-form RK4 whatever the handle's scheme.  Handles with a
+ * time-dependent field (heom_set_field), flow buffers or host pre-evaluate
+ * actions are refused with HEOM_E_UNSUPPORTED: that work needs buffers the
+ * static scratch does not hold.  The call runs on the handle's own stream,
+ * which does not wait for other streams: finish every write to d_state (for
+ * example, synchronise the stream that wrote it) before the call.  Scratch comes from a
  * static device array of 3 x 16 MiB built into the library and held on every
  * GPU that loads it until exit; hierarchies whose state needs more than
  * 16 MiB in the library's layout are rejected with HEOM_E_UNSUPPORTED.  The
@@ -329,6 +337,8 @@ int heom_ensemble_locate(const heom_ensemble* e, int32_t inst, int32_t* cls, int
 /* borrowed batch handle of a class (valid until heom_ensemble_destroy) */
 heom_handle* heom_ensemble_class(heom_ensemble* e, int32_t cls);
 int heom_ensemble_set_hamiltonian(heom_ensemble* e, int32_t inst, const double* hamiltonian);
+/* Zero the whole hierarchy state of every instance (then set the tops). */
+int heom_ensemble_clear(heom_ensemble* e);
 int heom_ensemble_set_top(heom_ensemble* e, int32_t inst, const double* host_top);
 int heom_ensemble_get_top(heom_ensemble* e, int32_t inst, double* host_top);
 /* Time the candidate stage-kernel grids (on the stage buffers, not on the
@@ -456,6 +466,35 @@ int64_t heom_adjoint_kernel_launches(const heom_adjoint* a);
  * recursive checkpointing, 0 when it used the sqrt(steps) layout. */
 int heom_adjoint_set_memory_limit(heom_adjoint* a, int64_t bytes);
 int64_t heom_adjoint_recursive_slots(const heom_adjoint* a);
+
+/* Adjoint gradients for an ensemble of systems of any sizes (an uneven
+ * batch).  No counterpart in the reference.  heom_ensemble_adjoint_gradient
+ * groups the systems into classes that share states, baths and bath
+ * parameters; within a class it packs instances, smallest first, into groups
+ * whose sqrt(steps) checkpoint layout fits in the memory budget (the limit
+ * set below, else 85 % of the free device memory) and sweeps every group as
+ * one batch adjoint, one group after another.  An instance whose layout alone
+ * does not fit is swept alone with recursive checkpointing.  Per-instance
+ * arrays hold the instances back to back in instance order: rho0,
+ * observable, grad_h, grad_rho0 states_k^2 complex each (instance k starts at
+ * complex element heom_ensemble_adjoint_offset(e, k)); loss, grad_lambda,
+ * grad_gamma one value each.  weights, dt and steps are common; NULL outputs
+ * are skipped as in heom_adjoint_gradient. */
+typedef struct heom_ensemble_adjoint heom_ensemble_adjoint;
+int heom_ensemble_adjoint_create(const heom_system_desc* systems, int32_t count, const heom_options* opt,
+                                 heom_ensemble_adjoint** out);
+int heom_ensemble_adjoint_destroy(heom_ensemble_adjoint* e);
+int heom_ensemble_adjoint_set_memory_limit(heom_ensemble_adjoint* e, int64_t bytes);
+int heom_ensemble_adjoint_gradient(heom_ensemble_adjoint* e, const double* rho0, const double* observable,
+                                   const double* weights, double dt, int64_t steps, double* loss, double* grad_h,
+                                   double* grad_lambda, double* grad_gamma, double* grad_rho0);
+/* groups of the last gradient call; the group of an instance and its
+ * recursive-checkpointing slots (0: the sqrt(steps) layout) */
+int32_t heom_ensemble_adjoint_groups(const heom_ensemble_adjoint* e);
+int heom_ensemble_adjoint_group_of(const heom_ensemble_adjoint* e, int32_t inst, int32_t* group,
+                                   int64_t* recursive_slots);
+int64_t heom_ensemble_adjoint_offset(const heom_ensemble_adjoint* e, int32_t inst);
+int64_t heom_ensemble_adjoint_kernel_launches(const heom_ensemble_adjoint* e);
 /* Derivatives of the bath tables (pf_same [baths*2], pf_circ [baths*2],
  * cbk [baths*matsubaras*2], SI units) with respect to theta = 0: lambda of
  * every bath together (per J), theta = 1: gamma = 1/invnu of every bath

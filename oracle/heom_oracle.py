@@ -58,7 +58,7 @@ class _Problem(C.Structure):
 
 
 _lib = None
-_ref = None
+_ref = {}
 
 
 def lib():
@@ -89,13 +89,29 @@ def lib():
     return _lib
 
 
-def ref_lib():
-    """The reference's own kernels compiled for the host, or None."""
-    global _ref
-    if _ref is None:
-        path = os.path.join(HERE, "_ref", "libheom_refcl.so")
+def _cpu_has_x86_64_v3():
+    try:
+        flags = set()
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    flags = set(line.split(":", 1)[1].split())
+                    break
+        return {"avx2", "fma", "bmi2", "movbe"} <= flags
+    except OSError:
+        return False
+
+
+def ref_lib(fast=False):
+    """The reference's own kernels compiled for the host, or None.  fast=True:
+    the build for timing (-O3, x86-64-v3, contraction allowed) when this CPU
+    runs it, else the parity build (-O2, no contraction)."""
+    key = "fast" if fast and _cpu_has_x86_64_v3() else "parity"
+    if key not in _ref:
+        name = "libheom_refcl_fast.so" if key == "fast" else "libheom_refcl.so"
+        path = os.path.join(HERE, "_ref", name)
         if not os.path.exists(path):
-            return None
+            return None if key == "parity" else ref_lib(False)
         R = C.CDLL(path)
         R.refcl_heom_ode.restype = C.c_int
         R.refcl_heom_ode.argtypes = [
@@ -105,8 +121,8 @@ def ref_lib():
         R.refcl_rk_weighted_add.restype = C.c_int
         R.refcl_rk_weighted_add.argtypes = [C.c_int, C.c_int64, C.c_int, C.c_double, _f64p, _f64p,
                                             _f64p, C.POINTER(C.c_void_p), C.c_int]
-        _ref = R
-    return _ref
+        _ref[key] = R
+    return _ref[key]
 
 
 def ref_ip_lib():
@@ -341,12 +357,12 @@ def propagate(prob: Problem, h: float, steps: int, observe_every: int, y=None, t
 
 
 def ref_derivative(prob: Problem, y: np.ndarray, threads=None, mode=0, out_coeff=1.0,
-                   acc=None, acc_coeff=1.0, acc_init=False):
+                   acc=None, acc_coeff=1.0, acc_init=False, fast=False):
     """One call of the reference's own heom_ode kernel (compiled for the host).
 
     mode 0 = pure evaluation, 1 = NOMA_NUM_ODE_ACCUMULATE, 2 = NOMA_NUM_ODE_SUBDIAGONAL.
     Returns (out, acc)."""
-    R = ref_lib()
+    R = ref_lib(fast)
     if R is None:
         raise RuntimeError("reference kernels not built (oracle/_ref)")
     s = prob.system
@@ -366,8 +382,8 @@ def ref_derivative(prob: Problem, y: np.ndarray, threads=None, mode=0, out_coeff
     return out, accb
 
 
-def ref_weighted_add(prob: Problem, h, y, coeffs, ks, threads=None):
-    R = ref_lib()
+def ref_weighted_add(prob: Problem, h, y, coeffs, ks, threads=None, fast=False):
+    R = ref_lib(fast)
     out = np.zeros_like(y)
     c = np.ascontiguousarray(np.asarray(coeffs, np.float64))
     kp = (C.c_void_p * len(ks))(*[k.ctypes.data for k in ks])
@@ -376,17 +392,19 @@ def ref_weighted_add(prob: Problem, h, y, coeffs, ks, threads=None):
     return out
 
 
-def ref_rk4_step(prob: Problem, h, y, threads=None):
+def ref_rk4_step(prob: Problem, h, y, threads=None, fast=False):
     """Classical RK4 step built from the reference's own kernels: pure heom_ode
-    evaluations and rk_weighted_add for the stage inputs and the result."""
-    k1, _ = ref_derivative(prob, y, threads)
-    s = ref_weighted_add(prob, h, y, [0.5], [k1], threads)
-    k2, _ = ref_derivative(prob, s, threads)
-    s = ref_weighted_add(prob, h, y, [0.0, 0.5], [k1, k2], threads)
-    k3, _ = ref_derivative(prob, s, threads)
-    s = ref_weighted_add(prob, h, y, [0.0, 0.0, 1.0], [k1, k2, k3], threads)
-    k4, _ = ref_derivative(prob, s, threads)
-    return ref_weighted_add(prob, h, y, [1.0 / 6, 1.0 / 3, 1.0 / 3, 1.0 / 6], [k1, k2, k3, k4], threads)
+    evaluations and rk_weighted_add for the stage inputs and the result
+    (fast=True: the timing build of the same sources)."""
+    k1, _ = ref_derivative(prob, y, threads, fast=fast)
+    s = ref_weighted_add(prob, h, y, [0.5], [k1], threads, fast=fast)
+    k2, _ = ref_derivative(prob, s, threads, fast=fast)
+    s = ref_weighted_add(prob, h, y, [0.0, 0.5], [k1, k2], threads, fast=fast)
+    k3, _ = ref_derivative(prob, s, threads, fast=fast)
+    s = ref_weighted_add(prob, h, y, [0.0, 0.0, 1.0], [k1, k2, k3], threads, fast=fast)
+    k4, _ = ref_derivative(prob, s, threads, fast=fast)
+    return ref_weighted_add(prob, h, y, [1.0 / 6, 1.0 / 3, 1.0 / 3, 1.0 / 6], [k1, k2, k3, k4], threads,
+                            fast=fast)
 
 
 def populations(prob: Problem, y: np.ndarray) -> np.ndarray:

@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 
 import heom_b200 as hb
+from parity import assert_pops
 import heom_oracle as ho
 from test_host import FMO_CFG, LA_CFG
 
@@ -37,7 +38,7 @@ def test_app_observers_match_oracle(tmp_path):
     _, ref = ho.propagate(prob, 1e-15, 20, 5)
     hd, d = read_dat(tmp_path / "d.dat")
     assert hd == ["time", "site_0", "site_1", "site_2"]
-    assert np.max(np.abs(d[:, 1:] - ref)) <= 1e-10
+    assert_pops(d[:, 1:], ref)
     assert np.allclose(d[:, 0], np.arange(5) * 5e-15, rtol=1e-15, atol=0)
     _, t = read_dat(tmp_path / "t.dat")
     assert np.max(np.abs(t[:, 1] - 1.0)) <= 1e-12

@@ -9,11 +9,11 @@ import numpy as np
 import pytest
 
 import heom_b200 as hb
+from parity import assert_pops
 import heom_oracle as ho
 
 pytestmark = pytest.mark.gpu
 
-POP_TOL = 1e-10
 DT = 1e-15
 
 
@@ -69,7 +69,7 @@ def test_batch_populations_match_oracle():
         pops = H.populations_from_tops(H.propagate(DT, 200, 20))
     for k, p in enumerate(probs):
         _, ref = ho.propagate(p, DT, 200, 20)
-        assert np.max(np.abs(pops[:, k, :] - ref)) <= POP_TOL
+        assert_pops(pops[:, k, :], ref)
 
 
 def test_batch_state_and_top_round_trip():
@@ -122,7 +122,7 @@ def test_ensemble_uneven_sizes_bitwise_and_oracle():
         assert np.array_equal(tops[k], alone(p, 60, 20)), f"instance {k}"
         _, ref = ho.propagate(p, DT, 60, 20)
         pops = tops[k][:, [(p.states + 1) * 2 * i for i in range(p.states)]]
-        assert np.max(np.abs(pops - ref)) <= POP_TOL
+        assert_pops(pops, ref)
 
 
 def test_ensemble_rejects_footprint_beyond_device_memory():

@@ -2,7 +2,7 @@
 
 Ensembles shard by instance with no exchange in the data path; the only
 collectives are one sum and one max all-reduce of the throughput
-(bench.reduce_throughput) and, for observables, a sum of per-rank population
+(heom_b200.reduce_throughput) and, for observables, a sum of per-rank population
 traces.  Here each rank propagates its shard of a small ensemble with the
 oracle on the CPU and the reduced results must equal a single-process run."""
 import os
@@ -11,7 +11,7 @@ import socket
 import numpy as np
 import pytest
 
-import bench
+import heom_b200 as hb
 import heom_oracle as ho
 
 
@@ -45,11 +45,11 @@ def worker(rank, world, port, out):
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
     sizes = [ho.build_graph(n * m, d).nodes * n * n for n, d, m, _ in SYSTEMS]
-    mine = bench.shard(sizes, world, rank)
+    mine = hb.shard_instances(sizes, world, rank)
     pop_sum, ados = ensemble_pops(mine)
     t = torch.tensor([pop_sum], dtype=torch.float64)
     dist.all_reduce(t)
-    job_ados, job_secs = bench.reduce_throughput(dist, ados, 1.0 + rank, "cpu")
+    job_ados, job_secs = hb.reduce_throughput(dist, ados, 1.0 + rank, "cpu")
     gathered = [None] * world
     dist.all_gather_object(gathered, mine)
     if rank == 0:
@@ -61,7 +61,7 @@ def worker(rank, world, port, out):
 def test_shard_covers_every_instance_once_and_balances():
     sizes = [int(x) for x in np.random.default_rng(3).integers(1, 1000, size=64)]
     for world in (1, 2, 3, 8):
-        parts = [bench.shard(sizes, world, r) for r in range(world)]
+        parts = [hb.shard_instances(sizes, world, r) for r in range(world)]
         flat = sorted(k for p in parts for k in p)
         assert flat == list(range(64))
         loads = [sum(sizes[k] for k in p) for p in parts]

@@ -13,7 +13,7 @@ import pytest
 
 import heom_oracle as ho
 
-REF = "/root/reference"
+REF = os.environ.get("HEOM_REFERENCE_ROOT", "/root/reference")
 
 
 def test_graph_invariants():
