@@ -632,6 +632,35 @@ int launch_wadd(heom_handle* h, int n, double step, double2* out, const double2*
     return 0;
 }
 
+// heom_ode.cl:436-441: flow_from_above += acc_coeff * plus term, flow_from_below
+// += acc_coeff * minus term of the evaluation of `in`; each term alone is L
+// with H, the same term and the other term's coefficients zeroed (no launch
+// when no flow buffer is set)
+int launch_flows(heom_handle* h, const double2* in, double acc_coeff)
+{
+    if (!h->flow_above && !h->flow_below) return 0;
+    const double2* z2 = reinterpret_cast<const double2*>(h->d_zero.p);
+    const double* z1 = h->d_zero.p;
+    for (int part = 0; part < 2; ++part) {
+        heom_buffer* dst = part == 0 ? h->flow_above : h->flow_below;
+        if (!dst) continue;
+        AdjTabs t;
+        t.pss = z2;
+        t.gamma0 = z2;
+        t.hfrag = z1;
+        t.adjoint = false;
+        if (part == 0) {
+            t.khat = z2;
+        } else {
+            t.chat = z1;
+        }
+        if (int rc = launch_stage(h, EPI_ACC, in, nullptr, h->flow_scratch.p, dst->data.p,
+                                  make_double2(acc_coeff, 0.0), 0, &t))
+            return rc;
+    }
+    return 0;
+}
+
 int ensure_work(heom_handle* h, int count)
 {
     for (int q = 0; q < count; ++q)
@@ -695,12 +724,47 @@ int enqueue_field_step(heom_handle* h, double dt)
     return launch_stage(h, EPI_AXPY_Y, s1, acc, y, nullptr, c(dt / 6), 0, &t1);
 }
 
+// one RK4 step with flow tracking (population_dynamics_solver.hpp:236-263 with
+// track_flows): the flow buffers are zeroed, then the classical RK4 of four
+// pure evaluations and rk_weighted_add (the reference's structure) runs with
+// every evaluation of stage input s_i adding dt b_i x its plus and minus
+// terms, b = (1/6, 1/3, 1/3, 1/6): after the step the buffers hold the
+// step's flows from the layer above and from the layer below
+int enqueue_flow_step(heom_handle* h, double dt)
+{
+    for (heom_buffer* b : {h->flow_above, h->flow_below})
+        if (b) CUDA_TRY(cudaMemsetAsync(b->data.p, 0, h->state_elems() * sizeof(double2), h->stream));
+    double2* y = h->y.data.p;
+    const double2 zero = make_double2(0.0, 0.0);
+    double2* k1 = h->work[0].p;
+    double2* k2 = h->work[1].p;
+    double2* k3 = h->work[2].p;
+    double2* k4 = h->work[3].p;
+    double2* st = h->work[4].p;
+    const double2* ks[4] = {k1, k2, k3, k4};
+    const double a2[1] = {0.5}, a3[2] = {0.0, 0.5}, a4[3] = {0.0, 0.0, 1.0};
+    const double bb[4] = {1.0 / 6, 1.0 / 3, 1.0 / 3, 1.0 / 6};
+    if (int rc = launch_stage(h, EPI_PURE, y, nullptr, k1, nullptr, zero, 0)) return rc;
+    if (int rc = launch_flows(h, y, dt * bb[0])) return rc;
+    if (int rc = launch_wadd(h, 1, dt, st, y, a2, ks)) return rc;
+    if (int rc = launch_stage(h, EPI_PURE, st, nullptr, k2, nullptr, zero, 0)) return rc;
+    if (int rc = launch_flows(h, st, dt * bb[1])) return rc;
+    if (int rc = launch_wadd(h, 2, dt, st, y, a3, ks)) return rc;
+    if (int rc = launch_stage(h, EPI_PURE, st, nullptr, k3, nullptr, zero, 0)) return rc;
+    if (int rc = launch_flows(h, st, dt * bb[2])) return rc;
+    if (int rc = launch_wadd(h, 3, dt, st, y, a4, ks)) return rc;
+    if (int rc = launch_stage(h, EPI_PURE, st, nullptr, k4, nullptr, zero, 0)) return rc;
+    if (int rc = launch_flows(h, st, dt * bb[3])) return rc;
+    return launch_wadd(h, 4, dt, y, y, bb, ks);
+}
+
 // enqueue one RK4 step of y_n (in place) on the handle's stream
 int enqueue_step(heom_handle* h, double dt)
 {
     double2* y = h->y.data.p;
     const double2 zero = make_double2(0.0, 0.0);
     if (h->field_on) return enqueue_field_step(h, dt);
+    if (h->flow_above || h->flow_below) return enqueue_flow_step(h, dt);
     switch (h->opt.rk4_scheme) {
     case HEOM_RK4_PRODUCT: {
         double2* a = h->work[0].p;
@@ -748,6 +812,7 @@ int enqueue_step(heom_handle* h, double dt)
 int prepare_scheme(heom_handle* h)
 {
     if (h->field_on) return ensure_work(h, 3);
+    if (h->flow_above || h->flow_below) return ensure_work(h, 5);
     switch (h->opt.rk4_scheme) {
     case HEOM_RK4_PRODUCT:
     case HEOM_RK4_HORNER: return ensure_work(h, 2);
@@ -759,6 +824,7 @@ int prepare_scheme(heom_handle* h)
 int launches_per_step(const heom_handle* h)
 {
     if (h->field_on) return 5;
+    if (h->flow_above || h->flow_below) return 8 + 4 * ((h->flow_above ? 1 : 0) + (h->flow_below ? 1 : 0));
     return h->opt.rk4_scheme == HEOM_RK4_REFERENCE ? 8 : 4;
 }
 
@@ -1405,6 +1471,22 @@ int heom_get_mask(const heom_handle* h, uint8_t* mask)
     return 0;
 }
 
+int heom_buffer_hierarchy_norm(heom_handle* h, const heom_buffer* b, double* norms)
+{
+    if (!h || !b || b->owner != h || !norms) return fail(HEOM_E_ARG, "bad argument");
+    CUDA_TRY(cudaSetDevice(h->device));
+    DevBuf<double> d_norm;
+    if (int rc = d_norm.alloc(h->nodes)) return rc;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((h->nodes + 7) / 8, (int64_t)h->sm_count * 8));
+    heomk::heom_hierarchy_norm<<<blocks, 256, 0, h->stream>>>(d_norm.p, b->data.p, h->d_ref_of_int.p, h->d_pair.p,
+                                                              h->nodes, h->P);
+    h->launches++;
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(norms, d_norm.p, h->nodes * 8, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
 int heom_hierarchy_norm(heom_handle* h, double threshold, double* norms)
 {
     if (!h) return fail(HEOM_E_ARG, "NULL handle");
@@ -1454,8 +1536,14 @@ int heom_buffer_destroy(heom_buffer* b)
     if (b->borrowed) return fail(HEOM_E_ARG, "cannot destroy a borrowed buffer view");
     if (heom_handle* h = b->owner) {
         cudaSetDevice(h->device);
-        if (h->flow_above == b) h->flow_above = nullptr;
-        if (h->flow_below == b) h->flow_below = nullptr;
+        if (h->flow_above == b || h->flow_below == b) {
+            if (h->flow_above == b) h->flow_above = nullptr;
+            if (h->flow_below == b) h->flow_below = nullptr;
+            if (h->step_graph) {
+                cudaGraphExecDestroy(h->step_graph);
+                h->step_graph = nullptr;
+            }
+        }
         auto& v = h->live_buffers;
         v.erase(std::remove(v.begin(), v.end(), b), v.end());
     }
@@ -1519,32 +1607,7 @@ int heom_solve(heom_handle* h, double time, double step_size, const heom_buffer*
     default: return fail(HEOM_E_ARG, "unknown solve mode %d", mode);
     }
     if (rc) return rc;
-    if (h->flow_above || h->flow_below) {
-        // heom_ode.cl:436-441: flow_from_above += acc_coeff * plus term, flow_from_below += acc_coeff * minus
-        // term; each term alone is L with H, the same term and the other term's coefficients zeroed
-        const double2* z2 = reinterpret_cast<const double2*>(h->d_zero.p);
-        const double* z1 = h->d_zero.p;
-        for (int part = 0; part < 2; ++part) {
-            heom_buffer* dst = part == 0 ? h->flow_above : h->flow_below;
-            if (!dst) continue;
-            AdjTabs t;
-            t.pss = z2;
-            t.gamma0 = z2;
-            t.hfrag = z1;
-            t.adjoint = false;
-            if (part == 0) {
-                t.khat = z2;
-            } else {
-                t.chat = z1;
-            }
-            if (tabs) { // keep the time-dependent H out of the bath terms too
-                t.hfrag = z1;
-            }
-            rc = launch_stage(h, EPI_ACC, in->data.p, nullptr, h->flow_scratch.p, dst->data.p,
-                              make_double2(acc_coeff, 0.0), 0, &t);
-            if (rc) return rc;
-        }
-    }
+    if (int frc = launch_flows(h, in->data.p, acc_coeff)) return frc;
     CUDA_TRY(cudaStreamSynchronize(h->stream));
     return check_kernel_error(h);
 }
@@ -1567,6 +1630,10 @@ int heom_set_flow_buffers(heom_handle* h, heom_buffer* flow_from_above, heom_buf
     }
     h->flow_above = flow_from_above;
     h->flow_below = flow_from_below;
+    if (h->step_graph) { // the captured step does not track (or stops tracking) the flows
+        cudaGraphExecDestroy(h->step_graph);
+        h->step_graph = nullptr;
+    }
     return 0;
 }
 

@@ -198,6 +198,42 @@ int main(int argc, char* argv[])
         std::vector<std::unique_ptr<file_observer>> obs;
         for (const auto& o : cfg.observations()) obs.emplace_back(new file_observer(o, n, h, g));
 
+        // flow tracking (population_dynamics_solver.hpp:141-150, 236-263): two
+        // flow buffers handed to the derivative, zeroed at every step by the
+        // stepping calls, their hierarchy norms taken after the step.  The
+        // reference computes the norms but writes no file; with a
+        // solver.flow_filename this application writes, at every observation,
+        // the sum over ADOs of each buffer's norm for the last step.
+        heom_buffer* flow_b[2] = {nullptr, nullptr};
+        std::unique_ptr<heom_buffer, int (*)(heom_buffer*)> flow_a_guard(nullptr, heom_buffer_destroy);
+        std::unique_ptr<heom_buffer, int (*)(heom_buffer*)> flow_b_guard(nullptr, heom_buffer_destroy);
+        std::ofstream flow_out;
+        std::vector<double> flow_norm(cfg.track_flows() ? inst.matrices : 0);
+        if (cfg.track_flows()) {
+            check(heom_buffer_create(h, &flow_b[0]));
+            flow_a_guard.reset(flow_b[0]);
+            check(heom_buffer_create(h, &flow_b[1]));
+            flow_b_guard.reset(flow_b[1]);
+            check(heom_set_flow_buffers(h, flow_b[0], flow_b[1]));
+            if (!cfg.flow_filename().empty()) {
+                flow_out.open(cfg.flow_filename());
+                if (!flow_out.is_open()) throw std::runtime_error("could not open flow file: " + cfg.flow_filename());
+                flow_out << "time" << kDelim << "flow_from_above_norm" << kDelim << "flow_from_below_norm" << '\n';
+                per_observation = true; // the flows are read after every observation's steps
+            }
+        }
+        auto observe_flows = [&](double time) {
+            if (!flow_out.is_open()) return;
+            flow_out << fmt(time);
+            for (heom_buffer* b : flow_b) {
+                check(heom_buffer_hierarchy_norm(h, b, flow_norm.data()));
+                double sum = 0.0;
+                for (double v : flow_norm) sum += v;
+                flow_out << kDelim << fmt(sum);
+            }
+            flow_out << '\n';
+        };
+
         const int64_t observe_steps = cfg.observe_steps();
         const int64_t iterations = cfg.steps() / observe_steps;
         const double dt = cfg.step_size();
@@ -211,6 +247,7 @@ int main(int argc, char* argv[])
                 check(heom_rk4_steps(h, dt, observe_steps));
                 check(heom_get_top(h, top.data()));
                 for (auto& o : obs) o->observe((double)(i * observe_steps) * dt, top.data());
+                observe_flows((double)(i * observe_steps) * dt);
             }
         } else {
             for (int64_t i = 0; i < iterations; i += chunk) {

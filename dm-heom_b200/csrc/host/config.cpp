@@ -206,7 +206,7 @@ config::config(const std::string& path)
     step_size_ = parse_real(raw("solver.step_size"));
     steps_ = parse_int(raw("solver.steps"));
     track_flows_ = parse_bool(raw("solver.track_flows"));
-    (void)raw("solver.flow_filename");
+    flow_filename_ = raw("solver.flow_filename");
 
     // system / baths, config units
     const int64_t sites = parse_int(raw("system.sites"));

@@ -127,6 +127,7 @@ public:
     double step_size() const { return step_size_; }
     int64_t steps() const { return steps_; }
     bool track_flows() const { return track_flows_; }
+    const std::string& flow_filename() const { return flow_filename_; }
     // configuration values in config units (cm^-1, fs)
     const heom_system_desc& system_desc() const { return desc_; }
     const system_params& system() const { return sys_; }   // SI
@@ -152,6 +153,7 @@ private:
     double step_size_ = 0.0;
     int64_t steps_ = 0;
     bool track_flows_ = false;
+    std::string flow_filename_;
     heom_system_desc desc_{};
     std::vector<double> h_flat_, lambda_, invnu_, omega_;
     std::vector<int32_t> coupling_;

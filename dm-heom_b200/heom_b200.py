@@ -54,7 +54,7 @@ EXPORTS = [
     "heom_tables_state", "heom_adjoint_set_memory_limit", "heom_adjoint_recursive_slots",
     "heom_ensemble_adjoint_create", "heom_ensemble_adjoint_destroy", "heom_ensemble_adjoint_set_memory_limit",
     "heom_ensemble_adjoint_gradient", "heom_ensemble_adjoint_groups", "heom_ensemble_adjoint_group_of",
-    "heom_ensemble_adjoint_offset", "heom_ensemble_adjoint_kernel_launches",
+    "heom_ensemble_adjoint_offset", "heom_ensemble_adjoint_kernel_launches", "heom_buffer_hierarchy_norm",
 ]
 
 PRE_EVALUATE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_void_p)
@@ -117,6 +117,7 @@ def lib():
         L.heom_clear_field.argtypes = [vp]
         L.heom_set_time.argtypes = [vp, dbl]
         L.heom_set_flow_buffers.argtypes = [vp, vp, vp]
+        L.heom_buffer_hierarchy_norm.argtypes = [vp, vp, vp]
         L.heom_add_pre_evaluate_action.argtypes = [vp, PRE_EVALUATE_FN, vp]
         L.heom_clear_pre_evaluate_actions.argtypes = [vp]
         for name in ["heom_hierarchy_add", "heom_hierarchy_subtract", "heom_hierarchy_dot_product"]:
@@ -503,6 +504,12 @@ class Heom:
 
     def set_flow_buffers(self, above: Buffer | None, below: Buffer | None):
         _check(lib().heom_set_flow_buffers(self.h, above.h if above else None, below.h if below else None))
+
+    def buffer_norm(self, b: Buffer):
+        """Per-ADO sum |sigma_ij|^2 of a buffer (uid order)."""
+        v = np.empty(self.matrices)
+        _check(lib().heom_buffer_hierarchy_norm(self.h, b.h, _ptr(v)))
+        return v
 
     def weighted_add(self, step, out: Buffer, y: Buffer, coeffs, ks):
         c = np.ascontiguousarray(np.asarray(coeffs, np.float64))

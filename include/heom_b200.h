@@ -224,8 +224,18 @@ int heom_solve(heom_handle* h, double time, double step_size, const heom_buffer*
  * element by element, reference layout in the buffers).  NULL buffers switch
  * tracking off.  (The reference kernel tests NOMA_NUM_ODE_TRACK_FLOWS while its
  * solver defines HEOM_ODE_TRACK_FLOWS; this build tracks whenever the buffers
- * are set.) */
+ * are set.)  While set, heom_rk4_steps and heom_propagate step as the
+ * reference's population_dynamics_solver::step_forward does with
+ * solver.track_flows (population_dynamics_solver.hpp:236-263): every step
+ * zeroes the buffers, then runs the classical RK4 of four pure evaluations and
+ * rk_weighted_add (the HEOM_RK4_REFERENCE structure, whatever the handle's
+ * scheme), evaluation i adding dt b_i times its terms (b = 1/6, 1/3, 1/3,
+ * 1/6); after a call the buffers hold the last step's flows. */
 int heom_set_flow_buffers(heom_handle* h, heom_buffer* flow_from_above, heom_buffer* flow_from_below);
+/* The hierarchy norm (sum |sigma_ij|^2 per ADO, uid order) of a buffer, as
+ * population_dynamics_solver::update_flow_norm takes it of the flow buffers
+ * (population_dynamics_solver.hpp:195-200, hierarchy_norm.cl:15-45). */
+int heom_buffer_hierarchy_norm(heom_handle* h, const heom_buffer* b, double* norms);
 /* out = y + step_size * sum_l coeffs[l] * k[l] (0 <= n <= 7), terms with a zero
  * coefficient skipped, in rk_weighted_add's operation order. */
 int heom_weighted_add(heom_handle* h, int n, double step_size, heom_buffer* out,

@@ -324,3 +324,98 @@ def test_gradient_subset_skips_work_and_keeps_bits():
     assert only_h["lambda"] is None and only_h["rho0"] is None and only_bath["h"] is None
     assert np.array_equal(only_h["h"], full["h"]) and only_h["loss"] == full["loss"]
     assert only_bath["lambda"] == full["lambda"] and only_bath["gamma"] == full["gamma"]
+
+
+def test_adjoint_at_full_size_matches_oracle_tangents():
+    """The adjoint of the 7-site, depth-8 hierarchy (6435 ADOs; the size of the
+    adjoint benchmark) against an FP64 reference gradient that shares no code
+    with it: forward-mode tangents of the oracle's RK4 steps,
+      dk1 = L dy + L' y, ..., dy_{n+1} = dy + dt/6 (dk1 + 2 dk2 + 2 dk3 + dk4),
+    with L' the derivative of the operator along the parameter.  For an H
+    entry L' is exact (L is affine in H: L' v = i/hbar (v E - E v) on every
+    ADO; checked against a difference of two oracle operators); for lambda
+    and gamma it is a central difference of oracle operators (steps 1e-4
+    relative), whose O(step^2) error bounds the comparison at 1e-6.
+    50 RK4 steps of 1 fs; loss = trapezoid integral of the site-3 population;
+    gradients w.r.t. the 7 site energies, 3 couplings (symmetric), lambda and
+    gamma."""
+    n, depth, steps, dt_fs = 7, 8, 50, 1.0
+    dt = dt_fs * 1e-15
+    h = ho.synthetic_hamiltonian(n, 44)
+    lam, inv = 35.0, 50.0
+    w = hb.trapezoid_weights(steps, dt_fs)
+    rho0 = np.zeros((n, n), complex)
+    rho0[0, 0] = 1.0
+    obs = np.zeros((n, n), complex)
+    obs[2, 2] = 1.0
+
+    with hb.Adjoint(hb.System(h, [lam] * n, [inv] * n, [0.0] * n, 1, 300.0, depth)) as A:
+        gpu = A.gradient(rho0, obs, w, dt, steps)
+
+    base = problem(h, lam, inv, 1, depth)
+    L = lambda prob, v: ho.derivative(prob, v)
+    y = base.initial_state()
+    j_idx = 2 * (2 * n + 2)  # Re rho(2, 2) of the top ADO
+    stages = []  # stage inputs of every step, for the tangents
+    J = w[0] * y[j_idx]
+    for k in range(steps):
+        k1 = L(base, y)
+        s2 = y + 0.5 * dt * k1
+        k2 = L(base, s2)
+        s3 = y + 0.5 * dt * k2
+        k3 = L(base, s3)
+        s4 = y + dt * k3
+        k4 = L(base, s4)
+        stages.append((y, s2, s3, s4))
+        y = y + dt / 6.0 * (k1 + 2.0 * k2 + 2.0 * k3 + k4)
+        J += w[k + 1] * y[j_idx]
+    assert abs(J - gpu["loss"]) <= 1e-12 * abs(J)
+
+    def tangent(dL):
+        dy = np.zeros_like(y)
+        dJ = 0.0
+        for k in range(steps):
+            dJ += w[k] * dy[j_idx]
+            y0, s2, s3, s4 = stages[k]
+            dk1 = L(base, dy) + dL(y0)
+            dk2 = L(base, dy + 0.5 * dt * dk1) + dL(s2)
+            dk3 = L(base, dy + 0.5 * dt * dk2) + dL(s3)
+            dk4 = L(base, dy + dt * dk3) + dL(s4)
+            dy = dy + dt / 6.0 * (dk1 + 2.0 * dk2 + 2.0 * dk3 + dk4)
+        return dJ + w[steps] * dy[j_idx]
+
+    hbar = 1.05457148e-34  # the reference's value (common.cl, constants.hpp)
+
+    def comm_dir(E_cm):
+        E = E_cm * INVCM
+
+        def apply(v):
+            s = v.view(np.complex128).reshape(-1, n, n)
+            return (1j / hbar * (s @ E - E @ s)).reshape(-1).view(np.float64)
+        return apply
+
+    # the exact H direction against a difference of two oracle operators
+    v = np.random.default_rng(5).normal(size=base.state_len)
+    E = np.zeros((n, n))
+    E[1, 4] = E[4, 1] = 1.0
+    diff = L(problem(h + E, lam, inv, 1, depth), v) - L(base, v)
+    assert np.max(np.abs(comm_dir(E)(v) - diff)) <= 1e-9 * np.max(np.abs(diff))
+
+    g_h = gpu["h"].real
+    entries = [(a, a) for a in range(n)] + [(0, 1), (1, 4), (2, 6)]
+    for (a, b) in entries:
+        E = np.zeros((n, n))
+        E[a, b] = E[b, a] = 1.0
+        ref = tangent(comm_dir(E))
+        got = g_h[a, b] + (g_h[b, a] if a != b else 0.0)
+        assert abs(got - ref) <= 1e-9 * max(abs(ref), 1e-3 * np.max(np.abs(g_h))), (a, b, got, ref)
+
+    dl = 1e-4 * lam
+    pl, ml = problem(h, lam + dl, inv, 1, depth), problem(h, lam - dl, inv, 1, depth)
+    ref_l = tangent(lambda v: (L(pl, v) - L(ml, v)) / (2 * dl))
+    assert abs(gpu["lambda"] - ref_l) <= 1e-6 * abs(ref_l), (gpu["lambda"], ref_l)
+    g = 1.0 / inv
+    dg = 1e-4 * g
+    pg, mg = problem(h, lam, 1.0 / (g + dg), 1, depth), problem(h, lam, 1.0 / (g - dg), 1, depth)
+    ref_g = tangent(lambda v: (L(pg, v) - L(mg, v)) / (2 * dg))
+    assert abs(gpu["gamma"] - ref_g) <= 1e-6 * abs(ref_g), (gpu["gamma"], ref_g)

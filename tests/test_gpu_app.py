@@ -168,3 +168,54 @@ def test_circular_dichroism_app_matches_oracle(tmp_path):
     scale = np.max(np.abs(want))
     assert np.max(np.abs(got[:, 1] - want.real)) <= 1e-10 * scale
     assert np.max(np.abs(got[:, 2] - want.imag)) <= 1e-10 * scale
+
+
+def test_app_tracks_flows_like_the_reference_solver(tmp_path):
+    """solver.track_flows = true (population_dynamics_solver.hpp:141-150,
+    236-263): the application hands two flow buffers to the derivative, the
+    stepping zeroes them at every step and accumulates dt b_i x the plus and
+    minus terms of every evaluation; the flow file holds, at every
+    observation, the sum over ADOs of each buffer's hierarchy norm after the
+    last step.  Checked against the reference's own kernel terms (the kernel
+    built with HEOM_ODE_DISABLE_PLUS / _MINUS) over the classical RK4 stage
+    inputs of the oracle; the populations are those of the untracked run."""
+    cfg = FMO_CFG.replace("track_flows=false", "track_flows=true").replace("flow_filename=", "flow_filename=f.dat")
+    (tmp_path / "heom.cfg").write_text(cfg)
+    (tmp_path / "rt.cfg").write_text("[cuda]\ndevice_index=0\n")
+    r = subprocess.run([APP, "rt.cfg", "heom.cfg"], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    h = np.array([[12410.0, -87.7, 5.5], [-87.7, 12530.0, 30.8], [5.5, 30.8, 12210.0]])
+    prob = ho.build_problem(ho.make_system(h, [35] * 3, [50] * 3, [0] * 3, 2, 77.0, 3))
+    dt = 1e-15
+    _, ref = ho.propagate(prob, dt, 20, 5)
+    _, d = read_dat(tmp_path / "d.dat")
+    assert_pops(d[:, 1:], ref)
+    hf, f = read_dat(tmp_path / "f.dat")
+    assert hf == ["time", "flow_from_above_norm", "flow_from_below_norm"]
+    assert f.shape == (4, 3)  # one row per observation after t = 0
+
+    def terms(v):
+        full, _ = ho.ref_derivative(prob, v)
+        return full - ho.ref_derivative(prob, v, mode=3)[0], full - ho.ref_derivative(prob, v, mode=4)[0]
+
+    y = prob.initial_state()
+    for obs_row in range(4):
+        for step in range(5):
+            k1, _ = ho.ref_derivative(prob, y)
+            s2 = y + 0.5 * dt * k1
+            k2, _ = ho.ref_derivative(prob, s2)
+            s3 = y + 0.5 * dt * k2
+            k3, _ = ho.ref_derivative(prob, s3)
+            s4 = y + dt * k3
+            k4, _ = ho.ref_derivative(prob, s4)
+            above = np.zeros_like(y)
+            below = np.zeros_like(y)
+            for s, b in zip((y, s2, s3, s4), (1 / 6, 1 / 3, 1 / 3, 1 / 6)):
+                p, m = terms(s)
+                above += dt * b * p
+                below += dt * b * m
+            y = y + dt / 6 * (k1 + 2 * k2 + 2 * k3 + k4)
+        want = [float(np.sum(x ** 2)) for x in (above, below)]
+        assert f[obs_row, 0] == pytest.approx((obs_row + 1) * 5 * dt, rel=1e-14)
+        for c in range(2):
+            assert abs(f[obs_row, 1 + c] - want[c]) <= 1e-10 * want[c], (obs_row, c, f[obs_row, 1 + c], want[c])
