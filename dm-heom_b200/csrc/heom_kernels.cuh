@@ -254,6 +254,42 @@ __device__ __forceinline__ void ld256_cg(const double2* src, double2& a, double2
                  : "l"(src));
 }
 
+// 32 bytes when ok, zeros otherwise, without a branch (non-coherent path: data the kernel does not write)
+__device__ __forceinline__ void ld256_if(bool ok, const double2* src, double2& a, double2& b)
+{
+    asm("{\n .reg .pred q;\n setp.ne.u32 q, %5, 0;\n"
+        " mov.f64 %0, 0d0000000000000000;\n mov.f64 %1, 0d0000000000000000;\n"
+        " mov.f64 %2, 0d0000000000000000;\n mov.f64 %3, 0d0000000000000000;\n"
+        " @q ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];\n}\n"
+        : "=d"(a.x), "=d"(a.y), "=d"(b.x), "=d"(b.y)
+        : "l"(src), "r"((unsigned)ok));
+}
+
+// as ld256_if, through the coherent path (data this kernel writes afterwards)
+__device__ __forceinline__ void ld256_cg_if(bool ok, const double2* src, double2& a, double2& b)
+{
+    asm volatile("{\n .reg .pred q;\n setp.ne.u32 q, %5, 0;\n"
+                 " mov.f64 %0, 0d0000000000000000;\n mov.f64 %1, 0d0000000000000000;\n"
+                 " mov.f64 %2, 0d0000000000000000;\n mov.f64 %3, 0d0000000000000000;\n"
+                 " @q ld.global.v4.f64 {%0,%1,%2,%3}, [%4];\n}\n"
+                 : "=d"(a.x), "=d"(a.y), "=d"(b.x), "=d"(b.y)
+                 : "l"(src), "r"((unsigned)ok));
+}
+
+// 32-byte stores when ok, without a branch (streaming / default cache policy)
+__device__ __forceinline__ void st256_cs_if(bool ok, double2* dst, double2 a, double2 b)
+{
+    asm volatile("{\n .reg .pred q;\n setp.ne.u32 q, %5, 0;\n @q st.global.cs.v4.f64 [%0], {%1,%2,%3,%4};\n}\n" ::"l"(dst),
+                 "d"(a.x), "d"(a.y), "d"(b.x), "d"(b.y), "r"((unsigned)ok)
+                 : "memory");
+}
+__device__ __forceinline__ void st256_if(bool ok, double2* dst, double2 a, double2 b)
+{
+    asm volatile("{\n .reg .pred q;\n setp.ne.u32 q, %5, 0;\n @q st.global.v4.f64 [%0], {%1,%2,%3,%4};\n}\n" ::"l"(dst),
+                 "d"(a.x), "d"(a.y), "d"(b.x), "d"(b.y), "r"((unsigned)ok)
+                 : "memory");
+}
+
 __device__ __forceinline__ void st256_cs(double2* dst, double2 a, double2 b)
 {
     asm volatile("st.global.cs.v4.f64 [%0], {%1,%2,%3,%4};\n" ::"l"(dst), "d"(a.x), "d"(a.y), "d"(b.x),
@@ -585,6 +621,30 @@ __global__ void __launch_bounds__(kCtaWarps * 32, 2) heom_dmma_stage(const DmmaP
 }
 
 // ---------------------------------------------------------------------------
+// Lockstep ensembles (N <= 8): K instances that share the hierarchy graph and
+// the bath tables and differ in H only (the realisations of a static-disorder
+// ensemble of one depth) are stored instance-minor: sector p of ADO u of
+// instance k at sector index (u * P + p) * Kp + k (Kp = K rounded up to 32),
+// so that the 32 instances of a block sit side by side in every row.
+//
+// Work item = (ADO u, block of 32 instances), swept grid-stride by a CTA of
+// eight warps:
+//   A  the block's 32 tiles arrive by 16-byte cp.async in a shared tile
+//      [p][32] whose columns are swizzled (k ^ (p & 3)), which keeps the
+//      conflict-free operand reads of the pair order; warp w computes the
+//      commutator of instances w, w+8, w+16, w+24 on the tensor pipe (the
+//      operand mapping and exchange of heom_dmma_stage) and writes the two
+//      commutator values of every sector into a second shared tile;
+//   B  warp w takes sectors w, w+8, ...; lane k is instance k of the block.
+//      Neighbour indices, tuple entries and bath coefficients are the same
+//      for every lane (warp-uniform), and each neighbour read is one
+//      contiguous 1-KB row (32 instances x 32 B) of the neighbour ADO, where
+//      heom_dmma_stage gathers 32-B sectors of eight different neighbours.
+// The derivative is the same element by element as heom_dmma_stage's (the
+// same bath-term order; the commutator from the same MMA sequence).
+// ---------------------------------------------------------------------------
+
+// ---------------------------------------------------------------------------
 // N = 9..16: a team of TW = ceil(P / 32) warps per ADO, thread p of the team
 // owns sector p.  Teams loop over ADOs (grid-stride) with a two-slot
 // pipeline: while ADO k is computed, its successor's tile (scattered into the
@@ -905,17 +965,26 @@ __global__ void heom_from_pairs(double2* __restrict__ ref, const double2* __rest
 
 // Copy the top matrix of every instance (block k: internal ADO tops[k], pair
 // layout) into row `row` of a row-major log [rows][n_inst][n*n].
+// sector index of sector p of internal ADO u: the per-instance layout (kp = 0)
+// or the lockstep layout of instance k (stride kp)
+__device__ __forceinline__ int64_t sector_index(int64_t u, int p, int P, int64_t kp, int64_t k)
+{
+    return kp ? (u * P + p) * kp + k : u * P + p;
+}
+
+// block b: the instance k0 + b of a lockstep handle (kp > 0), ignored otherwise
 __global__ void heom_record_top(double2* __restrict__ log, const double2* __restrict__ y,
                                 const int16_t* __restrict__ pe, const int64_t* __restrict__ tops, int n, int P,
-                                int64_t row)
+                                int64_t row, int64_t kp, int64_t k0)
 {
     const int k = blockIdx.x;
     const int64_t u = tops[k];
     double2* dst = log + (row * gridDim.x + k) * n * n;
     for (int pr = threadIdx.x; pr < P; pr += blockDim.x) {
         const int e1 = pe[2 * pr], e2 = pe[2 * pr + 1];
-        dst[e1] = y[(u * P + pr) * 2];
-        if (e2 != e1) dst[e2] = y[(u * P + pr) * 2 + 1];
+        const int64_t sx = sector_index(u, pr, P, kp, k0 + k);
+        dst[e1] = y[sx * 2];
+        if (e2 != e1) dst[e2] = y[sx * 2 + 1];
     }
 }
 
@@ -937,14 +1006,16 @@ __global__ void heom_record_top_at(double2* __restrict__ log, const double2* __r
 // Write row-major top matrices top[k] ([n_inst][n*n]) into the pair layout
 // of each instance's top ADO (block k).
 __global__ void heom_write_top(double2* __restrict__ y, const double2* __restrict__ top,
-                               const int16_t* __restrict__ pe, const int64_t* __restrict__ tops, int n, int P)
+                               const int16_t* __restrict__ pe, const int64_t* __restrict__ tops, int n, int P,
+                               int64_t kp, int64_t k0)
 {
     const int k = blockIdx.x;
     const int64_t u = tops[k];
     const double2* src = top + (int64_t)k * n * n;
     for (int pr = threadIdx.x; pr < P; pr += blockDim.x) {
-        y[(u * P + pr) * 2] = src[pe[2 * pr]];
-        y[(u * P + pr) * 2 + 1] = src[pe[2 * pr + 1]];
+        const int64_t sx = sector_index(u, pr, P, kp, k0 + k);
+        y[sx * 2] = src[pe[2 * pr]];
+        y[sx * 2 + 1] = src[pe[2 * pr + 1]];
     }
 }
 

@@ -19,6 +19,7 @@
 
 #include "heom_b200.h"
 #include "heom_kernels.cuh"
+#include "heom_lockstep.cuh"
 #include "host/heom_host.hpp"
 
 namespace {
@@ -165,6 +166,30 @@ dmma_fn_t pick_dmma(int n, int hk, int slt, bool multi, bool adj)
     }
 }
 
+typedef void (*lock_fn_t)(const heomk::LockParams);
+
+template <int N, int HK>
+lock_fn_t pick_lslt(int slt)
+{
+    return slt <= 1   ? heomk::heom_lockstep_stage<N, HK, 1>
+           : slt <= 2 ? heomk::heom_lockstep_stage<N, HK, 2>
+                      : heomk::heom_lockstep_stage<N, HK, 4>;
+}
+
+// lockstep ensemble kernel: N = 1..8, at most four slots per state
+lock_fn_t pick_lock(int n, int hk, int slt)
+{
+    if (slt > 4) return nullptr;
+    switch (n) {
+#define HEOM_CASE(K) \
+    case K: return hk == heomk::H_REAL_SYM ? pick_lslt<K, heomk::H_REAL_SYM>(slt) : pick_lslt<K, heomk::H_GENERIC>(slt);
+        HEOM_CASE(1) HEOM_CASE(2) HEOM_CASE(3) HEOM_CASE(4) HEOM_CASE(5) HEOM_CASE(6)
+        HEOM_CASE(7) HEOM_CASE(8)
+#undef HEOM_CASE
+    default: return nullptr;
+    }
+}
+
 // tables that replace the handle's own in one stage launch: those of the
 // adjoint operator L^H (adjoint = true: conj(pf_same_sum), conj(gamma0), -H^H),
 // or those of a time-dependent H(t) (adjoint = false, handle's pss and gamma0)
@@ -296,7 +321,12 @@ struct heom_handle {
     cudaGraphExec_t step_graph = nullptr;
     double graph_dt = 0.0;
 
-    size_t state_elems() const { return (size_t)nodes * 2 * P; } // double2 per internal state
+    // lockstep layout (instances of one hierarchy graph, ensembles only): sector
+    // p of internal ADO u of instance k at sector index (u * P + p) * kp + k
+    int64_t kp = 0;          // instance stride (instances rounded up to 32); 0: the per-instance layout
+    int64_t inst_nodes = 0;  // ADOs of every instance (lockstep)
+
+    size_t state_elems() const { return (size_t)(kp ? inst_nodes * kp : nodes) * 2 * P; } // double2 per state
     size_t ref_elems() const { return (size_t)nodes * N * N; }   // double2 per reference-layout state
 };
 
@@ -525,7 +555,12 @@ int resolve_stage(heom_handle* h, const void** fn_out, int* blocks_out = nullptr
     const void* fn = nullptr;
     size_t smem = 0;
     int threads = 0;
-    if (h->N <= 8) {
+    if (h->kp) {
+        if (adj) return fail(HEOM_E_UNSUPPORTED, "the lockstep layout has no adjoint stage");
+        fn = (const void*)pick_lock(h->N, h->hkind, h->SLT);
+        smem = heomk::lockstep_smem_bytes(h->P, h->W, h->NW, h->TWB, h->LS);
+        threads = heomk::kLockWarps * 32;
+    } else if (h->N <= 8) {
         fn = (const void*)pick_dmma(h->N, h->hkind, h->SLT, h->n_inst > 1, adj);
         smem = heomk::dmma_smem_bytes(h->P, h->W, h->NW, h->TWB, h->LS);
         threads = heomk::kCtaWarps * 32;
@@ -543,9 +578,15 @@ int resolve_stage(heom_handle* h, const void** fn_out, int* blocks_out = nullptr
         if (per_sm < 1) return fail(HEOM_E_UNSUPPORTED, "stage kernel cannot be resident");
     }
     const int teams = h->N <= 8 ? heomk::kCtaWarps : cta_teams(h->N);
-    const int64_t groups = std::max<int64_t>(1, (h->n_active + teams - 1) / teams);
+    const int64_t groups = h->kp ? h->inst_nodes * (h->kp / 32)
+                                 : std::max<int64_t>(1, (h->n_active + teams - 1) / teams);
     const int64_t want = h->grid_override > 0 ? h->grid_override : (int64_t)per_sm * h->sm_count;
-    if (blocks_out) *blocks_out = (int)std::max<int64_t>(1, std::min<int64_t>(groups, want));
+    int64_t blocks = std::max<int64_t>(1, std::min<int64_t>(groups, want));
+    if (h->kp) { // every CTA keeps one instance block: a multiple of the block count
+        const int64_t kb = h->kp / 32;
+        blocks = std::max<int64_t>(kb, blocks / kb * kb);
+    }
+    if (blocks_out) *blocks_out = (int)blocks;
     h->stage_smem = smem;
     *fn_out = fn;
     return 0;
@@ -606,6 +647,22 @@ int launch_stage(heom_handle* h, int epi, const double2* in, const double2* y, d
     dp.ct.sq = h->d_sq.p;
     dp.ct.pos = h->d_pos.p;
     dp.err = h->d_err.p;
+    if (h->kp) {
+        // lockstep: every instance uses instance 0's rows of the shared tables
+        heomk::LockParams lp;
+        lp.p = dp.p;
+        lp.p.nodes = h->inst_nodes;
+        lp.p.inst = nullptr;
+        lp.lt = dp.lt;
+        lp.ct = dp.ct;
+        lp.K = h->n_inst;
+        lp.Kp = (int)h->kp;
+        lp.nodes = h->inst_nodes;
+        ((lock_fn_t)fn)<<<blocks, heomk::kLockWarps * 32, h->stage_smem, h->stream>>>(lp);
+        h->launches++;
+        CUDA_TRY(cudaGetLastError());
+        return 0;
+    }
     ((dmma_fn_t)fn)<<<blocks, h->N <= 8 ? heomk::kCtaWarps * 32 : cta_threads(h->N), h->stage_smem, h->stream>>>(dp);
     h->launches++;
     CUDA_TRY(cudaGetLastError());
@@ -1064,6 +1121,42 @@ int from_internal(heom_handle* h, double* host, const double2* src)
 
 // rebuild the internal order (and everything indexed by it) after a change of
 // the mask or of the compaction mode; the propagation state keeps its values
+// Switch a freshly created batch handle whose instances share one hierarchy
+// graph (one depth) and have no mask to the lockstep layout: sector p of
+// internal ADO u of instance k at sector index (u * P + p) * kp + k, kp =
+// instances rounded up to 32.  Only the ensemble builds such handles; the
+// entry points that read or write the state in another layout refuse them.
+int make_lockstep(heom_handle* h)
+{
+    if (h->N > 8 || h->n_inst < 2 || h->SLT > 4 || h->compact || h->field_on)
+        return fail(HEOM_E_UNSUPPORTED, "lockstep layout: needs 2+ instances of at most 8 states");
+    const int64_t n0 = h->inst_base[1] - h->inst_base[0];
+    for (int k = 0; k < h->n_inst; ++k)
+        if (h->inst_base[k + 1] - h->inst_base[k] != n0 || h->inst_depth[k] != h->inst_depth[0])
+            return fail(HEOM_E_UNSUPPORTED, "lockstep layout: instances of different depths");
+    for (uint8_t m : h->mask)
+        if (!m) return fail(HEOM_E_UNSUPPORTED, "lockstep layout: masked hierarchies are not supported");
+    h->inst_nodes = n0;
+    h->kp = (h->n_inst + 31) / 32 * 32;
+    const std::vector<int64_t> tops(h->n_inst, h->top_int[0] - h->inst_base[0]);
+    CUDA_TRY(cudaMemcpy(h->d_top.p, tops.data(), tops.size() * 8, cudaMemcpyHostToDevice));
+    if (int rc = h->y.data.alloc(h->state_elems())) return rc;
+    CUDA_TRY(cudaMemset(h->y.data.p, 0, h->state_elems() * sizeof(double2)));
+    for (auto& w : h->work) w.reset();
+    for (auto& a : h->per_sm) a[0] = a[1] = 0;
+    h->stage_smem = 0;
+    if (h->step_graph) {
+        cudaGraphExecDestroy(h->step_graph);
+        h->step_graph = nullptr;
+    }
+    return 0;
+}
+
+int lockstep_refuses(const heom_handle* h, const char* what)
+{
+    return fail(HEOM_E_UNSUPPORTED, "%s: not available on a lockstep ensemble class (instance-minor state)", what);
+}
+
 int reorder(heom_handle* h)
 {
     std::vector<double> ref((size_t)h->nodes * h->N * h->N * 2);
@@ -1132,6 +1225,7 @@ int check_kernel_error(heom_handle* h)
 
 int hier_check(const heom_handle* h, const heom_buffer* a, const heom_buffer* b, const heom_buffer* out)
 {
+    if (h && h->kp) return lockstep_refuses(h, "hierarchy arithmetic");
     if (!h || !a || !out || a->owner != h || out->owner != h || (b && b->owner != h))
         return fail(HEOM_E_ARG, "buffers must belong to the handle");
     return 0;
@@ -1341,6 +1435,7 @@ int heom_set_instance_hamiltonian(heom_handle* h, int32_t inst, const double* ha
 
 int heom_set_mask(heom_handle* h, const uint8_t* mask)
 {
+    if (h && h->kp) return lockstep_refuses(h, "heom_set_mask");
     if (!h || !mask) return fail(HEOM_E_ARG, "NULL argument");
     CUDA_TRY(cudaSetDevice(h->device));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -1356,6 +1451,7 @@ int heom_set_mask(heom_handle* h, const uint8_t* mask)
 
 int heom_set_mask_compact(heom_handle* h, const uint8_t* mask)
 {
+    if (h && h->kp) return lockstep_refuses(h, "heom_set_mask_compact");
     if (!h || !mask) return fail(HEOM_E_ARG, "NULL argument");
     CUDA_TRY(cudaSetDevice(h->device));
     CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -1373,6 +1469,7 @@ int64_t heom_active_matrices(const heom_handle* h) { return h ? h->n_active : 0;
 int heom_set_field(heom_handle* h, const double* dipole_plus, const double* dipole_minus, const heom_pulse* pump,
                    const heom_pulse* probe)
 {
+    if (h && h->kp) return lockstep_refuses(h, "heom_set_field");
     if (!h || !dipole_plus || !dipole_minus || !pump || !probe) return fail(HEOM_E_ARG, "NULL argument");
     const heom_pulse* pl[2] = {pump, probe};
     for (int q = 0; q < 2; ++q)
@@ -1473,6 +1570,7 @@ int heom_get_mask(const heom_handle* h, uint8_t* mask)
 
 int heom_buffer_hierarchy_norm(heom_handle* h, const heom_buffer* b, double* norms)
 {
+    if (h && h->kp) return lockstep_refuses(h, "heom_buffer_hierarchy_norm");
     if (!h || !b || b->owner != h || !norms) return fail(HEOM_E_ARG, "bad argument");
     CUDA_TRY(cudaSetDevice(h->device));
     DevBuf<double> d_norm;
@@ -1489,6 +1587,7 @@ int heom_buffer_hierarchy_norm(heom_handle* h, const heom_buffer* b, double* nor
 
 int heom_hierarchy_norm(heom_handle* h, double threshold, double* norms)
 {
+    if (h && h->kp) return lockstep_refuses(h, "heom_hierarchy_norm");
     if (!h) return fail(HEOM_E_ARG, "NULL handle");
     CUDA_TRY(cudaSetDevice(h->device));
     DevBuf<double> d_norm;
@@ -1553,6 +1652,7 @@ int heom_buffer_destroy(heom_buffer* b)
 
 int heom_buffer_write(heom_handle* h, heom_buffer* b, const double* host)
 {
+    if (h && h->kp) return lockstep_refuses(h, "heom_buffer_write");
     if (!h || !b || !host || b->owner != h) return fail(HEOM_E_ARG, "bad argument");
     CUDA_TRY(cudaSetDevice(h->device));
     return to_internal(h, b->data.p, host);
@@ -1560,6 +1660,7 @@ int heom_buffer_write(heom_handle* h, heom_buffer* b, const double* host)
 
 int heom_buffer_read(heom_handle* h, const heom_buffer* b, double* host)
 {
+    if (h && h->kp) return lockstep_refuses(h, "heom_buffer_read");
     if (!h || !b || !host || b->owner != h) return fail(HEOM_E_ARG, "bad argument");
     CUDA_TRY(cudaSetDevice(h->device));
     return from_internal(h, host, b->data.p);
@@ -1568,6 +1669,7 @@ int heom_buffer_read(heom_handle* h, const heom_buffer* b, double* host)
 int heom_solve(heom_handle* h, double time, double step_size, const heom_buffer* in, heom_buffer* out,
                double out_coeff, heom_buffer* acc, double acc_coeff, int acc_init, int mode)
 {
+    if (h && h->kp) return lockstep_refuses(h, "heom_solve");
     if (!h || !in || in->owner != h) return fail(HEOM_E_ARG, "bad input buffer");
     CUDA_TRY(cudaSetDevice(h->device));
     int rc = 0;
@@ -1614,6 +1716,7 @@ int heom_solve(heom_handle* h, double time, double step_size, const heom_buffer*
 
 int heom_set_flow_buffers(heom_handle* h, heom_buffer* flow_from_above, heom_buffer* flow_from_below)
 {
+    if (h && h->kp) return lockstep_refuses(h, "heom_set_flow_buffers");
     if (!h) return fail(HEOM_E_ARG, "NULL handle");
     if ((flow_from_above && flow_from_above->owner != h) || (flow_from_below && flow_from_below->owner != h))
         return fail(HEOM_E_ARG, "flow buffers must belong to the handle");
@@ -1655,6 +1758,7 @@ int heom_weighted_add(heom_handle* h, int n, double step, heom_buffer* out, cons
 
 int heom_set_state(heom_handle* h, const double* host)
 {
+    if (h && h->kp) return lockstep_refuses(h, "heom_set_state");
     if (!h || !host) return fail(HEOM_E_ARG, "NULL argument");
     CUDA_TRY(cudaSetDevice(h->device));
     return to_internal(h, h->y.data.p, host);
@@ -1662,6 +1766,7 @@ int heom_set_state(heom_handle* h, const double* host)
 
 int heom_get_state(heom_handle* h, double* host)
 {
+    if (h && h->kp) return lockstep_refuses(h, "heom_get_state");
     if (!h || !host) return fail(HEOM_E_ARG, "NULL argument");
     CUDA_TRY(cudaSetDevice(h->device));
     return from_internal(h, host, h->y.data.p);
@@ -1674,7 +1779,7 @@ int heom_set_top(heom_handle* h, const double* top)
     const size_t nn = (size_t)h->N * h->N * h->n_inst;
     CUDA_TRY(cudaMemcpyAsync(h->topbuf.p, top, nn * 16, cudaMemcpyHostToDevice, h->stream));
     heomk::heom_write_top<<<h->n_inst, 128, 0, h->stream>>>(h->y.data.p, h->topbuf.p, h->d_pair.p, h->d_top.p, h->N,
-                                                            h->P);
+                                                            h->P, h->kp, 0);
     h->launches++;
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -1687,7 +1792,7 @@ int heom_get_top(heom_handle* h, double* top)
     CUDA_TRY(cudaSetDevice(h->device));
     const size_t nn = (size_t)h->N * h->N * h->n_inst;
     heomk::heom_record_top<<<h->n_inst, 128, 0, h->stream>>>(h->topbuf.p, h->y.data.p, h->d_pair.p, h->d_top.p, h->N,
-                                                             h->P, 0);
+                                                             h->P, 0, h->kp, 0);
     h->launches++;
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(top, h->topbuf.p, nn * 16, cudaMemcpyDeviceToHost, h->stream));
@@ -1703,7 +1808,7 @@ int heom_set_instance_top(heom_handle* h, int32_t inst, const double* top)
     const size_t nn = (size_t)h->N * h->N;
     CUDA_TRY(cudaMemcpyAsync(h->topbuf.p, top, nn * 16, cudaMemcpyHostToDevice, h->stream));
     heomk::heom_write_top<<<1, 128, 0, h->stream>>>(h->y.data.p, h->topbuf.p, h->d_pair.p, h->d_top.p + inst, h->N,
-                                                    h->P);
+                                                    h->P, h->kp, inst);
     h->launches++;
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -1717,7 +1822,7 @@ int heom_get_instance_top(heom_handle* h, int32_t inst, double* top)
     CUDA_TRY(cudaSetDevice(h->device));
     const size_t nn = (size_t)h->N * h->N;
     heomk::heom_record_top<<<1, 128, 0, h->stream>>>(h->topbuf.p, h->y.data.p, h->d_pair.p, h->d_top.p + inst, h->N,
-                                                     h->P, 0);
+                                                     h->P, 0, h->kp, inst);
     h->launches++;
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(top, h->topbuf.p, nn * 16, cudaMemcpyDeviceToHost, h->stream));
@@ -1763,13 +1868,13 @@ int heom_propagate(heom_handle* h, double dt, int64_t steps, int64_t observe_eve
     if ((int64_t)h->toplog.n < rows * nn)
         if (int rc = h->toplog.alloc(rows * nn)) return rc;
     heomk::heom_record_top<<<h->n_inst, 128, 0, h->stream>>>(h->toplog.p, h->y.data.p, h->d_pair.p, h->d_top.p, h->N,
-                                                             h->P, 0);
+                                                             h->P, 0, h->kp, 0);
     h->launches++;
     CUDA_TRY(cudaGetLastError());
     for (int64_t r = 1; r < rows; ++r) {
         if (int rc = run_steps(h, dt, observe_every)) return rc;
         heomk::heom_record_top<<<h->n_inst, 128, 0, h->stream>>>(h->toplog.p, h->y.data.p, h->d_pair.p, h->d_top.p,
-                                                                 h->N, h->P, r);
+                                                                 h->N, h->P, r, h->kp, 0);
         h->launches++;
         CUDA_TRY(cudaGetLastError());
     }
@@ -1790,6 +1895,7 @@ int heom_propagate(heom_handle* h, double dt, int64_t steps, int64_t observe_eve
 
 int heom_rk4_steps_noalloc(heom_handle* h, double* d_state, double dt, int64_t steps)
 {
+    if (h && h->kp) return lockstep_refuses(h, "heom_rk4_steps_noalloc");
     if (!h || !d_state || steps < 0 || !(dt > 0.0)) return fail(HEOM_E_ARG, "bad argument");
     if (reinterpret_cast<uintptr_t>(d_state) % 16 != 0) return fail(HEOM_E_ARG, "d_state must be 16-byte aligned");
     // the static scratch holds the three buffers of the time-independent
@@ -1906,6 +2012,49 @@ void group_classes(const heom_instance_desc* descs, int32_t count, std::vector<s
     g_last_error.clear();
 }
 
+// the ensemble's classes: every class of group_classes, split for N <= 8 into
+// its instances of one depth that are at least kLockstepMin many (a lockstep
+// class each) and the rest (one batch handle of mixed depths)
+constexpr size_t kLockstepMin = 8;
+struct ClassPlan {
+    std::vector<int32_t> members;
+    bool lockstep = false;
+};
+
+std::vector<ClassPlan> plan_classes(const heom_instance_desc* descs, int32_t count, bool lockstep)
+{
+    std::vector<std::vector<int32_t>> groups;
+    group_classes(descs, count, groups);
+    std::vector<ClassPlan> plan;
+    for (auto& g : groups) {
+        if (!lockstep || descs[g[0]].states > 8) {
+            plan.push_back({g, false});
+            continue;
+        }
+        std::vector<std::pair<int64_t, std::vector<int32_t>>> by_size;
+        for (int32_t k : g) {
+            bool placed = false;
+            for (auto& b : by_size)
+                if (b.first == descs[k].matrices && descs[b.second[0]].ado_depth == descs[k].ado_depth) {
+                    b.second.push_back(k);
+                    placed = true;
+                    break;
+                }
+            if (!placed) by_size.push_back({descs[k].matrices, {k}});
+        }
+        std::vector<int32_t> rest;
+        for (auto& b : by_size) {
+            if (b.second.size() >= kLockstepMin) plan.push_back({b.second, true});
+            else rest.insert(rest.end(), b.second.begin(), b.second.end());
+        }
+        if (!rest.empty()) {
+            std::sort(rest.begin(), rest.end());
+            plan.push_back({rest, false});
+        }
+    }
+    return plan;
+}
+
 // device bytes of one batch handle of these instances
 size_t class_footprint(const heom_instance_desc* descs, const std::vector<int32_t>& members, int scheme)
 {
@@ -1914,7 +2063,9 @@ size_t class_footprint(const heom_instance_desc* descs, const std::vector<int32_
     for (int32_t k : members) nodes += descs[k].matrices;
     const int P = heomk::pairs_of(d.states);
     const int W = d.ado_width;
-    const size_t state = (size_t)nodes * P * 32;
+    size_t state = (size_t)nodes * P * 32;
+    if (members.size() >= kLockstepMin && d.states <= 8) // a lockstep class pads to 32 instances
+        state = state / members.size() * ((members.size() + 31) / 32 * 32);
     const int buffers = 1 + (scheme == HEOM_RK4_REFERENCE ? 5 : 2);
     const size_t per_ado = (size_t)((2 * W + 3) & ~3) * 4 + ((W + 15) & ~15) + 16 + 8 + (members.size() > 1 ? 4 : 0);
     const size_t nn16 = (size_t)d.states * d.states * 16;
@@ -2176,10 +2327,9 @@ int heom_ensemble_footprint(const heom_instance_desc* descs, int32_t count, cons
     heom_options o;
     heom_default_options(&o);
     if (opt) o = *opt;
-    std::vector<std::vector<int32_t>> groups;
-    group_classes(descs, count, groups);
     size_t total = 0;
-    for (auto& g : groups) total += class_footprint(descs, g, o.rk4_scheme);
+    for (auto& c : plan_classes(descs, count, o.rk4_scheme == HEOM_RK4_PRODUCT || o.rk4_scheme == HEOM_RK4_HORNER))
+        total += class_footprint(descs, c.members, o.rk4_scheme);
     *bytes = total;
     return 0;
 }
@@ -2202,20 +2352,23 @@ int heom_ensemble_create(const heom_instance_desc* descs, int32_t count, const h
                     free_b / 1e9);
     CUDA_TRY(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
     CUDA_TRY(cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
-    std::vector<std::vector<int32_t>> groups;
-    group_classes(descs, count, groups);
+    const std::vector<ClassPlan> plan =
+        plan_classes(descs, count, e->opt.rk4_scheme == HEOM_RK4_PRODUCT || e->opt.rk4_scheme == HEOM_RK4_HORNER);
     e->cls_of.assign(count, 0);
     e->idx_of.assign(count, 0);
-    for (size_t c = 0; c < groups.size(); ++c) {
+    for (size_t c = 0; c < plan.size(); ++c) {
+        const std::vector<int32_t>& g = plan[c].members;
         std::vector<heom_instance_desc> members;
-        for (size_t i = 0; i < groups[c].size(); ++i) {
-            members.push_back(descs[groups[c][i]]);
-            e->cls_of[groups[c][i]] = (int32_t)c;
-            e->idx_of[groups[c][i]] = (int32_t)i;
+        for (size_t i = 0; i < g.size(); ++i) {
+            members.push_back(descs[g[i]]);
+            e->cls_of[g[i]] = (int32_t)c;
+            e->idx_of[g[i]] = (int32_t)i;
         }
         heom_handle* h = nullptr;
         if (int rc = heom_create_batch(members.data(), (int32_t)members.size(), &e->opt, &h))
             return fail(rc, "class %zu: %s", c, g_last_error.c_str());
+        // instances of one hierarchy graph: the lockstep layout when its kernel applies
+        if (plan[c].lockstep && make_lockstep(h) != 0) g_last_error.clear();
         e->cls.push_back(h);
         cudaEvent_t ev = nullptr;
         CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
@@ -2333,7 +2486,7 @@ int heom_ensemble_propagate(heom_ensemble* e, double dt, int64_t steps, int64_t 
     auto record = [&](int64_t row) -> int {
         for (heom_handle* h : e->cls) {
             heomk::heom_record_top<<<h->n_inst, 128, 0, e->stream>>>(h->toplog.p, h->y.data.p, h->d_pair.p,
-                                                                     h->d_top.p, h->N, h->P, row);
+                                                                     h->d_top.p, h->N, h->P, row, h->kp, 0);
             h->launches++;
             CUDA_TRY(cudaGetLastError());
         }
@@ -2923,9 +3076,10 @@ int heom_adjoint_gradient(heom_adjoint* A, const double* rho0, const double* obs
     // ---- forward: checkpoints and the observed tops ----
     CUDA_TRY(cudaMemsetAsync(h->y.data.p, 0, st * 16, h->stream));
     CUDA_TRY(cudaMemcpyAsync(h->topbuf.p, rho0, (size_t)K * NN * 16, cudaMemcpyHostToDevice, h->stream));
-    heomk::heom_write_top<<<K, 128, 0, h->stream>>>(h->y.data.p, h->topbuf.p, h->d_pair.p, h->d_top.p, N, h->P);
+    heomk::heom_write_top<<<K, 128, 0, h->stream>>>(h->y.data.p, h->topbuf.p, h->d_pair.p, h->d_top.p, N, h->P, 0, 0);
     h->launches++;
-    heomk::heom_record_top<<<K, 128, 0, h->stream>>>(A->toplog.p, h->y.data.p, h->d_pair.p, h->d_top.p, N, h->P, 0);
+    heomk::heom_record_top<<<K, 128, 0, h->stream>>>(A->toplog.p, h->y.data.p, h->d_pair.p, h->d_top.p, N, h->P, 0, 0,
+                                                     0);
     h->launches++;
     CUDA_TRY(cudaGetLastError());
     std::vector<int64_t> bases;
@@ -2984,7 +3138,7 @@ int heom_adjoint_gradient(heom_adjoint* A, const double* rho0, const double* obs
     std::vector<double> part((size_t)A->grid * (NN + 2) * 2);
     CUDA_TRY(cudaMemcpyAsync(part.data(), A->partial.p, part.size() * 8, cudaMemcpyDeviceToHost, h->stream));
     std::vector<double> g0top((size_t)K * NN * 2);
-    heomk::heom_record_top<<<K, 128, 0, h->stream>>>(h->topbuf.p, gcur, h->d_pair.p, h->d_top.p, N, h->P, 0);
+    heomk::heom_record_top<<<K, 128, 0, h->stream>>>(h->topbuf.p, gcur, h->d_pair.p, h->d_top.p, N, h->P, 0, 0, 0);
     h->launches++;
     CUDA_TRY(cudaMemcpyAsync(g0top.data(), h->topbuf.p, g0top.size() * 8, cudaMemcpyDeviceToHost, h->stream));
     CUDA_TRY(cudaStreamSynchronize(h->stream));

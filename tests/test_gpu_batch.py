@@ -136,3 +136,45 @@ def test_ensemble_rejects_footprint_beyond_device_memory():
     with pytest.raises(hb.HeomError) as e:
         hb.Ensemble([t] * 20000)  # rejected at admission, before any allocation
     assert "heom error -3" in str(e.value) and "GB of device memory" in str(e.value)
+
+
+@pytest.mark.parametrize("n,m,depth,count,complex_h", [(7, 1, 4, 40, False), (8, 2, 3, 33, False),
+                                                       (6, 2, 3, 12, True), (4, 1, 5, 64, False),
+                                                       (5, 3, 2, 9, False), (3, 4, 2, 8, True)])
+def test_ensemble_lockstep_class_bitwise_equal_to_single_instances(n, m, depth, count, complex_h):
+    """An ensemble class of 8 or more instances of one depth (the realisations
+    of a static-disorder ensemble) runs in the lockstep layout (instance-minor
+    state, one warp per sector with a lane per instance): every instance bit
+    for bit as when propagated alone, and the oracle's populations; instance
+    counts that are not a multiple of 32 leave padding lanes idle."""
+    probs = disorder_problems(count, n, [depth], m, seed=60 + n, complex_h=complex_h)
+    with hb.Ensemble([hb.Heom.tables_of(p) for p in probs]) as E:
+        assert E.classes() == 1
+        E.clear()
+        for k in range(count):
+            E.set_top(k, top0(n))
+        tops = E.propagate(DT, 40, 10)
+        assert np.array_equal(E.get_top(count - 1), tops[count - 1][-1])
+        # a lockstep class refuses the calls that read or write its state in another layout
+        cls = hb.lib().heom_ensemble_class(E.h, 0)
+        y = np.zeros(sum(int(hb.Heom.tables_of(p)["matrices"]) for p in probs) * n * n * 2)
+        assert hb.lib().heom_set_state(cls, y.ctypes.data) == -5
+    for k in sorted({0, 1, count // 2, count - 1}):
+        assert np.array_equal(tops[k], alone(probs[k], 40, 10)), f"instance {k}"
+    for k in (0, count - 1):
+        _, ref = ho.propagate(probs[k], DT, 40, 10)
+        assert_pops(tops[k][:, [(n + 1) * 2 * i for i in range(n)]], ref)
+
+
+def test_ensemble_splits_a_class_into_lockstep_and_mixed_depths():
+    """Ten instances of depth 3 form a lockstep class; three of depth 4 of the
+    same states and baths stay one batch handle."""
+    probs = disorder_problems(10, 7, [3], 1, seed=71) + disorder_problems(3, 7, [4], 1, seed=72)
+    with hb.Ensemble([hb.Heom.tables_of(p) for p in probs]) as E:
+        assert E.classes() == 2
+        E.clear()
+        for k in range(13):
+            E.set_top(k, top0(7))
+        tops = E.propagate(DT, 30, 10)
+    for k in (0, 9, 10, 12):
+        assert np.array_equal(tops[k], alone(probs[k], 30, 10)), f"instance {k}"
