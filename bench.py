@@ -181,7 +181,7 @@ def profiled_traffic():
     """Per-launch DRAM bytes of the benchmark stage kernel from the committed ncu
     summary, used only when the summary was taken on this build of the kernel
     (its kernel_source_hash line matches); otherwise None."""
-    path = os.path.join(ROOT, "profiles", "heom_stage_cfg2.md")
+    path = os.path.join(ROOT, "profiles", "heom_dmma_stage_n8_depth8.md")
     traffic, src = None, None
     try:
         for line in open(path):
@@ -194,7 +194,7 @@ def profiled_traffic():
         return None, "no profile summary"
     if traffic is None or src != kernel_source_hash():
         return None, "profile summary taken on another build of the kernel"
-    return traffic, "ncu dram__bytes_read.sum + dram__bytes_write.sum of this build (profiles/heom_stage_cfg2.md)"
+    return traffic, "ncu dram__bytes_read.sum + dram__bytes_write.sum of this build (profiles/heom_dmma_stage_n8_depth8.md)"
 
 
 def cpu_reference_sample(steps_cap=1):

@@ -557,7 +557,7 @@ int resolve_stage(heom_handle* h, const void** fn_out, int* blocks_out = nullptr
     int threads = 0;
     if (h->kp) {
         if (adj) return fail(HEOM_E_UNSUPPORTED, "the lockstep layout has no adjoint stage");
-        fn = (const void*)pick_lock(h->N, h->hkind, h->SLT);
+        fn = (const void*)pick_lock(h->N, h->hkind, h->SL); // its own slot count: 1, 2 or 4 slots per site
         smem = heomk::lockstep_smem_bytes(h->P, h->W, h->NW, h->TWB, h->LS);
         threads = heomk::kLockWarps * 32;
     } else if (h->N <= 8) {
@@ -1128,7 +1128,7 @@ int from_internal(heom_handle* h, double* host, const double2* src)
 // entry points that read or write the state in another layout refuse them.
 int make_lockstep(heom_handle* h)
 {
-    if (h->N > 8 || h->n_inst < 2 || h->SLT > 4 || h->compact || h->field_on)
+    if (h->N > 8 || h->n_inst < 2 || h->SL > 4 || h->compact || h->field_on)
         return fail(HEOM_E_UNSUPPORTED, "lockstep layout: needs 2+ instances of at most 8 states");
     const int64_t n0 = h->inst_base[1] - h->inst_base[0];
     for (int k = 0; k < h->n_inst; ++k)
