@@ -42,7 +42,7 @@ struct __align__(16) LockSector {
 __host__ __device__ inline int lock_row_bytes(int NW, int TWB) { return ((NW * 4 + 15) & ~15) + ((TWB + 15) & ~15) + 16; }
 __host__ inline size_t lockstep_smem_bytes(int P, int W, int NW, int TWB, int LS)
 {
-    return (size_t)dmma_lut_bytes(W, LS) + 3 * (size_t)P * 32 * 32 /* two tiles, the commutator tile */ +
+    return (size_t)dmma_lut_bytes(W, LS) + 2 * (size_t)P * 32 * 32 /* two tiles */ + 32 * 32 * 32 /* commutators */ +
            (size_t)kLockWarps * 64 * 16 + 32 * sizeof(LockSector) + 32 * sizeof(LockSlot) +
            2 * (size_t)lock_row_bytes(NW, TWB);
 }
@@ -77,9 +77,9 @@ __global__ void __launch_bounds__(kLockWarps * 32, 2) heom_lockstep_stage(const 
         s_sq[q] = make_double2(lp.ct.sq[q], q < LS ? lp.ct.sq[q + 1] : 0.0);
     unsigned char* base = smem + dmma_lut_bytes(W, LS);
     double2* tiles = reinterpret_cast<double2*>(base);      // [2][P][32] sectors (2 double2 each)
-    double2* ctile = tiles + 2 * 2 * P * 32;                 // [P][32] commutator values
-    double2* xch = ctile + 2 * P * 32 + (threadIdx.x >> 5) * 64;
-    LockSector* sectors = reinterpret_cast<LockSector*>(ctile + 2 * P * 32 + kLockWarps * 64);
+    double2* ctile = tiles + 2 * 2 * P * 32;                 // [32][32] commutator values (rows >= P unused)
+    double2* xch = ctile + 2 * 32 * 32 + (threadIdx.x >> 5) * 64;
+    LockSector* sectors = reinterpret_cast<LockSector*>(ctile + 2 * 32 * 32 + kLockWarps * 64);
     LockSlot* slots = reinterpret_cast<LockSlot*>(sectors + 32);
     unsigned char* rows0 = reinterpret_cast<unsigned char*>(slots + 32);
     const int rowb = lock_row_bytes(p.NW, p.TWB);
@@ -122,6 +122,20 @@ __global__ void __launch_bounds__(kLockWarps * 32, 2) heom_lockstep_stage(const 
     const int r = lane >> 2, t = lane & 3;
     const int xr1 = 8 * ai1 + (aj1 ^ swz(ai1)), xr2 = 8 * ai2 + (aj2 ^ swz(ai2));
     const int xw0 = 8 * r + ((2 * t) ^ swz(r)), xw1 = 8 * r + ((2 * t + 1) ^ swz(r));
+    // Phase A offsets (double2, from a tile buffer) of this lane's operands for the warp's first
+    // instance; its instance warp + 8 j adds 16 j, since the column swizzle k ^ (p & 3) changes
+    // bits 0-1 of k only. An operand outside the N x N block reads an arbitrary finite tile value
+    // (sector 0): its partner fragment of H is zero, so it adds only zeros, to rows and columns
+    // that are not read.
+    int oa[2], ob[2];
+#pragma unroll
+    for (int s = 0; s < 2; ++s) {
+        const int fs = s == 0 ? fs0 : fs1, ha = s == 0 ? ha0 : ha1;
+        const int row = fs >= 0 ? (fs * 32 + (warp ^ (fs & 3))) * 2 : 0;
+        oa[s] = fs >= 0 ? row + ha : 0;
+        ob[s] = fs >= 0 ? (r == 4 * s + t ? row + ha : row + (ha ^ 1)) : 0; // diagonal: its own transpose
+    }
+    const int oc = (lane * 32 + (warp ^ (lane & 3))) * 2; // this lane's commutator row (lanes >= P: unused rows)
     // the slot of site (lane / SLT) that lane of the table warp resolves
     const int tsite = lane / SLT, tq = lane - tsite * SLT;
     const int tsl = (warp == TW && tsite < N && tq < SL) ? __ldg(p.slots + tsite * SL + tq) : -1;
@@ -200,8 +214,6 @@ __global__ void __launch_bounds__(kLockWarps * 32, 2) heom_lockstep_stage(const 
             }
 #pragma unroll
             for (int j = 0; j < IPW; ++j) {
-                const int kk = warp + kLockWarps * j;
-                if (kb * 32 + kk >= lp.K) continue; // warp-uniform
                 double hb_r[2], hb_i[2], ha_r[2], ha_i[2];
 #pragma unroll
                 for (int s = 0; s < 2; ++s) {
@@ -219,14 +231,7 @@ __global__ void __launch_bounds__(kLockWarps * 32, 2) heom_lockstep_stage(const 
                 double cr0 = 0.0, cr1 = 0.0, ci0 = 0.0, ci1 = 0.0;
 #pragma unroll
                 for (int s = 0; s < 2; ++s) {
-                    const int fs = s == 0 ? fs0 : fs1;
-                    const int ha = s == 0 ? ha0 : ha1;
-                    double2 A = make_double2(0.0, 0.0), B = A;
-                    if (fs >= 0) {
-                        const double2* sec = tile + (fs * 32 + (kk ^ (fs & 3))) * 2;
-                        A = sec[ha];
-                        B = (r == 4 * s + t) ? A : sec[ha ^ 1];
-                    }
+                    const double2 A = tile[oa[s] + 16 * j], B = tile[ob[s] + 16 * j];
                     dmma(cr0, cr1, A.x, hb_r[s]);
                     dmma(ci0, ci1, A.y, hb_r[s]);
                     dmma(cr0, cr1, ha_r[s], B.x);
@@ -241,11 +246,8 @@ __global__ void __launch_bounds__(kLockWarps * 32, 2) heom_lockstep_stage(const 
                 xch[xw0] = make_double2(cr0, ci0);
                 xch[xw1] = make_double2(cr1, ci1);
                 __syncwarp();
-                if (owner) {
-                    double2* dst = ctile + (lane * 32 + (kk ^ (lane & 3))) * 2;
-                    dst[0] = xch[xr1];
-                    dst[1] = xch[xr2];
-                }
+                ctile[oc + 16 * j] = xch[xr1];
+                ctile[oc + 16 * j + 1] = xch[xr2];
                 __syncwarp();
             }
         }
