@@ -127,22 +127,29 @@ __global__ void __launch_bounds__(kLockWarps * 32, 2) heom_lockstep_stage(const 
     // bits 0-1 of k only. An operand outside the N x N block reads an arbitrary finite tile value
     // (sector 0): its partner fragment of H is zero, so it adds only zeros, to rows and columns
     // that are not read.
+    // Shared tiles store half h of instance column k at position h ^ ((k >> 2) & 1): a warp's
+    // 16-byte accesses to one half of 32 columns then cover all eight 16-byte bank groups.
+    const int hw = (warp >> 2) & 1; // (k >> 2) & 1 of the warp's phase A instances
     int oa[2], ob[2];
 #pragma unroll
     for (int s = 0; s < 2; ++s) {
         const int fs = s == 0 ? fs0 : fs1, ha = s == 0 ? ha0 : ha1;
         const int row = fs >= 0 ? (fs * 32 + (warp ^ (fs & 3))) * 2 : 0;
-        oa[s] = fs >= 0 ? row + ha : 0;
-        ob[s] = fs >= 0 ? (r == 4 * s + t ? row + ha : row + (ha ^ 1)) : 0; // diagonal: its own transpose
+        oa[s] = fs >= 0 ? row + (ha ^ hw) : 0;
+        ob[s] = fs >= 0 ? (r == 4 * s + t ? row + (ha ^ hw) : row + (ha ^ 1 ^ hw)) : 0; // diagonal: its own transpose
     }
     const int oc = (lane * 32 + (warp ^ (lane & 3))) * 2; // this lane's commutator row (lanes >= P: unused rows)
+    // its two commutator stores: first position (lane >> 2) & 1, whichever half lives there
+    const int cpa = (lane >> 2) & 1;
+    const int xra = (cpa ^ hw) == 0 ? xr1 : xr2, xrb = (cpa ^ hw) == 0 ? xr2 : xr1;
+    const int hk = (lane >> 2) & 1; // phase B: position of half 0 of this lane's instance
     // the slot of site (lane / SLT) that lane of the table warp resolves
     const int tsite = lane / SLT, tq = lane - tsite * SLT;
     const int tsl = (warp == TW && tsite < N && tq < SL) ? __ldg(p.slots + tsite * SL + tq) : -1;
     const int tpos = tsl >= 0 ? lp.ct.pos[tsl] : 0;
     // this thread's 16-byte pieces of a tile copy: sectors pp0, pp0 + 4, ... of instance column pk
     const int pp0 = threadIdx.x >> 6, pk = (threadIdx.x >> 1) & 31, ph = threadIdx.x & 1;
-    const int dst0 = (pp0 * 32 + (pk ^ (pp0 & 3))) * 2 + ph;
+    const int dst0 = (pp0 * 32 + (pk ^ (pp0 & 3))) * 2 + (ph ^ ((pk >> 2) & 1));
     const int64_t src0 = ((int64_t)pp0 * Kp + pk) * 2 + ph + (int64_t)kb * 64;
 
     // asynchronous copies of ADO u's tiles (this block's 32 instances) and rows into buffer b
@@ -246,8 +253,8 @@ __global__ void __launch_bounds__(kLockWarps * 32, 2) heom_lockstep_stage(const 
                 xch[xw0] = make_double2(cr0, ci0);
                 xch[xw1] = make_double2(cr1, ci1);
                 __syncwarp();
-                ctile[oc + 16 * j] = xch[xr1];
-                ctile[oc + 16 * j + 1] = xch[xr2];
+                ctile[oc + 16 * j + cpa] = xch[xra];
+                ctile[oc + 16 * j + (cpa ^ 1)] = xch[xrb];
                 __syncwarp();
             }
         }
@@ -280,9 +287,9 @@ __global__ void __launch_bounds__(kLockWarps * 32, 2) heom_lockstep_stage(const 
                     ld256_cg_if(p.y != nullptr, p.y + off, x1, x2);
                     ld256_cg_if(read_acc, p.acc + off, a1, a2);
                     const int col = (ps * 32 + (lane ^ (ps & 3))) * 2;
-                    s1 = tile[col];
-                    s2 = tile[col + 1];
-                    const double2 c1 = ctile[col], c2 = ctile[col + 1];
+                    s1 = tile[col + hk];
+                    s2 = tile[col + (hk ^ 1)];
+                    const double2 c1 = ctile[col + hk], c2 = ctile[col + (hk ^ 1)];
                     L1 = make_double2(-c1.y, c1.x); // i * (w H - H w) / hbar
                     L2 = make_double2(-c2.y, c2.x);
                     cmac(L1, make_double2(pss.x + sc.g1.x, pss.y + sc.g1.y), s1);
