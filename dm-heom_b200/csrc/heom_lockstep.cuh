@@ -47,6 +47,18 @@ __host__ inline size_t lockstep_smem_bytes(int P, int W, int NW, int TWB, int LS
            2 * (size_t)lock_row_bytes(NW, TWB);
 }
 
+// as ld256_cg_if, but schedulable: the stage kernel stores to the same address only values
+// computed from the loaded ones, which orders the load first
+__device__ __forceinline__ void ld256_co_if(bool ok, const double2* src, double2& a, double2& b)
+{
+    asm("{\n .reg .pred q;\n setp.ne.u32 q, %5, 0;\n"
+        " mov.f64 %0, 0d0000000000000000;\n mov.f64 %1, 0d0000000000000000;\n"
+        " mov.f64 %2, 0d0000000000000000;\n mov.f64 %3, 0d0000000000000000;\n"
+        " @q ld.global.v4.f64 {%0,%1,%2,%3}, [%4];\n}\n"
+        : "=d"(a.x), "=d"(a.y), "=d"(b.x), "=d"(b.y)
+        : "l"(src), "r"((unsigned)ok));
+}
+
 // Two CTAs of 8 warps per SM. CTA b keeps the instance block b % (Kp / 32)
 // and sweeps the ADOs u = b / (Kp / 32), + gridDim / (Kp / 32), ...; the next
 // ADO's tiles and rows are copied (cp.async) while the current one runs.
@@ -284,8 +296,8 @@ __global__ void __launch_bounds__(kLockWarps * 32, 2) heom_lockstep_stage(const 
                     }
                 }
                 if (sd0 == 0) {
-                    ld256_cg_if(p.y != nullptr, p.y + off, x1, x2);
-                    ld256_cg_if(read_acc, p.acc + off, a1, a2);
+                    ld256_co_if(p.y != nullptr, p.y + off, x1, x2);
+                    ld256_co_if(read_acc, p.acc + off, a1, a2);
                     const int col = (ps * 32 + (lane ^ (ps & 3))) * 2;
                     s1 = tile[col + hk];
                     s2 = tile[col + (hk ^ 1)];
