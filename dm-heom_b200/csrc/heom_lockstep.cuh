@@ -29,7 +29,7 @@ struct LockParams {
 constexpr int kLockWarps = 8;
 // one slot of one site at the current ADO: its neighbour rows and coefficients
 struct __align__(16) LockSlot {
-    int64_t op, om;   // offsets (double2) of the rows of ADO n + e (plus) and n - e (minus); -1: absent
+    int64_t op, om;   // byte offsets of the rows of ADO n + e (plus) and n - e (minus); -1: absent
     double c, sm;     // plus-side coefficient chat * sqrt(n + 1), minus-side scale sqrt(n)
     double2 kap[3];   // the three kappa-hat values of the slot's mode
     int present, pad[3];
@@ -47,16 +47,33 @@ __host__ inline size_t lockstep_smem_bytes(int P, int W, int NW, int TWB, int LS
            2 * (size_t)lock_row_bytes(NW, TWB);
 }
 
-// as ld256_cg_if, but schedulable: the stage kernel stores to the same address only values
-// computed from the loaded ones, which orders the load first
-__device__ __forceinline__ void ld256_co_if(bool ok, const double2* src, double2& a, double2& b)
+// 32 bytes at base + off (bytes) when off >= 0, zeros otherwise: the test, the address and the
+// load in one asm block
+__device__ __forceinline__ void ld256_at(const double2* base, int64_t off, double2& a, double2& b)
 {
-    asm("{\n .reg .pred q;\n setp.ne.u32 q, %5, 0;\n"
+    asm("{\n .reg .pred q;\n .reg .b64 ad;\n setp.ge.s64 q, %5, 0;\n add.s64 ad, %4, %5;\n"
         " mov.f64 %0, 0d0000000000000000;\n mov.f64 %1, 0d0000000000000000;\n"
         " mov.f64 %2, 0d0000000000000000;\n mov.f64 %3, 0d0000000000000000;\n"
-        " @q ld.global.v4.f64 {%0,%1,%2,%3}, [%4];\n}\n"
+        " @q ld.global.nc.v4.f64 {%0,%1,%2,%3}, [ad];\n}\n"
         : "=d"(a.x), "=d"(a.y), "=d"(b.x), "=d"(b.y)
-        : "l"(src), "r"((unsigned)ok));
+        : "l"(base), "l"(off));
+}
+// as ld256_at, and only when skip == 0
+__device__ __forceinline__ void ld256_at_unless(const double2* base, int64_t off, unsigned skip, double2& a, double2& b)
+{
+    asm("{\n .reg .pred q;\n .reg .b64 ad;\n setp.ge.s64 q, %5, 0;\n setp.eq.and.u32 q, %6, 0, q;\n"
+        " add.s64 ad, %4, %5;\n"
+        " mov.f64 %0, 0d0000000000000000;\n mov.f64 %1, 0d0000000000000000;\n"
+        " mov.f64 %2, 0d0000000000000000;\n mov.f64 %3, 0d0000000000000000;\n"
+        " @q ld.global.nc.v4.f64 {%0,%1,%2,%3}, [ad];\n}\n"
+        : "=d"(a.x), "=d"(a.y), "=d"(b.x), "=d"(b.y)
+        : "l"(base), "l"(off), "r"(skip));
+}
+// 32 bytes through the coherent path, schedulable: the stage kernel stores to the same address only
+// values computed from the loaded ones, which orders the load first
+__device__ __forceinline__ void ld256_co(const double2* src, double2& a, double2& b)
+{
+    asm("ld.global.v4.f64 {%0,%1,%2,%3}, [%4];\n" : "=d"(a.x), "=d"(a.y), "=d"(b.x), "=d"(b.y) : "l"(src));
 }
 
 // Two CTAs of 8 warps per SM. CTA b keeps the instance block b % (Kp / 32)
@@ -200,8 +217,8 @@ __global__ void __launch_bounds__(kLockWarps * 32, 2) heom_lockstep_stage(const 
             if (tsl >= 0) {
                 const int2 pm = reinterpret_cast<const int2*>(rows)[tsl];
                 const double2 sqp = s_sq[tu[tsl]];
-                e.op = pm.x >= 0 ? pm.x * PK2 : -1;
-                e.om = pm.y >= 0 ? pm.y * PK2 : -1;
+                e.op = pm.x >= 0 ? pm.x * PK2 * 16 : -1;
+                e.om = pm.y >= 0 ? pm.y * PK2 * 16 : -1;
                 e.present = 1;
                 e.c = s_ch[tpos] * sqp.y;
                 e.sm = sqp.x;
@@ -291,13 +308,13 @@ __global__ void __launch_bounds__(kLockWarps * 32, 2) heom_lockstep_stage(const 
 #pragma unroll
                     for (int q = 0; q < SLT; ++q) {
                         const longlong2 o = *reinterpret_cast<const longlong2*>(&es[q].op);
-                        ld256_if(!diag && o.x >= 0, in_l + o.x, xp[b][q][0], xp[b][q][1]);
-                        ld256_if(o.y >= 0, in_l + o.y, xm[b][q][0], xm[b][q][1]);
+                        ld256_at_unless(in_l, o.x, sc.diag, xp[b][q][0], xp[b][q][1]);
+                        ld256_at(in_l, o.y, xm[b][q][0], xm[b][q][1]);
                     }
                 }
                 if (sd0 == 0) {
-                    ld256_co_if(p.y != nullptr, p.y + off, x1, x2);
-                    ld256_co_if(read_acc, p.acc + off, a1, a2);
+                    if (p.y) ld256_co(p.y + off, x1, x2); // kernel parameters: uniform branches
+                    if (read_acc) ld256_co(p.acc + off, a1, a2);
                     const int col = (ps * 32 + (lane ^ (ps & 3))) * 2;
                     s1 = tile[col + hk];
                     s2 = tile[col + (hk ^ 1)];
