@@ -2056,7 +2056,7 @@ std::vector<ClassPlan> plan_classes(const heom_instance_desc* descs, int32_t cou
 }
 
 // device bytes of one batch handle of these instances
-size_t class_footprint(const heom_instance_desc* descs, const std::vector<int32_t>& members, int scheme)
+size_t class_footprint(const heom_instance_desc* descs, const std::vector<int32_t>& members, int scheme, bool lockstep)
 {
     const heom_instance_desc& d = descs[members[0]];
     int64_t nodes = 0;
@@ -2064,7 +2064,7 @@ size_t class_footprint(const heom_instance_desc* descs, const std::vector<int32_
     const int P = heomk::pairs_of(d.states);
     const int W = d.ado_width;
     size_t state = (size_t)nodes * P * 32;
-    if (members.size() >= kLockstepMin && d.states <= 8) // a lockstep class pads to 32 instances
+    if (lockstep) // a lockstep class pads to 32 instances
         state = state / members.size() * ((members.size() + 31) / 32 * 32);
     const int buffers = 1 + (scheme == HEOM_RK4_REFERENCE ? 5 : 2);
     const size_t per_ado = (size_t)((2 * W + 3) & ~3) * 4 + ((W + 15) & ~15) + 16 + 8 + (members.size() > 1 ? 4 : 0);
@@ -2329,7 +2329,7 @@ int heom_ensemble_footprint(const heom_instance_desc* descs, int32_t count, cons
     if (opt) o = *opt;
     size_t total = 0;
     for (auto& c : plan_classes(descs, count, o.rk4_scheme == HEOM_RK4_PRODUCT || o.rk4_scheme == HEOM_RK4_HORNER))
-        total += class_footprint(descs, c.members, o.rk4_scheme);
+        total += class_footprint(descs, c.members, o.rk4_scheme, c.lockstep);
     *bytes = total;
     return 0;
 }

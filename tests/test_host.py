@@ -245,6 +245,19 @@ def test_ensemble_footprint_groups_classes():
     assert hb.Ensemble.footprint([t3], scheme="reference") > one3
 
 
+def test_ensemble_footprint_pads_lockstep_classes():
+    # 8 or more instances of one class and depth (at most 8 states) form a lockstep class whose
+    # state is padded to a multiple of 32 instances; 7 stay a batch; the reference scheme has none
+    t = hb.build_tables(hb.System(ho.synthetic_hamiltonian(4, 3), [35] * 4, [50] * 4, [0] * 4, 1, 300.0, 3))
+    state1 = int(t["matrices"]) * 8 * 32  # one instance's state: ADOs x 8 pair sectors x 32 B
+    seven, eight = hb.Ensemble.footprint([t] * 7), hb.Ensemble.footprint([t] * 8)
+    assert eight - seven >= 24 * state1 * 3  # 25 more padded instances, state + 2 stage buffers
+    # up to 32 instances the padded state is already counted: only tables and per-instance items grow
+    assert hb.Ensemble.footprint([t] * 32) - eight < 24 * state1 * 3
+    ref7, ref8 = hb.Ensemble.footprint([t] * 7, scheme="reference"), hb.Ensemble.footprint([t] * 8, scheme="reference")
+    assert ref8 - ref7 < 2 * state1 * 6
+
+
 def test_batch_admission_rejects_mixed_classes():
     t3 = hb.build_tables(hb.System(ho.synthetic_hamiltonian(3, 2), [35] * 3, [50] * 3, [0] * 3, 1, 300.0, 2))
     t3l = hb.build_tables(hb.System(ho.synthetic_hamiltonian(3, 2), [40] * 3, [50] * 3, [0] * 3, 1, 300.0, 2))
