@@ -249,42 +249,51 @@ __global__ void __launch_bounds__(kLockWarps * 32, 2) heom_lockstep_stage(const 
                 }
             }
 #pragma unroll
-            for (int j = 0; j < IPW; ++j) {
-                double hb_r[2], hb_i[2], ha_r[2], ha_i[2];
+            for (int j0 = 0; j0 < IPW; j0 += 2) {
+                double cr[2][2], ci[2][2]; // the two instances' accumulators
 #pragma unroll
-                for (int s = 0; s < 2; ++s) {
-                    if (HK == H_GENERIC) {
-                        hb_r[s] = gf[HK == H_GENERIC ? j : 0][s][0];
-                        hb_i[s] = gf[HK == H_GENERIC ? j : 0][s][1];
-                        ha_r[s] = gf[HK == H_GENERIC ? j : 0][s][2];
-                        ha_i[s] = gf[HK == H_GENERIC ? j : 0][s][3];
-                    } else {
-                        hb_r[s] = hbk[j][s];
-                        ha_r[s] = -hbk[j][s]; // -H(r, c) = -H(c, r): H is real symmetric
-                        hb_i[s] = ha_i[s] = 0.0;
+                for (int jj = 0; jj < 2; ++jj) {
+                    const int j = j0 + jj;
+                    double hb_r[2], hb_i[2], ha_r[2], ha_i[2];
+#pragma unroll
+                    for (int s = 0; s < 2; ++s) {
+                        if (HK == H_GENERIC) {
+                            hb_r[s] = gf[HK == H_GENERIC ? j : 0][s][0];
+                            hb_i[s] = gf[HK == H_GENERIC ? j : 0][s][1];
+                            ha_r[s] = gf[HK == H_GENERIC ? j : 0][s][2];
+                            ha_i[s] = gf[HK == H_GENERIC ? j : 0][s][3];
+                        } else {
+                            hb_r[s] = hbk[j][s];
+                            ha_r[s] = -hbk[j][s]; // -H(r, c) = -H(c, r): H is real symmetric
+                            hb_i[s] = ha_i[s] = 0.0;
+                        }
+                    }
+                    cr[jj][0] = cr[jj][1] = ci[jj][0] = ci[jj][1] = 0.0;
+#pragma unroll
+                    for (int s = 0; s < 2; ++s) {
+                        const double2 A = tile[oa[s] + 16 * j], B = tile[ob[s] + 16 * j];
+                        dmma(cr[jj][0], cr[jj][1], A.x, hb_r[s]);
+                        dmma(ci[jj][0], ci[jj][1], A.y, hb_r[s]);
+                        dmma(cr[jj][0], cr[jj][1], ha_r[s], B.x);
+                        dmma(ci[jj][0], ci[jj][1], ha_r[s], B.y);
+                        if (HK == H_GENERIC) {
+                            dmma(cr[jj][0], cr[jj][1], -A.y, hb_i[s]);
+                            dmma(ci[jj][0], ci[jj][1], A.x, hb_i[s]);
+                            dmma(cr[jj][0], cr[jj][1], -ha_i[s], B.y);
+                            dmma(ci[jj][0], ci[jj][1], ha_i[s], B.x);
+                        }
                     }
                 }
-                double cr0 = 0.0, cr1 = 0.0, ci0 = 0.0, ci1 = 0.0;
 #pragma unroll
-                for (int s = 0; s < 2; ++s) {
-                    const double2 A = tile[oa[s] + 16 * j], B = tile[ob[s] + 16 * j];
-                    dmma(cr0, cr1, A.x, hb_r[s]);
-                    dmma(ci0, ci1, A.y, hb_r[s]);
-                    dmma(cr0, cr1, ha_r[s], B.x);
-                    dmma(ci0, ci1, ha_r[s], B.y);
-                    if (HK == H_GENERIC) {
-                        dmma(cr0, cr1, -A.y, hb_i[s]);
-                        dmma(ci0, ci1, A.x, hb_i[s]);
-                        dmma(cr0, cr1, -ha_i[s], B.y);
-                        dmma(ci0, ci1, ha_i[s], B.x);
-                    }
+                for (int jj = 0; jj < 2; ++jj) {
+                    const int j = j0 + jj;
+                    xch[xw0] = make_double2(cr[jj][0], ci[jj][0]);
+                    xch[xw1] = make_double2(cr[jj][1], ci[jj][1]);
+                    __syncwarp();
+                    ctile[oc + 16 * j + cpa] = xch[xra];
+                    ctile[oc + 16 * j + (cpa ^ 1)] = xch[xrb];
+                    __syncwarp();
                 }
-                xch[xw0] = make_double2(cr0, ci0);
-                xch[xw1] = make_double2(cr1, ci1);
-                __syncwarp();
-                ctile[oc + 16 * j + cpa] = xch[xra];
-                ctile[oc + 16 * j + (cpa ^ 1)] = xch[xrb];
-                __syncwarp();
             }
         }
         __syncthreads();
