@@ -324,3 +324,18 @@ def test_instance_file_rejects_garbage(tmp_path):
     with pytest.raises(hb.HeomError) as e:
         hb.read_instance(p)
     assert "heom error -7" in str(e.value)
+
+
+def test_bench_reports_profiled_traffic_only_for_the_profiled_build(monkeypatch):
+    # roofline.traffic comes from the committed ncu summary only when the summary's
+    # kernel_source_hash line names the kernel sources being run
+    import bench
+    path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "profiles",
+                        "heom_dmma_stage_n8_depth8.md")
+    recorded = [ln.split("=")[1].strip() for ln in open(path) if ln.startswith("kernel_source_hash")][0]
+    monkeypatch.setattr(bench, "kernel_source_hash", lambda: recorded)
+    traffic, src = bench.profiled_traffic()
+    assert traffic is not None and traffic > 1.5e9 and "this build" in src
+    monkeypatch.setattr(bench, "kernel_source_hash", lambda: "0" * 16)
+    traffic, src = bench.profiled_traffic()
+    assert traffic is None and "another build" in src
