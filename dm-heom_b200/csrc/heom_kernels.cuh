@@ -254,28 +254,6 @@ __device__ __forceinline__ void ld256_cg(const double2* src, double2& a, double2
                  : "l"(src));
 }
 
-// 32 bytes when ok, zeros otherwise, without a branch (non-coherent path: data the kernel does not write)
-__device__ __forceinline__ void ld256_if(bool ok, const double2* src, double2& a, double2& b)
-{
-    asm("{\n .reg .pred q;\n setp.ne.u32 q, %5, 0;\n"
-        " mov.f64 %0, 0d0000000000000000;\n mov.f64 %1, 0d0000000000000000;\n"
-        " mov.f64 %2, 0d0000000000000000;\n mov.f64 %3, 0d0000000000000000;\n"
-        " @q ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];\n}\n"
-        : "=d"(a.x), "=d"(a.y), "=d"(b.x), "=d"(b.y)
-        : "l"(src), "r"((unsigned)ok));
-}
-
-// as ld256_if, through the coherent path (data this kernel writes afterwards)
-__device__ __forceinline__ void ld256_cg_if(bool ok, const double2* src, double2& a, double2& b)
-{
-    asm volatile("{\n .reg .pred q;\n setp.ne.u32 q, %5, 0;\n"
-                 " mov.f64 %0, 0d0000000000000000;\n mov.f64 %1, 0d0000000000000000;\n"
-                 " mov.f64 %2, 0d0000000000000000;\n mov.f64 %3, 0d0000000000000000;\n"
-                 " @q ld.global.v4.f64 {%0,%1,%2,%3}, [%4];\n}\n"
-                 : "=d"(a.x), "=d"(a.y), "=d"(b.x), "=d"(b.y)
-                 : "l"(src), "r"((unsigned)ok));
-}
-
 // 32-byte stores when ok, without a branch (streaming / default cache policy)
 __device__ __forceinline__ void st256_cs_if(bool ok, double2* dst, double2 a, double2 b)
 {
