@@ -3000,14 +3000,20 @@ int heom_adjoint_gradient(heom_adjoint* A, const double* rho0, const double* obs
     int64_t ncp = (steps + S - 1) / S;
     // device memory: the sqrt layout (checkpoints, stage inputs of one segment)
     // or, when it does not fit, recursive checkpointing in the slots that do;
-    // plus the adjoint ping-pong and one scratch state
+    // plus the adjoint ping-pong and one scratch state. The forward handle's
+    // stage buffers are allocated first, so that free memory counts them, and
+    // without a limit a slack stays free for the sweep's small buffers (top
+    // log, weights, graphs) and the allocator's granularity.
+    if (int rc = prepare_scheme(h)) return rc;
     int64_t slots = 0;
     {
         size_t free_b = 0, total_b = 0;
         CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
         const double sb = (double)st * 16.0;
         const double held = (double)(A->cap_cps + A->cap_seg + (A->ga.p ? 3 : 0)) * sb;
-        const double budget = A->mem_limit > 0 ? (double)A->mem_limit : (double)free_b + held;
+        const double slack = std::max(512.0 * 1024 * 1024, 0.02 * (double)total_b);
+        const double budget =
+            A->mem_limit > 0 ? (double)A->mem_limit : std::max(0.0, (double)free_b - slack) + held;
         if ((double)(ncp + 4 * S + 3) * sb > budget) {
             slots = std::min<int64_t>((int64_t)(budget / sb) - 7, steps);
             if (slots < 1)
