@@ -132,6 +132,7 @@ template <int N, int HK, bool MI, bool ADJ>
 dmma_fn_t pick_dslt(int slt)
 {
     switch (slt) {
+    case 1: return heomk::heom_dmma_stage<N, HK, 1, MI, ADJ>;
     case 2: return heomk::heom_dmma_stage<N, HK, 2, MI, ADJ>;
     case 4: return heomk::heom_dmma_stage<N, HK, 4, MI, ADJ>;
     default: return heomk::heom_dmma_stage<N, HK, 8, MI, ADJ>;
@@ -561,7 +562,7 @@ int resolve_stage(heom_handle* h, const void** fn_out, int* blocks_out = nullptr
         smem = heomk::lockstep_smem_bytes(h->P, h->W, h->NW, h->TWB, h->LS);
         threads = heomk::kLockWarps * 32;
     } else if (h->N <= 8) {
-        fn = (const void*)pick_dmma(h->N, h->hkind, h->SLT, h->n_inst > 1, adj);
+        fn = (const void*)pick_dmma(h->N, h->hkind, h->SL == 1 ? 1 : h->SLT, h->n_inst > 1, adj); // one slot: exact
         smem = heomk::dmma_smem_bytes(h->P, h->W, h->NW, h->TWB, h->LS);
         threads = heomk::kCtaWarps * 32;
     } else {
