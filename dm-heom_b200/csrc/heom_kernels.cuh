@@ -799,56 +799,66 @@ __global__ void __launch_bounds__(kCtaWarps * 32, SLT <= 2 ? 3 : 2) heom_pair_st
 
             // ---- neighbours: per side all loads first, then the updates ----
             // side 0 = slots of site i, side 1 = slots of site j
+            // one slot per state: both sides' neighbour rows in one batch
+            constexpr int SB = SLT == 1 ? 2 : 1;
 #pragma unroll
-            for (int sd = 0; sd < 2; ++sd) {
-                double2 xp[SLT][2], xm[SLT][2];
-                int nn[SLT];
+            for (int sd0 = 0; sd0 < 2; sd0 += SB) {
+                double2 xp[SB][SLT][2], xm[SB][SLT][2];
+                int nn[SB][SLT];
 #pragma unroll
-                for (int q = 0; q < SLT; ++q) {
-                    const int sl = sd == 0 ? sli[q] : slj[q];
-                    const int2 pm = sl >= 0 ? reinterpret_cast<const int2*>(nb)[sl] : make_int2(-1, -1);
-                    const int32_t vp = (ADJ || !diag) ? pm.x : -1;
-                    const int32_t vm = (!ADJ || !diag) ? pm.y : -1;
-                    nn[q] = sl >= 0 ? tu[sl] : 0;
-                    xp[q][0] = xp[q][1] = xm[q][0] = xm[q][1] = make_double2(0.0, 0.0);
-                    if (vp >= 0) ld256(p.in + (int64_t)vp * (2 * P) + 2 * lt, xp[q][0], xp[q][1]);
-                    if (vm >= 0) ld256(p.in + (int64_t)vm * (2 * P) + 2 * lt, xm[q][0], xm[q][1]);
+                for (int bb = 0; bb < SB; ++bb) {
+                    const int sd = sd0 + bb;
+#pragma unroll
+                    for (int q = 0; q < SLT; ++q) {
+                        const int sl = sd == 0 ? sli[q] : slj[q];
+                        const int2 pm = sl >= 0 ? reinterpret_cast<const int2*>(nb)[sl] : make_int2(-1, -1);
+                        const int32_t vp = (ADJ || !diag) ? pm.x : -1;
+                        const int32_t vm = (!ADJ || !diag) ? pm.y : -1;
+                        nn[bb][q] = sl >= 0 ? tu[sl] : 0;
+                        xp[bb][q][0] = xp[bb][q][1] = xm[bb][q][0] = xm[bb][q][1] = make_double2(0.0, 0.0);
+                        if (vp >= 0) ld256(p.in + (int64_t)vp * (2 * P) + 2 * lt, xp[bb][q][0], xp[bb][q][1]);
+                        if (vm >= 0) ld256(p.in + (int64_t)vm * (2 * P) + 2 * lt, xm[bb][q][0], xm[bb][q][1]);
+                    }
                 }
 #pragma unroll
-                for (int q = 0; q < SLT; ++q) {
-                    const int sl = sd == 0 ? sli[q] : slj[q];
-                    if (sl < 0) continue;
-                    const int ps = s_pos[sl];
-                    const double2 sqp = s_sq[nn[q]];
-                    const double sq_lo = sqp.x, sq_hi = sqp.y;
-                    // L: i chat sqrt(n+1) on the plus neighbour, khat sqrt(n) on the minus one;
-                    // L^H: -i chat sqrt(n) on the minus neighbour, conj(khat) sqrt(n+1) on the plus one
-                    const double c = diag ? 0.0 : (ADJ ? -s_ch[ps] * sq_lo : s_ch[ps] * sq_hi);
-                    const double sk = ADJ ? sq_hi : sq_lo;
-                    const double2 t1 = ADJ ? xm[q][0] : xp[q][0], t2 = ADJ ? xm[q][1] : xp[q][1];
-                    const double2 k1 = ADJ ? xp[q][0] : xm[q][0], k2 = ADJ ? xp[q][1] : xm[q][1];
-                    const double2 m1 = make_double2(k1.x * sk, k1.y * sk);
-                    const double2 m2 = make_double2(k2.x * sk, k2.y * sk);
-                    auto kap = [&](const double2* tab) {
-                        const double2 v = tab[ps];
-                        return ADJ ? make_double2(v.x, -v.y) : v;
-                    };
-                    if (sd == 0) {
-                        // site i: element 1 (i,j) i-side (+i c, kappa_i); element 2 (j,i) j-side (-i c, kappa_j)
-                        L1.x = fma(-c, t1.y, L1.x);
-                        L1.y = fma(c, t1.x, L1.y);
-                        L2.x = fma(c, t2.y, L2.x);
-                        L2.y = fma(-c, t2.x, L2.y);
-                        cmac(L1, kap(kap_i1), m1);
-                        if (!diag) cmac(L2, kap(kap_i2), m2);
-                    } else {
-                        // site j: element 1 j-side (-i c, kappa_j); element 2 i-side (+i c, kappa_i)
-                        L1.x = fma(c, t1.y, L1.x);
-                        L1.y = fma(-c, t1.x, L1.y);
-                        L2.x = fma(-c, t2.y, L2.x);
-                        L2.y = fma(c, t2.x, L2.y);
-                        if (!diag) cmac(L1, kap(kap_j1), m1);
-                        cmac(L2, kap(kap_j2), m2);
+                for (int bb = 0; bb < SB; ++bb) {
+                    const int sd = sd0 + bb;
+#pragma unroll
+                    for (int q = 0; q < SLT; ++q) {
+                        const int sl = sd == 0 ? sli[q] : slj[q];
+                        if (sl < 0) continue;
+                        const int ps = s_pos[sl];
+                        const double2 sqp = s_sq[nn[bb][q]];
+                        const double sq_lo = sqp.x, sq_hi = sqp.y;
+                        // L: i chat sqrt(n+1) on the plus neighbour, khat sqrt(n) on the minus one;
+                        // L^H: -i chat sqrt(n) on the minus neighbour, conj(khat) sqrt(n+1) on the plus one
+                        const double c = diag ? 0.0 : (ADJ ? -s_ch[ps] * sq_lo : s_ch[ps] * sq_hi);
+                        const double sk = ADJ ? sq_hi : sq_lo;
+                        const double2 t1 = ADJ ? xm[bb][q][0] : xp[bb][q][0], t2 = ADJ ? xm[bb][q][1] : xp[bb][q][1];
+                        const double2 k1 = ADJ ? xp[bb][q][0] : xm[bb][q][0], k2 = ADJ ? xp[bb][q][1] : xm[bb][q][1];
+                        const double2 m1 = make_double2(k1.x * sk, k1.y * sk);
+                        const double2 m2 = make_double2(k2.x * sk, k2.y * sk);
+                        auto kap = [&](const double2* tab) {
+                            const double2 v = tab[ps];
+                            return ADJ ? make_double2(v.x, -v.y) : v;
+                        };
+                        if (sd == 0) {
+                            // site i: element 1 (i,j) i-side (+i c, kappa_i); element 2 (j,i) j-side (-i c, kappa_j)
+                            L1.x = fma(-c, t1.y, L1.x);
+                            L1.y = fma(c, t1.x, L1.y);
+                            L2.x = fma(c, t2.y, L2.x);
+                            L2.y = fma(-c, t2.x, L2.y);
+                            cmac(L1, kap(kap_i1), m1);
+                            if (!diag) cmac(L2, kap(kap_i2), m2);
+                        } else {
+                            // site j: element 1 j-side (-i c, kappa_j); element 2 i-side (+i c, kappa_i)
+                            L1.x = fma(c, t1.y, L1.x);
+                            L1.y = fma(-c, t1.x, L1.y);
+                            L2.x = fma(-c, t2.y, L2.x);
+                            L2.y = fma(c, t2.x, L2.y);
+                            if (!diag) cmac(L1, kap(kap_j1), m1);
+                            cmac(L2, kap(kap_j2), m2);
+                        }
                     }
                 }
             }

@@ -99,6 +99,7 @@ template <int N, int HK, bool ADJ>
 stage_fn_t pick_slt(int slt)
 {
     switch (slt) {
+    case 1: return heomk::heom_pair_stage<N, HK, 1, ADJ>;
     case 2: return heomk::heom_pair_stage<N, HK, 2, ADJ>;
     case 4: return heomk::heom_pair_stage<N, HK, 4, ADJ>;
     default: return heomk::heom_pair_stage<N, HK, 8, ADJ>;
@@ -566,7 +567,7 @@ int resolve_stage(heom_handle* h, const void** fn_out, int* blocks_out = nullptr
         smem = heomk::dmma_smem_bytes(h->P, h->W, h->NW, h->TWB, h->LS);
         threads = heomk::kCtaWarps * 32;
     } else {
-        fn = (const void*)pick_stage(h->N, h->hkind, h->SLT, adj);
+        fn = (const void*)pick_stage(h->N, h->hkind, h->SL == 1 ? 1 : h->SLT, adj); // one slot: exact
         smem = heomk::pair_smem_bytes(h->N, h->W, h->NW, h->TWB, h->LS);
         threads = cta_threads(h->N);
     }
