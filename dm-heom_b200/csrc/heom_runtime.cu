@@ -1138,12 +1138,23 @@ int make_lockstep(heom_handle* h)
             return fail(HEOM_E_UNSUPPORTED, "lockstep layout: instances of different depths");
     for (uint8_t m : h->mask)
         if (!m) return fail(HEOM_E_UNSUPPORTED, "lockstep layout: masked hierarchies are not supported");
-    h->inst_nodes = n0;
-    h->kp = (h->n_inst + 31) / 32 * 32;
+    // the instance-minor state first: if it cannot be had, the handle stays the batch handle it was
+    const int64_t kp = (h->n_inst + 31) / 32 * 32;
+    const size_t elems = (size_t)n0 * kp * 2 * h->P;
+    double2* ny = nullptr;
+    if (cudaMalloc(&ny, elems * sizeof(double2)) != cudaSuccess)
+        return fail(HEOM_E_NOMEM, "lockstep layout: cudaMalloc of %zu bytes failed", elems * sizeof(double2));
     const std::vector<int64_t> tops(h->n_inst, h->top_int[0] - h->inst_base[0]);
-    CUDA_TRY(cudaMemcpy(h->d_top.p, tops.data(), tops.size() * 8, cudaMemcpyHostToDevice));
-    if (int rc = h->y.data.alloc(h->state_elems())) return rc;
-    CUDA_TRY(cudaMemset(h->y.data.p, 0, h->state_elems() * sizeof(double2)));
+    if (cudaMemset(ny, 0, elems * sizeof(double2)) != cudaSuccess ||
+        cudaMemcpy(h->d_top.p, tops.data(), tops.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(ny);
+        return fail(HEOM_E_CUDA, "lockstep layout: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    h->y.data.reset();
+    h->y.data.p = ny;
+    h->y.data.n = elems;
+    h->inst_nodes = n0;
+    h->kp = kp;
     for (auto& w : h->work) w.reset();
     for (auto& a : h->per_sm) a[0] = a[1] = 0;
     h->stage_smem = 0;
