@@ -225,6 +225,13 @@ def lib():
     return _lib
 
 
+def _need(ok, what):
+    """Array sizes are checked before a pointer goes to the library (not with
+    assert, which python -O removes)."""
+    if not ok:
+        raise ValueError(f"array size does not match the handle: {what}")
+
+
 def _check(rc):
     if rc != 0:
         msg = lib().heom_last_error().decode(errors="replace")
@@ -243,7 +250,7 @@ class Buffer:
 
     def write(self, y):
         y = np.ascontiguousarray(y, dtype=np.float64)
-        assert y.size == self.owner.state_len
+        _need(y.size == self.owner.state_len, "y.size == self.owner.state_len")
         _check(lib().heom_buffer_write(self.owner.h, self.h, _ptr(y)))
 
     def read(self):
@@ -361,7 +368,7 @@ class Heom:
     # -- state ---------------------------------------------------------------
     def set_state(self, y):
         y = np.ascontiguousarray(y, dtype=np.float64)
-        assert y.size == self.state_len
+        _need(y.size == self.state_len, "y.size == self.state_len")
         _check(lib().heom_set_state(self.h, _ptr(y)))
 
     def get_state(self):
@@ -380,7 +387,7 @@ class Heom:
 
     def set_instance_top(self, k, top):
         top = np.ascontiguousarray(top, dtype=np.float64)
-        assert top.size == self.states * self.states * 2
+        _need(top.size == self.states * self.states * 2, "top.size == self.states * self.states * 2")
         _check(lib().heom_set_instance_top(self.h, k, _ptr(top)))
 
     def get_instance_top(self, k):
@@ -390,12 +397,12 @@ class Heom:
 
     def set_hamiltonian(self, ham):
         ham = np.ascontiguousarray(ham, dtype=np.float64)
-        assert ham.size == self.instances * self.states * self.states * 2
+        _need(ham.size == self.instances * self.states * self.states * 2, "ham.size == self.instances * self.states * self.states * 2")
         _check(lib().heom_set_hamiltonian(self.h, _ptr(ham)))
 
     def set_instance_hamiltonian(self, k, ham):
         ham = np.ascontiguousarray(ham, dtype=np.float64)
-        assert ham.size == self.states * self.states * 2
+        _need(ham.size == self.states * self.states * 2, "ham.size == self.states * self.states * 2")
         _check(lib().heom_set_instance_hamiltonian(self.h, k, _ptr(ham)))
 
     def set_mask(self, mask, compact=False):
@@ -575,7 +582,7 @@ class Ensemble:
 
     def set_top(self, k, top):
         top = np.ascontiguousarray(top, dtype=np.float64)
-        assert top.size == self.states[k] ** 2 * 2
+        _need(top.size == self.states[k] ** 2 * 2, "top.size == self.states[k] ** 2 * 2")
         _check(lib().heom_ensemble_set_top(self.h, k, _ptr(top)))
 
     def get_top(self, k):
@@ -585,7 +592,7 @@ class Ensemble:
 
     def set_hamiltonian(self, k, ham):
         ham = np.ascontiguousarray(ham, dtype=np.float64)
-        assert ham.size == self.states[k] ** 2 * 2
+        _need(ham.size == self.states[k] ** 2 * 2, "ham.size == self.states[k] ** 2 * 2")
         _check(lib().heom_ensemble_set_hamiltonian(self.h, k, _ptr(ham)))
 
     def autotune(self):
@@ -719,7 +726,7 @@ class Adjoint:
         rho0 = per_instance(rho0)
         obs = per_instance(observable)
         w = np.ascontiguousarray(np.asarray(weights, np.float64))
-        assert w.size == steps + 1
+        _need(w.size == steps + 1, "w.size == steps + 1")
         loss, gl, gg = np.zeros(K), np.zeros(K), np.zeros(K)
         gh = np.zeros(2 * K * n * n)
         gr = np.zeros(2 * K * n * n)
@@ -803,7 +810,7 @@ class EnsembleAdjoint:
         K = self.instances
         r0, ob = self._pack(rho0), self._pack(observable)
         w = np.ascontiguousarray(np.asarray(weights, np.float64))
-        assert w.size == steps + 1
+        _need(w.size == steps + 1, "w.size == steps + 1")
         loss, gl, gg = np.zeros(K), np.zeros(K), np.zeros(K)
         gh, gr = np.zeros(2 * self.offsets[-1]), np.zeros(2 * self.offsets[-1])
 
