@@ -2,8 +2,9 @@
 ensemble adjoint (heom_ensemble_adjoint_*) against single-instance sweeps.
 
   * the static-disorder draw (256 realisations of 7 sites, depth 6, seed 33):
-    the whole ensemble propagated in one ensemble handle, a sample of 8
-    realisations checked against the oracle after 100 steps;
+    the whole ensemble propagated in one ensemble handle (one lockstep class),
+    a sample of 8 realisations checked against the oracle after 100 steps and
+    the first and last bit for bit against their single-instance solves;
   * the uneven draw (64 instances, seed 5): one instance per class (the
     smallest of each of its 18 classes, 4..12 sites, 0 or 1 Matsubara term)
     propagated together, each checked against the oracle (20 steps; 4 for
@@ -46,6 +47,7 @@ def test_static_disorder_draw_sample_matches_oracle():
     systems = bench.ensemble_systems(256)
     tables = [hb.build_tables(s) for s in systems]
     with hb.Ensemble(tables) as E:
+        assert E.classes() == 1
         E.clear()
         for k, s in enumerate(systems):
             E.set_top(k, top0(s.sites))
@@ -53,6 +55,11 @@ def test_static_disorder_draw_sample_matches_oracle():
         for k in range(0, 256, 32):
             assert_pops(E.populations(tops[k], k), oracle_pops(systems[k], 100, 50),
                         what=f"realisation {k} of the 256-member draw")
+    # the draw runs as one lockstep class; its first and last realisations equal their own solves
+    for k in (0, 255):
+        with hb.Heom(**tables[k]) as H:
+            H.set_top(top0(systems[k].sites))
+            assert np.array_equal(tops[k], H.propagate(DT, 100, 50)), f"realisation {k}"
 
 
 def test_uneven_draw_one_instance_per_class_matches_oracle():
