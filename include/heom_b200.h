@@ -325,7 +325,15 @@ int heom_get_instance_top(heom_handle* h, int32_t inst, double* host_top);
 
 /* Ensembles: instances of any sizes (states, depth, Matsubara terms, baths).
  * Instances that can share a batch handle are grouped into one class (in
- * order of first appearance); each class is a batch handle.  One RK4 step of
+ * order of first appearance); each class is a batch handle.  With the product
+ * or Horner scheme, 8 or more instances of one such group with at most 8
+ * states and one depth (the realisations of a static-disorder ensemble) form
+ * a class of their own in the lockstep layout: its state is stored
+ * instance-minor, and its handle (heom_ensemble_class) refuses with
+ * HEOM_E_UNSUPPORTED the calls that read or write a state in the
+ * single-instance layout (heom_set_state, heom_get_state, masks, buffers,
+ * flows, a field, the hierarchy norm); the ensemble calls below serve every
+ * class.  One RK4 step of
  * the ensemble is one CUDA graph in which the classes' stage launches run as
  * concurrent branches; the grid of every class's stage kernel is chosen by
  * heom_ensemble_autotune, which times candidate shapes on the device (run
